@@ -1,0 +1,207 @@
+/*
+ * theseus_b200.h -- C ABI of the B200-native DGSEM right-hand-side evaluation.
+ *
+ * The library evaluates dU/dt = L(U) for the compressible Euler and
+ * Navier-Stokes equations discretised with DGSEM on Legendre-Gauss-Lobatto
+ * nodes, exactly the operator that Theseus exposes as
+ *   RHSOperator<PhysicsT>::Mult(const mfem::Vector &u, mfem::Vector &dudt)
+ *   (include/RHSOperator.hpp:100,172; include/RHSOperator_impl.hpp:719-793)
+ * with the flow-specific body EulerOperator::FlowMult
+ *   (include/EulerOperator_impl.hpp:396-421) or NSOperator::FlowMult
+ *   (include/NSOperator_impl.hpp:161-192).
+ *
+ * Conventions shared by every entry point:
+ *  - State vectors are the MFEM "byNODES" L-vector of an L2 DG space whose
+ *    element DOFs are lexicographic (x fastest):  u[eq][elem][node], with
+ *    eq in [rho, rho*u_0 .. rho*u_{dim-1}, rho*E] (include/GasState.hpp:16-26,
+ *    69-92) and node = i + Np*(j + Np*k).
+ *  - Device pointers are caller-owned CUDA global-memory pointers; the library
+ *    never frees them.  Host pointers are only read during the call.
+ *  - Every call returns a thx_status; no C++ exception crosses the ABI.
+ *  - One handle is bound to one CUDA device (the current device at
+ *    thx_create).  Calls on one handle must not overlap: the handle owns its
+ *    scratch buffers, like the reference's mutable operator caches
+ *    (include/RHSOperator.hpp:129-130).  Distinct handles are independent.
+ *  - thx_rhs and thx_rk3_steps only enqueue work on the given stream (no host
+ *    synchronisation inside).
+ */
+#ifndef THESEUS_B200_H
+#define THESEUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  THX_OK = 0,
+  THX_ERR_INVALID_ARGUMENT = 1,   /* bad size, null pointer, unknown selector */
+  THX_ERR_UNSUPPORTED = 2,        /* valid but not built (order, dim, combination) */
+  THX_ERR_CUDA = 3,               /* a CUDA runtime call failed */
+  THX_ERR_NO_DEVICE = 4,          /* no CUDA device visible: there is no CPU fallback */
+  THX_ERR_OUT_OF_MEMORY = 5,
+  THX_ERR_NUMERICS = 6            /* device-side status flag set (non-positive state, Newton failure) */
+} thx_status;
+
+/* Two-point volume fluxes and surface (Riemann) fluxes.  The numbering is the
+ * reference's selection list (include/SimFactory_impl.hpp:75-128).  Volume and
+ * surface fluxes are selected independently; for the central fluxes
+ * (HLL/LLF/Roe) the volume flux is the arithmetic average of the physical
+ * fluxes, as in include/HLLFlux.hpp:21-51 and include/RoeFlux.hpp:12-37. */
+typedef enum {
+  THX_FLUX_CHANDRASHEKAR = 0, /* include/ChandrashekarFlux.hpp:20-89, face: +scalar dissipation :91-155 */
+  THX_FLUX_RANOCHA = 1,       /* include/RanochaFlux.hpp:20-79, face: +Roe dissipation :81-134 */
+  THX_FLUX_PIROZZOLI = 2,     /* include/PirozzoliFlux.hpp:19-71, face: +Roe dissipation :73-120 */
+  THX_FLUX_HLL = 3,           /* include/HLLFlux.hpp:53-116 */
+  THX_FLUX_LLF = 4,           /* include/LaxFriedrichsFlux.hpp:54-77 */
+  THX_FLUX_ROE = 5,           /* include/RoeFlux.hpp:42-149 */
+  THX_FLUX_COUNT = 6
+} thx_flux;
+
+typedef enum {
+  THX_FLOW_EULER = 0,           /* EulerOperator */
+  THX_FLOW_NAVIER_STOKES = 1    /* NSOperator, BR1 gradients of entropy variables */
+} thx_flow_model;
+
+typedef enum {
+  THX_PRECISION_FP64 = 0,       /* every operation in double */
+  THX_PRECISION_FP32_MIXED = 1  /* flux arithmetic in float, FP64 log-mean series and RK accumulation */
+} thx_precision;
+
+/* Physics and discretisation switches.  Defaults mirror the reference's
+ * runtime JSON defaults (include/SimFactory_impl.hpp:131-135) and
+ * include/Physics.hpp (mu_bulk = 2/3). */
+typedef struct {
+  int32_t flow_model;        /* thx_flow_model */
+  int32_t volume_flux;       /* thx_flux */
+  int32_t surface_flux;      /* thx_flux */
+  int32_t fv_flux;           /* thx_flux used on subcell faces when blending */
+  int32_t blending;          /* 1 = Persson-Peraire indicator + subcell FV blending */
+  int32_t precision;         /* thx_precision */
+  int32_t sutherland;        /* 1 = Sutherland viscosity (reference compile flag SUTHERLAND) */
+  int32_t reserved0;
+  double gamma;              /* 1.4 */
+  double Pr;                 /* 0.72 */
+  double R_gas;              /* 287.05 */
+  double mu;                 /* 0.02 */
+  double mu0;                /* 1.716e-5 (Sutherland) */
+  double mu_bulk;            /* 2/3 */
+  double T0;                 /* 273.15 */
+  double Ts;                 /* 110.4 */
+  double alpha_max;          /* 0.5  (src/Simulation.cpp:482-489) */
+  double alpha_min;          /* 0.001 */
+  double sharpness;          /* 9.21024 (include/RHSOperator.hpp:33) */
+  double modal_threshold;    /* <= 0: 0.5*10^(-1.8 p^0.25) (include/RHSOperator.hpp:64) */
+} thx_config;
+
+/* Mesh and geometric factors, in the layout of the reference's device cache
+ * DGSEMDeviceCacheT (include/dgsem_cache.hpp:173-241), on the host.
+ *
+ *  jac[e][node]                        Tr.Weight() at each LGL node
+ *  metric[e][node][dir][phys]          adjugate Jacobian, row dir
+ *                                      (include/dgsem_cache_utilities.hpp:503-511)
+ *  face_elem[f][2], face_lface[f][2]   minus/plus element of interior face f and
+ *                                      the local face index in that element
+ *                                      (0:x-, 1:x+, 2:y-, 3:y+, 4:z-, 5:z+)
+ *  face_normal[f][fp][dim]             MFEM CalcOrtho normal of side 0, scaled by
+ *                                      the face Jacobian (:601-605)
+ *  face_wminus[f][fp], face_wplus[f][fp]  1/(w0*J) lift weights (:555,609-611)
+ *
+ * Face point fp enumerates the trace nodes of both sides in the same
+ * lexicographic order of the two (one) tangential reference coordinates,
+ * i.e. faces are conforming and aligned.  This replaces MFEM's interior face
+ * restriction (include/dgsem_cache_utilities.hpp:67-79). */
+typedef struct {
+  int32_t dim;               /* 2 or 3 */
+  int32_t order;             /* polynomial order p (Np = p+1 nodes per direction) */
+  int32_t num_elements;
+  int32_t num_faces;         /* interior faces (periodic wrap faces included) */
+  const double *jac;
+  const double *metric;
+  const int32_t *face_elem;
+  const int32_t *face_lface;
+  const double *face_normal;
+  const double *face_wminus;
+  const double *face_wplus;
+} thx_geometry;
+
+typedef struct thx_operator_s *thx_handle;
+
+/* ---- version and status ------------------------------------------------- */
+const char *thx_version(void);
+const char *thx_status_string(int status);
+/* Default configuration (CPG air, Chandrashekar volume / Chandrashekar surface,
+ * blending off, FP64). */
+void thx_config_default(thx_config *cfg);
+
+/* ---- host-side set-up (no device work) ---------------------------------- */
+/* Number of LGL nodes per element (Np^dim), face points (Np^(dim-1)),
+ * conserved variables (dim+2). */
+int thx_sizes(int dim, int order, int32_t *nodes_per_element,
+              int32_t *points_per_face, int32_t *num_equations);
+
+/* Periodic axis-aligned box [lo,hi] split into n[0] x n[1] (x n[2]) equal
+ * elements, numbered x fastest like mfem::Mesh::MakeCartesian2D/3D.  Fills
+ * caller-allocated geometry arrays sized by thx_box_counts.  Stands in for
+ * MFEM's mesh + FiniteElementSpace + geometric-factor set-up
+ * (include/dgsem_cache_utilities.hpp:83-215, 516-639) for this mesh family. */
+int thx_box_counts(int dim, const int32_t *n, int32_t *num_elements,
+                   int32_t *num_faces);
+int thx_box_geometry(int dim, int order, const int32_t *n, const double *lo,
+                     const double *hi, double *jac, double *metric,
+                     int32_t *face_elem, int32_t *face_lface,
+                     double *face_normal, double *face_wminus,
+                     double *face_wplus, double *node_coords /* [dim][e][node] or NULL */);
+
+/* LGL nodes and weights on [0,1] (MFEM's GaussLobatto rule on the segment). */
+int thx_lgl(int np, double *x, double *w);
+
+/* ---- operator ------------------------------------------------------------ */
+/* Builds the operator on the current CUDA device: uploads geometry, derives
+ * D, D-hat, D-hat2 (include/dgsem_cache_utilities.hpp:123-181), subcell
+ * metrics (:641-763) and the Persson modal transform (:867-943).
+ * Replaces RHSOperator::Finalize (include/RHSOperator_impl.hpp:273-314) and
+ * MakeRHSOperator (include/SimFactory_impl.hpp:63-488). */
+int thx_create(const thx_geometry *geom, const thx_config *cfg,
+               thx_handle *out);
+int thx_destroy(thx_handle h);
+
+/* dudt = L(u).  u and dudt are device L-vectors (byNODES).  For
+ * THX_PRECISION_FP64 they hold double; for THX_PRECISION_FP32_MIXED they hold
+ * float (the FP32 working copy).  Replaces RHSOperator<PhysicsT>::Mult
+ * (include/RHSOperator_impl.hpp:719-793). */
+int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream);
+
+/* nsteps SSP-RK3 steps (Shu-Osher form, as mfem::RK3SSPSolver::Step driven at
+ * src/Simulation.cpp:1255) on a device FP64 state u, in place, with fixed dt.
+ * In FP32-mixed mode the FP64 master state is accumulated in double and each
+ * RHS is evaluated on a float working copy. */
+int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream);
+
+/* Per-element blending coefficient alpha of the last RHS (device, double[E])
+ * and the Persson smoothness eta (double[E]); either pointer may be NULL.
+ * Mirrors ComputeBlendingCoefficient / CheckIndicatorSmoothness
+ * (include/RHSOperator_impl.hpp:411-527). */
+int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev,
+                              void *stream);
+
+/* Stable time step estimate: sigma = max(adv, surface) + diffusive rate and
+ * dt = cfl/sigma (include/RHSOperator_impl.hpp:10-270,
+ * include/StabilityEstimate.hpp:12-92).  u is a device FP64 state.  Blocks
+ * until the reduction is finished (it returns a host value). */
+int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out,
+                    double *rates_out /* [3]: advective, surface, diffusive */);
+
+/* Device status word of the last evaluations (non-finite or non-positive
+ * density/pressure seen).  Reading it synchronises the stream. */
+int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
+
+/* Diagnostics of the configured kernels (for roofline bookkeeping). */
+int thx_describe(thx_handle h, char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* THESEUS_B200_H */

@@ -1,0 +1,256 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle.
+
+Loads oracle/libthx_oracle.so (the FP64 restatement of the reference's DGSEM
+right-hand side, built by `make -C oracle`) and, when it was built here,
+oracle/_ref/libthx_ref.so (the reference's own header kernels driven by
+oracle/ref_harness.cpp).  Only tests, the smoke check and the benchmark's CPU
+baseline import this module; the product never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from theseus_b200._abi import Config, Geometry, make_config, FLOW_NAVIER_STOKES  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libthx_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libthx_ref.so")
+
+_lib = None
+_ref = None
+
+D = C.POINTER(C.c_double)
+I32 = C.POINTER(C.c_int32)
+
+
+def build(ref=False):
+    """Compile the oracle (and, if asked and the reference tree exists, _ref)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+    if ref and os.path.isdir("/root/reference/include"):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(REF_PATH)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(REF_PATH)
+    return _ref
+
+
+def _dp(a):
+    return a.ctypes.data_as(D) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(I32) if a is not None else None
+
+
+def sizes(dim, order):
+    N = order + 1
+    return (N ** dim, N ** (dim - 1), dim + 2)
+
+
+class Mesh:
+    """Geometry arrays in the thx_geometry layout, kept alive for ctypes."""
+
+    def __init__(self, dim, order, jac, metric, face_elem, face_lface, face_normal,
+                 face_wminus, face_wplus, coords=None, shape=None):
+        self.dim, self.order = dim, order
+        self.jac = np.ascontiguousarray(jac, dtype=np.float64)
+        self.metric = np.ascontiguousarray(metric, dtype=np.float64)
+        self.face_elem = np.ascontiguousarray(face_elem, dtype=np.int32)
+        self.face_lface = np.ascontiguousarray(face_lface, dtype=np.int32)
+        self.face_normal = np.ascontiguousarray(face_normal, dtype=np.float64)
+        self.face_wminus = np.ascontiguousarray(face_wminus, dtype=np.float64)
+        self.face_wplus = np.ascontiguousarray(face_wplus, dtype=np.float64)
+        self.coords = coords
+        self.shape = shape
+        self.num_elements = self.jac.shape[0]
+        self.num_faces = self.face_elem.shape[0]
+        self.nd, self.nfp, self.neq = sizes(dim, order)
+
+    def struct(self):
+        g = Geometry()
+        g.dim, g.order = self.dim, self.order
+        g.num_elements, g.num_faces = self.num_elements, self.num_faces
+        g.jac, g.metric = _dp(self.jac), _dp(self.metric)
+        g.face_elem, g.face_lface = _ip(self.face_elem), _ip(self.face_lface)
+        g.face_normal = _dp(self.face_normal)
+        g.face_wminus, g.face_wplus = _dp(self.face_wminus), _dp(self.face_wplus)
+        self._g = g
+        return g
+
+    def state_shape(self):
+        return (self.neq, self.num_elements, self.nd)
+
+
+def box_mesh(dim, order, n, lo, hi):
+    """Periodic Cartesian box, restated in the oracle (independent of the product)."""
+    nd, nfp, neq = sizes(dim, order)
+    nn = list(n) + [1] * (3 - len(n))
+    ne = int(np.prod(nn[:dim]))
+    nf = dim * ne
+    jac = np.zeros((ne, nd))
+    metric = np.zeros((ne, nd, dim, dim))
+    fe = np.zeros((nf, 2), np.int32)
+    fl = np.zeros((nf, 2), np.int32)
+    fn = np.zeros((nf, nfp, dim))
+    wm = np.zeros((nf, nfp))
+    wp = np.zeros((nf, nfp))
+    coords = np.zeros((dim, ne, nd))
+    n32 = np.array(nn, np.int32)
+    lo = np.array(list(lo) + [0.0] * (3 - len(lo)))
+    hi = np.array(list(hi) + [1.0] * (3 - len(hi)))
+    st = lib().orc_box_geometry(dim, order, _ip(n32), _dp(lo), _dp(hi), _dp(jac), _dp(metric),
+                                _ip(fe), _ip(fl), _dp(fn), _dp(wm), _dp(wp), _dp(coords))
+    if st:
+        raise RuntimeError(f"orc_box_geometry failed ({st})")
+    return Mesh(dim, order, jac, metric, fe, fl, fn, wm, wp, coords=coords, shape=tuple(nn[:dim]))
+
+
+def _check(st, what):
+    if st:
+        raise RuntimeError(f"{what} failed with status {st}")
+
+
+def rhs(mesh, cfg, u, nthreads=1, want_alpha=False):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    du = np.zeros_like(u)
+    alpha = np.zeros(mesh.num_elements) if want_alpha else None
+    eta = np.zeros(mesh.num_elements) if want_alpha else None
+    _check(lib().orc_rhs(C.byref(mesh.struct()), C.byref(cfg), _dp(u), _dp(du), int(nthreads),
+                         _dp(alpha), _dp(eta)), "orc_rhs")
+    if want_alpha:
+        return du, alpha, eta
+    return du
+
+
+def gradient(mesh, cfg, u, nthreads=1):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    g = np.zeros((mesh.dim,) + u.shape)
+    _check(lib().orc_gradient(C.byref(mesh.struct()), C.byref(cfg), _dp(u), _dp(g), int(nthreads)),
+           "orc_gradient")
+    return g
+
+
+def rk3_steps(mesh, cfg, u, dt, nsteps, nthreads=1):
+    u = np.array(u, dtype=np.float64, copy=True)
+    _check(lib().orc_rk3_steps(C.byref(mesh.struct()), C.byref(cfg), _dp(u), C.c_double(dt),
+                               int(nsteps), int(nthreads)), "orc_rk3_steps")
+    return u
+
+
+def estimate_dt(mesh, cfg, u, cfl):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    dt = C.c_double()
+    rates = np.zeros(3)
+    _check(lib().orc_estimate_dt(C.byref(mesh.struct()), C.byref(cfg), _dp(u), C.c_double(cfl),
+                                 C.byref(dt), _dp(rates)), "orc_estimate_dt")
+    return dt.value, rates
+
+
+def blending(mesh, cfg, u):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    a = np.zeros(mesh.num_elements)
+    e = np.zeros(mesh.num_elements)
+    _check(lib().orc_blending(C.byref(mesh.struct()), C.byref(cfg), _dp(u), _dp(a), _dp(e)),
+           "orc_blending")
+    return a, e
+
+
+def entropy_residual(mesh, cfg, u, du):
+    out = C.c_double()
+    _check(lib().orc_entropy_residual(C.byref(mesh.struct()), C.byref(cfg),
+                                      _dp(np.ascontiguousarray(u, np.float64)),
+                                      _dp(np.ascontiguousarray(du, np.float64)), C.byref(out)),
+           "orc_entropy_residual")
+    return out.value
+
+
+def operators(order):
+    N = order + 1
+    Dm, Dh, Dh2 = np.zeros(N * N), np.zeros(N * N), np.zeros(N * N)
+    _check(lib().orc_operators(order, _dp(Dm), _dp(Dh), _dp(Dh2)), "orc_operators")
+    x, w = np.zeros(N), np.zeros(N)
+    _check(lib().orc_lgl(N, _dp(x), _dp(w)), "orc_lgl")
+    return x, w, Dm, Dh, Dh2
+
+
+def subcell_metrics(mesh, cfg):
+    dim, N, ne = mesh.dim, mesh.order + 1, mesh.num_elements
+    Nz = N if dim > 2 else 1
+    xi = np.zeros(((N + 1) * N * Nz) * dim * ne)
+    eta = np.zeros((N * (N + 1) * Nz) * dim * ne)
+    zeta = np.zeros((N * N * (N + 1)) * dim * ne) if dim > 2 else np.zeros(1)
+    _check(lib().orc_subcell_metrics(C.byref(mesh.struct()), C.byref(cfg), _dp(xi), _dp(eta),
+                                     _dp(zeta)), "orc_subcell_metrics")
+    return xi, eta, zeta
+
+
+def _point(fn, flux, cfg, dim, *arrs):
+    arrs = [np.ascontiguousarray(a, np.float64) for a in arrs]
+    F = np.zeros(dim + 2)
+    _check(fn(int(flux), C.byref(cfg), int(dim), *[_dp(a) for a in arrs], _dp(F)), "pointwise flux")
+    return F
+
+
+def volume_flux(flux, cfg, dim, q1, q2, m1, m2, use_ref=False):
+    L = ref() if use_ref else lib()
+    fn = L.ref_volume_flux if use_ref else L.orc_volume_flux
+    return _point(fn, flux, cfg, dim, q1, q2, m1, m2)
+
+
+def face_flux(flux, cfg, dim, qm, qp, n, use_ref=False):
+    L = ref() if use_ref else lib()
+    fn = L.ref_face_flux if use_ref else L.orc_face_flux
+    return _point(fn, flux, cfg, dim, qm, qp, n)
+
+
+def entropy_vars(cfg, dim, q, use_ref=False):
+    L = ref() if use_ref else lib()
+    fn = L.ref_entropy_vars if use_ref else L.orc_entropy_vars
+    w = np.zeros(dim + 2)
+    _check(fn(C.byref(cfg), int(dim), _dp(np.ascontiguousarray(q, np.float64)), _dp(w)), "entropy")
+    return w
+
+
+def viscous_flux(cfg, dim, q, dprim, use_ref=False):
+    L = ref() if use_ref else lib()
+    fn = L.ref_viscous_flux if use_ref else L.orc_viscous_flux
+    out = np.zeros((dim + 2) * dim)
+    _check(fn(C.byref(cfg), int(dim), _dp(np.ascontiguousarray(q, np.float64)),
+              _dp(np.ascontiguousarray(dprim, np.float64)), _dp(out)), "viscous")
+    return out.reshape(dim + 2, dim)
+
+
+def ref_rhs(mesh, cfg, u, alpha=None):
+    """Full RHS through the reference's own point kernels (oracle/_ref)."""
+    x, w, Dm, Dh, Dh2 = operators(mesh.order)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    du = np.zeros_like(u)
+    xi = eta = zeta = None
+    if alpha is not None:
+        xi, eta, zeta = subcell_metrics(mesh, cfg)
+        alpha = np.ascontiguousarray(alpha, np.float64)
+    _check(ref().ref_rhs(C.byref(mesh.struct()), C.byref(cfg), _dp(Dm), _dp(Dh), _dp(Dh2), _dp(w),
+                         _dp(alpha), _dp(xi), _dp(eta), _dp(zeta), _dp(u), _dp(du)), "ref_rhs")
+    return du
+
+
+def max_threads():
+    return lib().orc_max_threads()
