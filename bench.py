@@ -1,0 +1,341 @@
+"""Benchmark: DGSEM right-hand-side throughput (DOF*RHS/s) on the
+Navier-Stokes Taylor-Green vortex, 32^3 hex mesh, p=4 (4,096,000 LGL nodes x 5
+conserved variables), Ranocha volume / HLL surface flux, BR1 viscous terms,
+Ma=0.1, Re=1600, Pr=0.71, FP64.  One step = one right-hand side L(u) of the
+whole mesh (RHSOperator::Mult).  DOF = solution nodes (E*N^d).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  --impl reference times the CPU implementation
+of the path (the FP64 oracle restatement of the reference's RHS, all host
+threads) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "ns_tgv_32^3_p4", "mesh": [32, 32, 32], "order": 4, "dim": 3,
+            "volume_flux": "ranocha", "surface_flux": "hll", "mach": 0.1, "reynolds": 1600,
+            "Pr": 0.71, "noise": 1e-6}
+METRIC = "DOF*RHS/s (solution nodes x right-hand-side evaluations per second)"
+UNIT = "DOF*RHS/s"
+
+
+def build_case(n=None, order=4):
+    import theseus_b200 as T
+    from theseus_b200 import cases
+    n = n or WORKLOAD["mesh"]
+    m = T.periodic_box(3, order, n, [0.0] * 3, [2 * np.pi] * 3)
+    u = cases.taylor_green(m.coords, mach=WORKLOAD["mach"], noise=WORKLOAD["noise"], seed=0)
+    return m, u
+
+
+def physics():
+    return dict(mu=1.0 / WORKLOAD["reynolds"], Pr=WORKLOAD["Pr"])
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except OSError:
+            pass
+        finally:
+            if self.path:
+                try:
+                    os.unlink(self.path)
+                except OSError:
+                    pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_per_phase(m, elem_size=8):
+    """Algorithmic HBM bytes of each kernel for one RHS (compressed geometry):
+    gradient: read u, write grad; face: read both traces of u and grad, write F*;
+    volume: read u, grad, F* once, write dudt."""
+    nodes = m.num_nodes
+    neq, dim = m.neq, m.dim
+    fpts = m.num_faces * m.nfp
+    s = elem_size
+    grad = nodes * neq * s + nodes * dim * neq * s
+    face = fpts * (2 * neq + 2 * dim * neq + neq) * s
+    vol = nodes * neq * s * 2 + nodes * dim * neq * s + fpts * neq * s
+    return {"blend": nodes * neq * s, "grad": grad, "face": face, "volume": vol}
+
+
+def cpu_reference(args, sample_n=(16, 16, 16), budget_s=20.0):
+    """FP64 oracle on a bounded sample of the workload, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import theseus_b200 as T
+    m, u = build_case(sample_n)
+    om = O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
+                m.face_wminus, m.face_wplus)
+    cfg = T.make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
+                        surface_flux=WORKLOAD["surface_flux"], **physics())
+    threads = O.max_threads()
+    O.rhs(om, cfg, u, nthreads=threads)  # warm-up
+    t0 = time.perf_counter()
+    evals = 0
+    while True:
+        O.rhs(om, cfg, u, nthreads=threads)
+        evals += 1
+        if time.perf_counter() - t0 > budget_s or evals >= 200:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": m.num_nodes * evals / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"TGV {sample_n[0]}x{sample_n[1]}x{sample_n[2]} p=4 ({m.num_nodes} nodes), "
+                      f"{evals} RHS evaluations in {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import theseus_b200 as T
+    sample = (16, 16, 16)
+    m, u = build_case(sample)
+    om = O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
+                m.face_wminus, m.face_wplus)
+    cfg = T.make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
+                        surface_flux=WORKLOAD["surface_flux"], **physics())
+    threads = O.max_threads()
+    for _ in range(args.warmup):
+        O.rhs(om, cfg, u, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.rhs(om, cfg, u, nthreads=threads)
+    dt = time.perf_counter() - t0
+    value = m.num_nodes * args.steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": dict(WORKLOAD, sample=f"{sample[0]}^3 p=4 sub-mesh of the workload",
+                           parallelism="cpu threads"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"TGV {sample[0]}^3 p=4 ({m.num_nodes} nodes) per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import theseus_b200 as T
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        import datetime
+        dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = dist_
+    m, u = build_case()
+    prec = "fp32" if args.precision == "fp32" else "fp64"
+    op = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"], surface_flux=WORKLOAD["surface_flux"],
+                      precision=prec, **physics())
+    ud = torch.as_tensor(u, device="cuda").to(op.dtype).contiguous()
+    du = torch.empty_like(ud)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        op.Mult(ud, du)
+    barrier()
+    with ClockSampler(local) as clk:
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            op.Mult(ud, du)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    nodes = m.num_nodes
+    value = world * nodes * args.steps / (ms * 1e-3)
+
+    # end to end through the C ABI with host buffers (pinned), copies timed
+    hu = torch.as_tensor(u).to(op.dtype).pin_memory()
+    hdu = torch.empty_like(hu).pin_memory()
+    for _ in range(2):
+        ud.copy_(hu, non_blocking=True)
+        op.Mult(ud, du)
+        hdu.copy_(du, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ud.copy_(hu, non_blocking=True)
+        op.Mult(ud, du)
+        hdu.copy_(du, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * nodes * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": hu.numel() * hu.element_size(),
+           "d2h_bytes_per_step": hdu.numel() * hdu.element_size()}
+
+    # per-kernel device times for the roofline (after the timed region)
+    ud.copy_(torch.as_tensor(u).to(op.dtype))
+    phases = np.zeros(4)
+    nprof = max(3, min(args.steps, 10))
+    for _ in range(nprof):
+        phases += np.array(op.profile(ud, du))
+    phases /= nprof
+    names = ["blend", "grad", "face", "volume"]
+    algo = bytes_per_phase(m, 4 if prec == "fp32" else 8)
+    dom = int(np.argmax(phases))
+    peak, peak_kind = peaks()
+    achieved = algo[names[dom]] / (phases[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": names[dom] + "_kernel", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": None,
+                "phase_ms": {k: float(v) for k, v in zip(names, phases)},
+                "algorithmic_bytes": {k: int(v) for k, v in algo.items()}}
+    # FP64 pipe view of the flux-differencing kernel: pairs x F_pair flops
+    pairs = m.num_elements * 3 * 25 * 10
+    roofline["volume_pair_evals_per_s"] = pairs / (phases[3] * 1e-3)
+
+    # FP32-mixed companion number and its error against FP64
+    extra = {}
+    if prec == "fp64" and not args.no_mixed:
+        op32 = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"],
+                            surface_flux=WORKLOAD["surface_flux"], precision="fp32", **physics())
+        u32 = torch.as_tensor(u, device="cuda").float().contiguous()
+        d32 = torch.empty_like(u32)
+        for _ in range(3):
+            op32.Mult(u32, d32)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            op32.Mult(u32, d32)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms32 = a.elapsed_time(b)
+        op.Mult(torch.as_tensor(u, device="cuda"), du)
+        ref = du.double()
+        err = ((d32.double() - ref).pow(2).sum(dim=(1, 2)) / ref.pow(2).sum(dim=(1, 2))).sqrt()
+        extra["fp32_mixed"] = {"value": nodes * args.steps / (ms32 * 1e-3), "unit": UNIT,
+                               "rhs_rel_l2_vs_fp64_max": float(err.max().item()),
+                               "speedup_vs_fp64": (ms / ms32) if ms32 > 0 else None}
+        del op32
+
+    launches = args.steps * (3 if True else 2)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32-mixed",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, precision=prec, parallelism=f"replicas x{world}",
+                           l2="working set (u 164 MB, gradients 492 MB) larger than the 126 MB L2",
+                           kernel_layout=op.describe()),
+            "e2e": e2e, "roofline": roofline, "clocks": clk.summary(),
+            "gpu_launches": launches}
+    line.update(extra)
+    if rank == 0 and not args.skip_cpu:
+        line["cpu_baseline"] = cpu_reference(args)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -81,7 +81,8 @@ typedef struct {
   int32_t blending;          /* 1 = Persson-Peraire indicator + subcell FV blending */
   int32_t precision;         /* thx_precision */
   int32_t sutherland;        /* 1 = Sutherland viscosity (reference compile flag SUTHERLAND) */
-  int32_t reserved0;
+  int32_t geometry_layout;   /* 0: store geometric factors once where they are exactly
+                                constant over nodes/elements/faces; 1: full per-node arrays */
   double gamma;              /* 1.4 */
   double Pr;                 /* 0.72 */
   double R_gas;              /* 287.05 */
@@ -200,6 +201,12 @@ int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
 
 /* Diagnostics of the configured kernels (for roofline bookkeeping). */
 int thx_describe(thx_handle h, char *buf, size_t len);
+
+/* One right-hand side like thx_rhs, with CUDA events between its kernels;
+ * synchronises the stream and returns the device time of each phase in
+ * milliseconds: ms[0] indicator, ms[1] gradient, ms[2] face fluxes,
+ * ms[3] volume + lift (0 for phases the configuration does not run). */
+int thx_rhs_profile(thx_handle h, const void *u, void *dudt, void *stream, double *ms);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,290 @@
+"""theseus_b200 -- B200-native DGSEM right-hand side (sm_100a CUDA behind a C ABI).
+
+Python mirror of the reference's operator interface:
+
+    op = MakeRHSOperator({"flow_model": "navier-stokes", "numerical_flux": "ranocha",
+                          "surface_flux": "hll"}, mesh)
+    op.Mult(u, dudt)                 # RHSOperator<PhysicsT>::Mult (include/RHSOperator.hpp:100)
+    op.EstimateStability(u)          # include/RHSOperator_impl.hpp:10-270
+    op.rk3_steps(u, dt, nsteps)      # mfem::RK3SSPSolver::Step, fused on the device
+
+States are torch CUDA tensors shaped (num_equations, num_elements, nodes_per_element)
+holding the byNODES L-vector.  The shared library is loaded from this package
+directory; if it is missing, or no CUDA device is visible, every compute call
+raises -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (Config, Geometry, make_config, flux_id, FLUX, FLUX_NAMES,  # noqa: F401
+                   FLOW_EULER, FLOW_NAVIER_STOKES, PRECISION_FP64, PRECISION_FP32_MIXED,
+                   THX_OK)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtheseus_b200.so")
+
+_lib = None
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int32)
+
+
+class THXError(RuntimeError):
+    pass
+
+
+def library():
+    """Load libtheseus_b200.so (build it with theseus_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise THXError(f"{LIB_PATH} is missing: run `python theseus_b200/build.py` "
+                           "(the CUDA extension is required; there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        lib.thx_version.restype = C.c_char_p
+        lib.thx_status_string.restype = C.c_char_p
+        lib.thx_create.argtypes = [C.POINTER(Geometry), C.POINTER(Config), C.POINTER(C.c_void_p)]
+        lib.thx_destroy.argtypes = [C.c_void_p]
+        lib.thx_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.thx_rk3_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        lib.thx_blending_coefficients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.thx_estimate_dt.argtypes = [C.c_void_p, C.c_void_p, C.c_double, _D, _D]
+        lib.thx_read_status.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
+        lib.thx_describe.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        lib.thx_rhs_profile.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _D]
+        _lib = lib
+    return _lib
+
+
+def _check(st, what):
+    if st != THX_OK:
+        msg = library().thx_status_string(st).decode()
+        raise THXError(f"{what}: {msg} (status {st})")
+
+
+def sizes(dim, order):
+    N = order + 1
+    return N ** dim, N ** (dim - 1), dim + 2
+
+
+class Mesh:
+    """Geometric factors in the thx_geometry layout (host numpy arrays)."""
+
+    def __init__(self, dim, order, jac, metric, face_elem, face_lface, face_normal, face_wminus,
+                 face_wplus, coords=None, shape=None):
+        self.dim, self.order = int(dim), int(order)
+        self.jac = np.ascontiguousarray(jac, np.float64)
+        self.metric = np.ascontiguousarray(metric, np.float64)
+        self.face_elem = np.ascontiguousarray(face_elem, np.int32)
+        self.face_lface = np.ascontiguousarray(face_lface, np.int32)
+        self.face_normal = np.ascontiguousarray(face_normal, np.float64)
+        self.face_wminus = np.ascontiguousarray(face_wminus, np.float64)
+        self.face_wplus = np.ascontiguousarray(face_wplus, np.float64)
+        self.coords = coords
+        self.shape = shape
+        self.num_elements = self.jac.shape[0]
+        self.num_faces = self.face_elem.shape[0]
+        self.nd, self.nfp, self.neq = sizes(self.dim, self.order)
+
+    @property
+    def num_nodes(self):
+        return self.num_elements * self.nd
+
+    def state_shape(self):
+        return (self.neq, self.num_elements, self.nd)
+
+    def struct(self):
+        g = Geometry()
+        g.dim, g.order, g.num_elements, g.num_faces = self.dim, self.order, self.num_elements, self.num_faces
+        g.jac = self.jac.ctypes.data_as(_D)
+        g.metric = self.metric.ctypes.data_as(_D)
+        g.face_elem = self.face_elem.ctypes.data_as(_I)
+        g.face_lface = self.face_lface.ctypes.data_as(_I)
+        g.face_normal = self.face_normal.ctypes.data_as(_D)
+        g.face_wminus = self.face_wminus.ctypes.data_as(_D)
+        g.face_wplus = self.face_wplus.ctypes.data_as(_D)
+        self._g = g
+        return g
+
+
+def periodic_box(dim, order, n, lo, hi, coords=True):
+    """Periodic Cartesian box mesh (host set-up in the library, no device work)."""
+    lib = library()
+    nd, nfp, neq = sizes(dim, order)
+    n32 = np.array(list(n) + [1] * (3 - len(n)), np.int32)
+    ne, nf = C.c_int32(), C.c_int32()
+    _check(lib.thx_box_counts(dim, n32.ctypes.data_as(_I), C.byref(ne), C.byref(nf)), "thx_box_counts")
+    ne, nf = ne.value, nf.value
+    jac = np.zeros((ne, nd))
+    metric = np.zeros((ne, nd, dim, dim))
+    fe = np.zeros((nf, 2), np.int32)
+    fl = np.zeros((nf, 2), np.int32)
+    fn = np.zeros((nf, nfp, dim))
+    wm = np.zeros((nf, nfp))
+    wp = np.zeros((nf, nfp))
+    xyz = np.zeros((dim, ne, nd)) if coords else None
+    lo3 = np.array(list(lo) + [0.0] * (3 - len(lo)))
+    hi3 = np.array(list(hi) + [1.0] * (3 - len(hi)))
+    _check(lib.thx_box_geometry(dim, order, n32.ctypes.data_as(_I), lo3.ctypes.data_as(_D),
+                                hi3.ctypes.data_as(_D), jac.ctypes.data_as(_D),
+                                metric.ctypes.data_as(_D), fe.ctypes.data_as(_I),
+                                fl.ctypes.data_as(_I), fn.ctypes.data_as(_D), wm.ctypes.data_as(_D),
+                                wp.ctypes.data_as(_D),
+                                xyz.ctypes.data_as(_D) if coords else None), "thx_box_geometry")
+    return Mesh(dim, order, jac, metric, fe, fl, fn, wm, wp, coords=xyz, shape=tuple(n[:dim]))
+
+
+def lgl(np_):
+    x, w = np.zeros(np_), np.zeros(np_)
+    _check(library().thx_lgl(np_, x.ctypes.data_as(_D), w.ctypes.data_as(_D)), "thx_lgl")
+    return x, w
+
+
+def _stream_ptr(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class RHSOperator:
+    """Mirror of Theseus::RHSOperator<PhysicsT> (include/RHSOperator.hpp:119-188)
+    whose Mult forwards to the sm_100a kernels through the C ABI."""
+
+    flow = "euler"
+
+    def __init__(self, mesh, numerical_flux="chandrashekar", surface_flux=None, fv_flux="llf",
+                 blending=False, precision="fp64", device=None, **physics):
+        import torch
+        if not torch.cuda.is_available():
+            raise THXError("no CUDA device: the DGSEM operator has no CPU fallback")
+        self.mesh = mesh
+        self.cfg = make_config(flow=self.flow, volume_flux=numerical_flux,
+                               surface_flux=surface_flux, fv_flux=fv_flux, blending=blending,
+                               precision=precision, **physics)
+        self.mixed = self.cfg.precision == PRECISION_FP32_MIXED
+        self.dtype = torch.float32 if self.mixed else torch.float64
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            _check(library().thx_create(C.byref(mesh.struct()), C.byref(self.cfg), C.byref(h)),
+                   "thx_create")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                library().thx_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # -- shape helpers --------------------------------------------------
+    @property
+    def height(self):
+        return self.mesh.neq * self.mesh.num_nodes
+
+    def _check_state(self, t, dtype):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()
+                and t.numel() == self.height and t.device == self.device):
+            raise THXError(f"expected a contiguous {dtype} CUDA tensor with {self.height} entries "
+                           f"on {self.device}")
+
+    # -- the reference interface ------------------------------------------
+    def Mult(self, u, dudt, stream=None):
+        """dudt = L(u)."""
+        self._check_state(u, self.dtype)
+        self._check_state(dudt, self.dtype)
+        _check(library().thx_rhs(self._h, C.c_void_p(u.data_ptr()), C.c_void_p(dudt.data_ptr()),
+                                 _stream_ptr(stream)), "thx_rhs")
+        return dudt
+
+    def EstimateStability(self, u):
+        """(advective, surface, diffusive) rates (include/StabilityEstimate.hpp:38-54)."""
+        import torch
+        self._check_state(u, torch.float64)
+        dt = C.c_double()
+        rates = np.zeros(3)
+        torch.cuda.current_stream().synchronize()
+        _check(library().thx_estimate_dt(self._h, C.c_void_p(u.data_ptr()), 1.0, C.byref(dt),
+                                         rates.ctypes.data_as(_D)), "thx_estimate_dt")
+        return rates
+
+    def estimate_dt(self, u, cfl):
+        r = self.EstimateStability(u)
+        return cfl / (max(r[0], r[1]) + r[2])
+
+    def rk3_steps(self, u, dt, nsteps, stream=None):
+        """nsteps SSP-RK3 steps on the FP64 master state u, in place."""
+        import torch
+        self._check_state(u, torch.float64)
+        _check(library().thx_rk3_steps(self._h, C.c_void_p(u.data_ptr()), float(dt), int(nsteps),
+                                       _stream_ptr(stream)), "thx_rk3_steps")
+        return u
+
+    def blending_coefficients(self, stream=None):
+        import torch
+        a = torch.zeros(self.mesh.num_elements, dtype=torch.float64, device=self.device)
+        e = torch.zeros_like(a)
+        _check(library().thx_blending_coefficients(self._h, C.c_void_p(a.data_ptr()),
+                                                   C.c_void_p(e.data_ptr()), _stream_ptr(stream)),
+               "thx_blending_coefficients")
+        return a, e
+
+    def read_status(self, stream=None):
+        v = C.c_uint32()
+        _check(library().thx_read_status(self._h, C.byref(v), _stream_ptr(stream)), "thx_read_status")
+        return v.value
+
+    def profile(self, u, dudt, stream=None):
+        """One Mult with per-kernel device times (ms): indicator, gradient, faces, volume."""
+        self._check_state(u, self.dtype)
+        self._check_state(dudt, self.dtype)
+        ms = np.zeros(4)
+        _check(library().thx_rhs_profile(self._h, C.c_void_p(u.data_ptr()),
+                                         C.c_void_p(dudt.data_ptr()), _stream_ptr(stream),
+                                         ms.ctypes.data_as(_D)), "thx_rhs_profile")
+        return ms
+
+    def describe(self):
+        buf = C.create_string_buffer(1024)
+        _check(library().thx_describe(self._h, buf, 1024), "thx_describe")
+        return buf.value.decode()
+
+    def NumFluxName(self):
+        return FLUX_NAMES[self.cfg.volume_flux]
+
+    def FlowModelName(self):
+        return self.flow
+
+
+class EulerOperator(RHSOperator):
+    """Mirror of Theseus::EulerOperator (include/EulerOperator.hpp)."""
+    flow = "euler"
+
+
+class NSOperator(RHSOperator):
+    """Mirror of Theseus::NSOperator (include/NSOperator.hpp)."""
+    flow = "navier-stokes"
+
+
+def MakeRHSOperator(runtime, mesh, device=None):
+    """Selection by the reference's runtime JSON keys (include/SimFactory_impl.hpp:63-488):
+    flow_model, numerical_flux, gamma, Pr, R_gas, mu; plus the keys this library adds to
+    decouple the volume and surface fluxes (surface_flux, fv_flux), blending and precision."""
+    flow = str(runtime.get("flow_model", "euler")).lower()
+    viscous = flow.startswith(("visc", "nav", "cns", "ns"))
+    gas = str(runtime.get("gas_model", "cpg")).lower()
+    if gas not in ("", "cpg", "ideal", "ideal_gas"):
+        raise THXError(f"gas_model '{gas}' is not built in this library")
+    cls = NSOperator if viscous else EulerOperator
+    phys = {k: runtime[k] for k in ("gamma", "Pr", "R_gas", "mu", "mu0") if k in runtime}
+    if "alpha_max" in runtime:
+        phys["alpha_max"] = runtime["alpha_max"]
+    return cls(mesh, numerical_flux=runtime.get("numerical_flux", "chandrashekar"),
+               surface_flux=runtime.get("surface_flux"), fv_flux=runtime.get("fv_flux", "llf"),
+               blending=bool(runtime.get("blending", False)),
+               precision=runtime.get("precision", "fp64"), device=device, **phys)

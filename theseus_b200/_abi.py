@@ -24,7 +24,7 @@ class Config(C.Structure):
     _fields_ = [
         ("flow_model", C.c_int32), ("volume_flux", C.c_int32), ("surface_flux", C.c_int32),
         ("fv_flux", C.c_int32), ("blending", C.c_int32), ("precision", C.c_int32),
-        ("sutherland", C.c_int32), ("reserved0", C.c_int32),
+        ("sutherland", C.c_int32), ("geometry_layout", C.c_int32),
         ("gamma", C.c_double), ("Pr", C.c_double), ("R_gas", C.c_double), ("mu", C.c_double),
         ("mu0", C.c_double), ("mu_bulk", C.c_double), ("T0", C.c_double), ("Ts", C.c_double),
         ("alpha_max", C.c_double), ("alpha_min", C.c_double), ("sharpness", C.c_double),
@@ -63,7 +63,8 @@ def flux_id(name_or_id):
 def make_config(flow="euler", volume_flux="chandrashekar", surface_flux=None, fv_flux="llf",
                 blending=False, precision="fp64", gamma=1.4, Pr=0.72, R_gas=287.05, mu=0.02,
                 mu0=1.716e-5, mu_bulk=2.0 / 3.0, T0=273.15, Ts=110.4, alpha_max=0.5,
-                alpha_min=0.001, sharpness=9.21024, modal_threshold=0.0, sutherland=False):
+                alpha_min=0.001, sharpness=9.21024, modal_threshold=0.0, sutherland=False,
+                geometry_layout=0):
     cfg = Config()
     f = str(flow).lower()
     viscous = f.startswith(("visc", "nav", "cns", "ns"))
@@ -74,6 +75,7 @@ def make_config(flow="euler", volume_flux="chandrashekar", surface_flux=None, fv
     cfg.blending = 1 if blending else 0
     cfg.precision = PRECISION_FP32_MIXED if str(precision).lower() in ("fp32", "fp32_mixed", "mixed") else PRECISION_FP64
     cfg.sutherland = 1 if sutherland else 0
+    cfg.geometry_layout = int(geometry_layout)
     cfg.gamma, cfg.Pr, cfg.R_gas, cfg.mu, cfg.mu0 = gamma, Pr, R_gas, mu, mu0
     cfg.mu_bulk, cfg.T0, cfg.Ts = mu_bulk, T0, Ts
     cfg.alpha_max, cfg.alpha_min, cfg.sharpness = alpha_max, alpha_min, sharpness

@@ -1,0 +1,731 @@
+// thx_api.cu -- the C ABI (include/theseus_b200.h): operator set-up on the
+// device, kernel selection, right-hand side, fused SSP-RK3 steps, stability
+// estimate and status.  No CPU fallback exists: without a CUDA device every
+// compute entry point returns THX_ERR_NO_DEVICE.
+#include "thx_launch.cuh"
+#include "thx_host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace thx;
+
+namespace {
+
+struct Layout {
+  long long jac_es = 0, jac_ns = 0, met_es = 0, met_ns = 0;
+  long long n_fs = 0, n_ps = 0, w_fs = 0, w_ps = 0;
+  long long sub_es[3] = {0, 0, 0};
+};
+
+// Pack a [outer][inner][block] array, dropping the outer and/or inner
+// dimension where every entry is bitwise equal along it.
+//   returns strides (outer stride, inner stride) in units of `block`.
+void pack_strided(const double *src, long long outer, long long inner, int block, bool full,
+                  std::vector<double> &dst, long long &os, long long &is) {
+  auto eqb = [&](long long a, long long b) {
+    return std::memcmp(src + a * block, src + b * block, sizeof(double) * block) == 0;
+  };
+  bool inner_const = !full, outer_same = !full;
+  if (!full) {
+    for (long long o = 0; o < outer && inner_const; ++o)
+      for (long long i = 1; i < inner; ++i)
+        if (!eqb(o * inner + i, o * inner)) { inner_const = false; break; }
+    for (long long o = 1; o < outer && outer_same; ++o)
+      if (std::memcmp(src + o * inner * block, src, sizeof(double) * inner * block) != 0) outer_same = false;
+  }
+  if (outer_same && inner_const) {
+    dst.assign(src, src + block);
+    os = 0; is = 0;
+  } else if (outer_same) {
+    dst.assign(src, src + inner * block);
+    os = 0; is = block;
+  } else if (inner_const) {
+    dst.resize(outer * block);
+    for (long long o = 0; o < outer; ++o) std::memcpy(dst.data() + o * block, src + o * inner * block, sizeof(double) * block);
+    os = block; is = 0;
+  } else {
+    dst.assign(src, src + outer * inner * block);
+    os = inner * block; is = block;
+  }
+}
+
+template <typename R>
+GasT<R> make_gas(const thx_config &c) {
+  GasT<R> g;
+  const double gm1 = c.gamma - 1.0;
+  const double gm1_inv = 1.0 / gm1;
+  const double cp = (c.gamma * gm1_inv) * c.R_gas;
+  g.gamma = (R)c.gamma;
+  g.gm1 = (R)gm1;
+  g.gm1_inv = (R)gm1_inv;
+  g.R_gas = (R)c.R_gas;
+  g.cp = (R)cp;
+  g.Pr_inv = (R)(1.0 / c.Pr);
+  g.mu = (R)c.mu;
+  g.mu0 = (R)c.mu0;
+  g.mu_bulk = (R)c.mu_bulk;
+  g.T0 = (R)c.T0;
+  g.Ts = (R)c.Ts;
+  g.gm1_av_inv = (R)(2.0 / (c.gamma + c.gamma - 2.0));
+  g.inv_gm1 = (R)(1.0 / (c.gamma - 1.0));
+  g.cv = (R)(cp / c.gamma);
+  g.sutherland = c.sutherland;
+  return g;
+}
+
+template <typename T>
+int dev_alloc(T **p, size_t n, std::vector<void *> &track) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return THX_ERR_OUT_OF_MEMORY;
+  }
+  track.push_back(*p);
+  return THX_OK;
+}
+
+template <typename T>
+int upload(T **p, const T *src, size_t n, std::vector<void *> &track) {
+  int st = dev_alloc(p, n, track);
+  if (st) return st;
+  if (cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return THX_ERR_CUDA;
+  return THX_OK;
+}
+
+int upload_both(const std::vector<double> &h, double **d64, float **d32, bool want32,
+                std::vector<void *> &track) {
+  int st = upload(d64, h.data(), h.size(), track);
+  if (st) return st;
+  if (want32) {
+    std::vector<float> f(h.begin(), h.end());
+    st = upload(d32, f.data(), f.size(), track);
+  } else {
+    *d32 = nullptr;
+  }
+  return st;
+}
+
+}  // namespace
+
+namespace thx {
+__global__ void convert_f64_f32(long long n, const double *src, float *dst) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    dst[i] = (float)src[i];
+}
+}  // namespace thx
+
+struct thx_operator_s {
+  int device = 0;
+  thx_config cfg{};
+  int dim = 0, order = 0, N = 0, nd = 0, nfp = 0, neq = 0, ne = 0, nf = 0;
+  long long L = 0;
+  bool mixed = false, ns = false, blend = false;
+  Layout lay;
+  double *jac64 = nullptr, *met64 = nullptr, *nrm64 = nullptr, *wm64 = nullptr, *wp64 = nullptr;
+  double *sub64[3] = {nullptr, nullptr, nullptr}, *ops64 = nullptr, *D64 = nullptr;
+  float *jac32 = nullptr, *met32 = nullptr, *nrm32 = nullptr, *wm32 = nullptr, *wp32 = nullptr;
+  float *sub32[3] = {nullptr, nullptr, nullptr}, *ops32 = nullptr, *D32 = nullptr;
+  int *face_elem = nullptr, *face_lface = nullptr, *elem_face = nullptr;
+  void *fstar = nullptr, *grad = nullptr;
+  double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
+  unsigned *status = nullptr;
+  unsigned long long *stab = nullptr;
+  double *y = nullptr;
+  float *yf = nullptr;
+  VolLaunch<double> vol64 = nullptr;
+  GradLaunch<double> grad64 = nullptr;
+  BlendLaunch<double> blend64 = nullptr;
+  FaceLaunch<double> face64 = nullptr;
+  VolLaunch<float> vol32 = nullptr;
+  GradLaunch<float> grad32 = nullptr;
+  BlendLaunch<float> blend32 = nullptr;
+  FaceLaunch<float> face32 = nullptr;
+  GasT<double> g64;
+  GasT<float> g32;
+  double threshold = 0.0;
+  double adv_scale = 0.0, dif_scale = 0.0, surf_scale = 0.0;
+  std::vector<void *> allocs;
+  std::string desc;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) { prev = -1; ok = false; cudaGetLastError(); return; }
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) { ok = false; cudaGetLastError(); }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+bool pick_order_kernels(thx_operator_s *h, int vk) {
+  const bool ns = h->ns;
+#define THX_PICK(P, D, NN)                                                  \
+  if (h->dim == D && h->N == NN) {                                          \
+    auto k = order_kernels_##P##_##D##_##NN();                              \
+    if (P == 0) {                                                           \
+      h->vol64 = reinterpret_cast<VolLaunch<double>>(k.vol[vk][ns ? 1 : 0]); \
+      h->grad64 = reinterpret_cast<GradLaunch<double>>(k.grad);             \
+      h->blend64 = reinterpret_cast<BlendLaunch<double>>(k.blend);          \
+    } else {                                                                \
+      h->vol32 = reinterpret_cast<VolLaunch<float>>(k.vol[vk][ns ? 1 : 0]); \
+      h->grad32 = reinterpret_cast<GradLaunch<float>>(k.grad);              \
+      h->blend32 = reinterpret_cast<BlendLaunch<float>>(k.blend);           \
+    }                                                                       \
+    return true;                                                            \
+  }
+  if (!h->mixed) {
+    THX_FOR_ORDERS(THX_PICK, 0, 2)
+    THX_FOR_ORDERS(THX_PICK, 0, 3)
+  } else {
+    THX_FOR_ORDERS(THX_PICK, 1, 2)
+    THX_FOR_ORDERS(THX_PICK, 1, 3)
+  }
+#undef THX_PICK
+  return false;
+}
+
+void pick_face_kernels(thx_operator_s *h) {
+  const int s = h->cfg.surface_flux, ns = h->ns ? 1 : 0;
+  if (!h->mixed) {
+    FaceKernels0 k = h->dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
+    h->face64 = k.face[s][ns];
+  } else {
+    FaceKernels1 k = h->dim == 2 ? face_kernels_1_2() : face_kernels_1_3();
+    h->face32 = k.face[s][ns];
+  }
+}
+
+void free_all(thx_operator_s *h) {
+  for (void *p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+}
+
+// Subcell-FV metrics of one element (include/dgsem_cache_utilities.hpp:641-763),
+// node-indexed as in the reference; D row-major [l*N+m].
+void subcell_element(int dim, int N, const double *metric_el, const double *D, const double *w,
+                     double *xi, double *eta, double *zeta) {
+  const int Nx = N, Ny = N, Nz = dim > 2 ? N : 1;
+  const int nxi = (Nx + 1) * Ny * Nz, neta = Nx * (Ny + 1) * Nz, nzeta = Nx * Ny * (Nz + 1);
+  std::memset(xi, 0, sizeof(double) * nxi * dim);
+  if (eta) std::memset(eta, 0, sizeof(double) * neta * dim);
+  if (zeta) std::memset(zeta, 0, sizeof(double) * nzeta * dim);
+  auto M = [&](int node, int row, int d) { return metric_el[(node * dim + row) * dim + d]; };
+  for (int k = 0; k < Nz; ++k)
+    for (int j = 0; j < Ny; ++j)
+      for (int i = 1; i < Nx; ++i)
+        for (int d = 0; d < dim; ++d) {
+          const int line = k * Ny * Nx + j * Nx;
+          double nrm = M(line, 0, d);
+          for (int l = 0; l < i; ++l) {
+            double sum = 0.0;
+            for (int m = 0; m < Nx; ++m) sum += M(line + m, 0, d) * D[l * Nx + m];
+            sum *= w[l];
+            nrm += sum;
+          }
+          xi[(line + i) * dim + d] = nrm;
+        }
+  if (dim > 1 && eta)
+    for (int k = 0; k < Nz; ++k)
+      for (int i = 0; i < Nx; ++i)
+        for (int j = 1; j < Ny; ++j)
+          for (int d = 0; d < dim; ++d) {
+            const int line = k * Ny * Nx + i;
+            double nrm = M(line, 1, d);
+            for (int l = 0; l < j; ++l) {
+              double sum = 0.0;
+              for (int m = 0; m < Ny; ++m) sum += M(line + m * Nx, 1, d) * D[l * Nx + m];
+              sum *= w[l];
+              nrm += sum;
+            }
+            eta[(k * Ny * Nx + j * Nx + i) * dim + d] = nrm;
+          }
+  if (dim > 2 && zeta)
+    for (int j = 0; j < Ny; ++j)
+      for (int i = 0; i < Nx; ++i)
+        for (int k = 1; k < Nz; ++k)
+          for (int d = 0; d < dim; ++d) {
+            const int line = j * Nx + i;
+            double nrm = M(line, 2, d);
+            for (int l = 0; l < k; ++l) {
+              double sum = 0.0;
+              for (int m = 0; m < Nz; ++m) sum += M(line + m * Ny * Nx, 2, d) * D[l * Nx + m];
+              sum *= w[l];
+              nrm += sum;
+            }
+            zeta[(k * Ny * Nx + line) * dim + d] = nrm;
+          }
+}
+
+int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h) {
+  h->cfg = *cfg;
+  h->dim = g->dim;
+  h->order = g->order;
+  h->N = g->order + 1;
+  h->nd = g->dim == 2 ? h->N * h->N : h->N * h->N * h->N;
+  h->nfp = g->dim == 2 ? h->N : h->N * h->N;
+  h->neq = g->dim + 2;
+  h->ne = g->num_elements;
+  h->nf = g->num_faces;
+  h->L = (long long)h->ne * h->nd;
+  h->mixed = cfg->precision == THX_PRECISION_FP32_MIXED;
+  h->ns = cfg->flow_model == THX_FLOW_NAVIER_STOKES;
+  h->blend = cfg->blending != 0;
+  h->g64 = make_gas<double>(*cfg);
+  h->g32 = make_gas<float>(*cfg);
+  const int vk = (cfg->volume_flux == THX_FLUX_CHANDRASHEKAR) ? VOL_CHANDRASHEKAR
+               : (cfg->volume_flux == THX_FLUX_RANOCHA)     ? VOL_RANOCHA
+               : (cfg->volume_flux == THX_FLUX_PIROZZOLI)   ? VOL_PIROZZOLI
+                                                            : VOL_CENTRAL;
+  if (!pick_order_kernels(h, vk)) return THX_ERR_UNSUPPORTED;
+  pick_face_kernels(h);
+  const bool full = cfg->geometry_layout == 1;
+  const int dim = h->dim, N = h->N, nd = h->nd, nfp = h->nfp, MB = dim * dim;
+  const bool w32 = h->mixed;
+  auto &A = h->allocs;
+  int st;
+  // geometry
+  std::vector<double> tmp;
+  pack_strided(g->jac, h->ne, nd, 1, full, tmp, h->lay.jac_es, h->lay.jac_ns);
+  if ((st = upload_both(tmp, &h->jac64, &h->jac32, w32, A))) return st;
+  pack_strided(g->metric, h->ne, nd, MB, full, tmp, h->lay.met_es, h->lay.met_ns);
+  if ((st = upload_both(tmp, &h->met64, &h->met32, w32, A))) return st;
+  pack_strided(g->face_normal, h->nf, nfp, dim, full, tmp, h->lay.n_fs, h->lay.n_ps);
+  // normals are indexed as (f*n_fs + fp*n_ps)*DIM: convert block strides to point units
+  h->lay.n_fs /= dim;
+  h->lay.n_ps /= dim;
+  if ((st = upload_both(tmp, &h->nrm64, &h->nrm32, w32, A))) return st;
+  {
+    // lift weights share one layout
+    std::vector<double> both((size_t)h->nf * nfp * 2);
+    for (long long i = 0; i < (long long)h->nf * nfp; ++i) {
+      both[2 * i] = g->face_wminus[i];
+      both[2 * i + 1] = g->face_wplus[i];
+    }
+    long long fs, ps;
+    pack_strided(both.data(), h->nf, nfp, 2, full, tmp, fs, ps);
+    h->lay.w_fs = fs / 2;
+    h->lay.w_ps = ps / 2;
+    std::vector<double> wm(tmp.size() / 2), wp(tmp.size() / 2);
+    for (size_t i = 0; i < wm.size(); ++i) { wm[i] = tmp[2 * i]; wp[i] = tmp[2 * i + 1]; }
+    if ((st = upload_both(wm, &h->wm64, &h->wm32, w32, A))) return st;
+    if ((st = upload_both(wp, &h->wp64, &h->wp32, w32, A))) return st;
+  }
+  // connectivity
+  if ((st = upload(&h->face_elem, g->face_elem, (size_t)2 * h->nf, A))) return st;
+  if ((st = upload(&h->face_lface, g->face_lface, (size_t)2 * h->nf, A))) return st;
+  {
+    std::vector<int> ef((size_t)h->ne * 2 * dim, -1);
+    for (int f = 0; f < h->nf; ++f)
+      for (int s = 0; s < 2; ++s) {
+        const int e = g->face_elem[2 * f + s], lf = g->face_lface[2 * f + s];
+        if (e < 0 || e >= h->ne || lf < 0 || lf >= 2 * dim) return THX_ERR_INVALID_ARGUMENT;
+        ef[(size_t)e * 2 * dim + lf] = 2 * f + s;
+      }
+    if ((st = upload(&h->elem_face, ef.data(), ef.size(), A))) return st;
+  }
+  // operators
+  std::vector<double> x(N), w(N), D(N * N), Dh(N * N), Dh2(N * N);
+  lgl_rule(N, x.data(), w.data());
+  derivative_operators(N, x.data(), w.data(), D.data(), Dh.data(), Dh2.data());
+  {
+    std::vector<double> ops(2 * N * N + N);
+    std::memcpy(ops.data(), Dh2.data(), sizeof(double) * N * N);
+    std::memcpy(ops.data() + N * N, Dh.data(), sizeof(double) * N * N);
+    std::memcpy(ops.data() + 2 * N * N, w.data(), sizeof(double) * N);
+    if ((st = upload_both(ops, &h->ops64, &h->ops32, w32, A))) return st;
+    if ((st = upload_both(D, &h->D64, &h->D32, w32, A))) return st;
+  }
+  // scratch
+  const size_t fsz = (size_t)h->nf * h->neq * nfp;
+  if (h->mixed) {
+    float *p;
+    if ((st = dev_alloc(&p, fsz, A))) return st;
+    h->fstar = p;
+    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * h->neq * h->L, A))) return st; h->grad = p; }
+  } else {
+    double *p;
+    if ((st = dev_alloc(&p, fsz, A))) return st;
+    h->fstar = p;
+    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * h->neq * h->L, A))) return st; h->grad = p; }
+  }
+  if ((st = dev_alloc(&h->status, 1, A))) return st;
+  if ((st = dev_alloc(&h->stab, 3, A))) return st;
+  if (cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess) return THX_ERR_CUDA;
+  if ((st = dev_alloc(&h->alpha, h->ne, A))) return st;
+  if ((st = dev_alloc(&h->eta, h->ne, A))) return st;
+  if (cudaMemset(h->alpha, 0, sizeof(double) * h->ne) != cudaSuccess) return THX_ERR_CUDA;
+  if (cudaMemset(h->eta, 0, sizeof(double) * h->ne) != cudaSuccess) return THX_ERR_CUDA;
+  // blending: modal transform and subcell metrics
+  h->threshold = cfg->modal_threshold > 0 ? cfg->modal_threshold
+                                          : 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->order, 0.25));
+  if (h->blend) {
+    std::vector<double> vinv(N * N);
+    if (!legendre_vinv(N, x.data(), vinv.data())) return THX_ERR_NUMERICS;
+    if ((st = upload(&h->vinv, vinv.data(), vinv.size(), A))) return st;
+    const int Nz = dim > 2 ? N : 1;
+    const long long nsub[3] = {(long long)(N + 1) * N * Nz * dim, (long long)N * (N + 1) * Nz * dim,
+                               (long long)N * N * (N + 1) * dim};
+    const bool shared = h->lay.met_es == 0;
+    const long long nel = shared ? 1 : h->ne;
+    std::vector<double> xi(nsub[0] * nel), et(nsub[1] * nel), ze(dim > 2 ? nsub[2] * nel : 1);
+    std::vector<double> mel((size_t)nd * MB);
+    for (long long e = 0; e < nel; ++e) {
+      for (int a = 0; a < nd; ++a)
+        std::memcpy(mel.data() + (size_t)a * MB, g->metric + ((size_t)e * nd + a) * MB, sizeof(double) * MB);
+      subcell_element(dim, N, mel.data(), D.data(), w.data(), xi.data() + e * nsub[0],
+                      et.data() + e * nsub[1], dim > 2 ? ze.data() + e * nsub[2] : nullptr);
+    }
+    for (int d = 0; d < 3; ++d) h->lay.sub_es[d] = shared ? 0 : nsub[d];
+    if ((st = upload_both(xi, &h->sub64[0], &h->sub32[0], w32, A))) return st;
+    if ((st = upload_both(et, &h->sub64[1], &h->sub32[1], w32, A))) return st;
+    if (dim > 2 && (st = upload_both(ze, &h->sub64[2], &h->sub32[2], w32, A))) return st;
+  }
+  // stability scales (include/StabilityEstimate.hpp:61-92)
+  {
+    static const double adv_cal[] = {0.0, 2.19706891727, 5.41995189335, 9.64849524786,
+                                     14.7297419321, 20.5984751391, 27.2141622680, 34.5459214016,
+                                     42.5691944324, 51.2637780299, 60.6126232210, 70.6010566044,
+                                     81.2162499718};
+    static const double dif_cal[] = {0.0, 4.0, 25.5969429388, 82.9000427145, 203.470468982,
+                                     426.230394541, 799.733889878, 1383.0975821, 2244.38177282,
+                                     3461.2550528, 5121.29136549, 7321.77632194, 10169.7148876};
+    const int p = h->order;
+    h->adv_scale = (p > 0 && p < 13) ? 1.05 * adv_cal[p] : 0.65 * (p + 1) * (p + 1);
+    h->dif_scale = (p > 0 && p < 13) ? 1.25 * dif_cal[p] : 0.5 * std::pow(p + 1.0, 4);
+    h->surf_scale = h->adv_scale / (1.0 / w[0]);
+  }
+  // kernel attributes (dynamic shared memory)
+  cudaError_t ce;
+  if (h->mixed) {
+    VolArgs<float> va{};
+    GradArgs<float> ga{};
+    ce = h->vol32(va, 0, 1);
+    if (ce == cudaSuccess && h->ns) ce = h->grad32(ga, 0, 1);
+  } else {
+    VolArgs<double> va{};
+    GradArgs<double> ga{};
+    ce = h->vol64(va, 0, 1);
+    if (ce == cudaSuccess && h->ns) ce = h->grad64(ga, 0, 1);
+  }
+  if (ce != cudaSuccess) { cudaGetLastError(); return THX_ERR_CUDA; }
+  char buf[512];
+  std::snprintf(buf, sizeof(buf),
+                "dim=%d p=%d ne=%d nf=%d flow=%s vol=%d surf=%d fv=%d blend=%d prec=%s "
+                "layout jac(%lld,%lld) met(%lld,%lld) nrm(%lld,%lld) w(%lld,%lld) sub(%lld)",
+                dim, h->order, h->ne, h->nf, h->ns ? "ns" : "euler", cfg->volume_flux,
+                cfg->surface_flux, cfg->fv_flux, cfg->blending, h->mixed ? "fp32-mixed" : "fp64",
+                h->lay.jac_es, h->lay.jac_ns, h->lay.met_es, h->lay.met_ns, h->lay.n_fs, h->lay.n_ps,
+                h->lay.w_fs, h->lay.w_ps, h->lay.sub_es[0]);
+  h->desc = buf;
+  return THX_OK;
+}
+
+template <typename R>
+struct Geo {
+  const R *jac, *met, *nrm, *wm, *wp, *sub[3], *ops, *D;
+};
+Geo<double> geo(thx_operator_s *h, double *) {
+  return {h->jac64, h->met64, h->nrm64, h->wm64, h->wp64, {h->sub64[0], h->sub64[1], h->sub64[2]}, h->ops64, h->D64};
+}
+Geo<float> geo(thx_operator_s *h, float *) {
+  return {h->jac32, h->met32, h->nrm32, h->wm32, h->wp32, {h->sub32[0], h->sub32[1], h->sub32[2]}, h->ops32, h->D32};
+}
+VolLaunch<double> volk(thx_operator_s *h, double *) { return h->vol64; }
+VolLaunch<float> volk(thx_operator_s *h, float *) { return h->vol32; }
+GradLaunch<double> gradk(thx_operator_s *h, double *) { return h->grad64; }
+GradLaunch<float> gradk(thx_operator_s *h, float *) { return h->grad32; }
+BlendLaunch<double> blendk(thx_operator_s *h, double *) { return h->blend64; }
+BlendLaunch<float> blendk(thx_operator_s *h, float *) { return h->blend32; }
+FaceLaunch<double> facek(thx_operator_s *h, double *) { return h->face64; }
+FaceLaunch<float> facek(thx_operator_s *h, float *) { return h->face32; }
+const GasT<double> &gas(thx_operator_s *h, double *) { return h->g64; }
+const GasT<float> &gas(thx_operator_s *h, float *) { return h->g32; }
+
+// One right-hand side: [indicator] [gradient] face fluxes, volume+lift.
+// stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
+template <typename R>
+int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
+            double *um, double *y, float *yf, cudaEvent_t *ev = nullptr) {
+  R *tag = nullptr;
+  if (ev) cudaEventRecord(ev[0], s);
+  const Geo<R> G = geo(h, tag);
+  const GasT<R> &g = gas(h, tag);
+  cudaError_t ce;
+  if (h->blend) {
+    BlendArgs<R> b;
+    b.u = u; b.ne = h->ne; b.vinv = h->vinv; b.gas = g;
+    b.threshold = h->threshold; b.sharpness = h->cfg.sharpness;
+    b.alpha_min = h->cfg.alpha_min; b.alpha_max = h->cfg.alpha_max;
+    b.alpha = h->alpha; b.eta = h->eta;
+    if ((ce = blendk(h, tag)(b, s)) != cudaSuccess) return THX_ERR_CUDA;
+  }
+  if (ev) cudaEventRecord(ev[1], s);
+  R *gradp = reinterpret_cast<R *>(h->grad);
+  if (h->ns) {
+    GradArgs<R> a;
+    a.u = u; a.grad = gradp; a.ne = h->ne;
+    a.jac = G.jac; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
+    a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
+    a.elem_face = h->elem_face; a.face_elem = h->face_elem; a.face_lface = h->face_lface;
+    a.normal = G.nrm; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
+    a.wm = G.wm; a.wp = G.wp; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
+    a.D = G.D; a.gas = g;
+    if ((ce = gradk(h, tag)(a, s, 0)) != cudaSuccess) return THX_ERR_CUDA;
+  }
+  if (ev) cudaEventRecord(ev[2], s);
+  R *fst = reinterpret_cast<R *>(h->fstar);
+  {
+    FaceArgs<R> a;
+    a.u = u; a.ne = h->ne; a.nf = h->nf; a.N = h->N;
+    a.face_elem = h->face_elem; a.face_lface = h->face_lface;
+    a.normal = G.nrm; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
+    a.grad = gradp; a.fstar = fst; a.gas = g;
+    if ((ce = facek(h, tag)(a, s)) != cudaSuccess) return THX_ERR_CUDA;
+  }
+  if (ev) cudaEventRecord(ev[3], s);
+  {
+    VolArgs<R> a;
+    a.u = u; a.du = du; a.ne = h->ne;
+    a.jac = G.jac; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
+    a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
+    a.elem_face = h->elem_face; a.fstar = fst;
+    a.wm = G.wm; a.wp = G.wp; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
+    a.grad = gradp;
+    a.alpha = h->blend ? h->alpha : nullptr;
+    for (int d = 0; d < 3; ++d) { a.sub[d] = G.sub[d]; a.sub_es[d] = h->lay.sub_es[d]; }
+    a.fv_flux = h->cfg.fv_flux;
+    a.gas = g;
+    a.ops = G.ops;
+    a.stage = stage; a.dt = dt; a.um = um; a.y = y; a.yf = yf;
+    a.status = h->status;
+    if ((ce = volk(h, tag)(a, s, 0)) != cudaSuccess) return THX_ERR_CUDA;
+  }
+  if (ev) cudaEventRecord(ev[4], s);
+  return THX_OK;
+}
+
+int check_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return THX_ERR_NO_DEVICE;
+  }
+  return THX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *thx_version(void) { return "theseus-b200 0.1 (sm_100a)"; }
+
+const char *thx_status_string(int status) {
+  switch (status) {
+    case THX_OK: return "ok";
+    case THX_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case THX_ERR_UNSUPPORTED: return "unsupported configuration";
+    case THX_ERR_CUDA: return "CUDA runtime error";
+    case THX_ERR_NO_DEVICE: return "no CUDA device (no CPU fallback exists)";
+    case THX_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case THX_ERR_NUMERICS: return "numerical status flag set";
+  }
+  return "unknown status";
+}
+
+void thx_config_default(thx_config *c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->flow_model = THX_FLOW_EULER;
+  c->volume_flux = THX_FLUX_CHANDRASHEKAR;
+  c->surface_flux = THX_FLUX_CHANDRASHEKAR;
+  c->fv_flux = THX_FLUX_LLF;
+  c->precision = THX_PRECISION_FP64;
+  c->gamma = 1.4;
+  c->Pr = 0.72;
+  c->R_gas = 287.05;
+  c->mu = 0.02;
+  c->mu0 = 1.716e-5;
+  c->mu_bulk = 2.0 / 3.0;
+  c->T0 = 273.15;
+  c->Ts = 110.4;
+  c->alpha_max = 0.5;
+  c->alpha_min = 0.001;
+  c->sharpness = 9.21024;
+  c->modal_threshold = 0.0;
+}
+
+int thx_create(const thx_geometry *g, const thx_config *cfg, thx_handle *out) {
+  if (!g || !cfg || !out) return THX_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (g->dim < 2 || g->dim > 3 || g->order < 1 || g->num_elements <= 0 || g->num_faces < 0 ||
+      !g->jac || !g->metric || (g->num_faces > 0 && (!g->face_elem || !g->face_lface ||
+                                                     !g->face_normal || !g->face_wminus ||
+                                                     !g->face_wplus)))
+    return THX_ERR_INVALID_ARGUMENT;
+  if (cfg->volume_flux < 0 || cfg->volume_flux >= THX_FLUX_COUNT || cfg->surface_flux < 0 ||
+      cfg->surface_flux >= THX_FLUX_COUNT || cfg->fv_flux < 0 || cfg->fv_flux >= THX_FLUX_COUNT ||
+      (cfg->flow_model != THX_FLOW_EULER && cfg->flow_model != THX_FLOW_NAVIER_STOKES) ||
+      (cfg->precision != THX_PRECISION_FP64 && cfg->precision != THX_PRECISION_FP32_MIXED) ||
+      !(cfg->gamma > 1.0) || !(cfg->Pr > 0.0))
+    return THX_ERR_INVALID_ARGUMENT;
+  if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
+  int st = check_device();
+  if (st) return st;
+  thx_operator_s *h = new (std::nothrow) thx_operator_s();
+  if (!h) return THX_ERR_OUT_OF_MEMORY;
+  cudaGetDevice(&h->device);
+  try {
+    st = create_impl(g, cfg, h);
+  } catch (...) {
+    st = THX_ERR_OUT_OF_MEMORY;
+  }
+  if (st) {
+    free_all(h);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return THX_OK;
+}
+
+int thx_destroy(thx_handle h) {
+  if (!h) return THX_ERR_INVALID_ARGUMENT;
+  {
+    DeviceGuard dg(h->device);
+    free_all(h);
+  }
+  delete h;
+  return THX_OK;
+}
+
+int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream) {
+  if (!h || !u || !dudt) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->mixed)
+    return run_rhs<float>(h, (const float *)u, (float *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr);
+  return run_rhs<double>(h, (const double *)u, (double *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr);
+}
+
+int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream) {
+  if (!h || !u || nsteps < 0 || !std::isfinite(dt)) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = h->L * h->neq;
+  int st;
+  if (!h->y && (st = dev_alloc(&h->y, (size_t)n, h->allocs))) return st;
+  if (h->mixed && !h->yf && (st = dev_alloc(&h->yf, (size_t)n, h->allocs))) return st;
+  if (h->mixed) {
+    convert_f64_f32<<<(int)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, s>>>(n, u, h->yf);
+    if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
+  }
+  for (int step = 0; step < nsteps; ++step) {
+    if (h->mixed) {
+      for (int stage = 1; stage <= 3; ++stage)
+        if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, dt, u, h->y, h->yf))) return st;
+    } else {
+      if ((st = run_rhs<double>(h, u, nullptr, s, 1, dt, u, h->y, nullptr))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 2, dt, u, h->y, nullptr))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 3, dt, u, h->y, nullptr))) return st;
+    }
+  }
+  return THX_OK;
+}
+
+int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev, void *stream) {
+  if (!h) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (alpha_dev && cudaMemcpyAsync(alpha_dev, h->alpha, sizeof(double) * h->ne, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return THX_ERR_CUDA;
+  if (eta_dev && cudaMemcpyAsync(eta_dev, h->eta, sizeof(double) * h->ne, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return THX_ERR_CUDA;
+  return THX_OK;
+}
+
+int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, double *rates_out) {
+  if (!h || !u || !dt_out) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  StabArgs a;
+  a.u = u; a.ne = h->ne; a.N = h->N;
+  a.jac = h->jac64; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
+  a.met = h->met64; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
+  a.face_elem = h->face_elem; a.face_lface = h->face_lface; a.nf = h->nf;
+  a.normal = h->nrm64; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
+  a.wm = h->wm64; a.wp = h->wp64; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
+  a.gas = h->g64;
+  a.adv_scale = h->adv_scale; a.dif_scale = h->dif_scale; a.surf_scale = h->surf_scale;
+  a.viscous = h->ns ? 1 : 0;
+  a.out = h->stab;
+  if (cudaMemset(h->stab, 0, sizeof(unsigned long long) * 3) != cudaSuccess) return THX_ERR_CUDA;
+  const long long work = h->L + (long long)h->nf * h->nfp;
+  const int grid = (int)std::min<long long>((work + 255) / 256, 148LL * 8);
+  if (h->dim == 2) stability_kernel<2><<<grid, 256>>>(a);
+  else stability_kernel<3><<<grid, 256>>>(a);
+  if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
+  unsigned long long r[3];
+  if (cudaMemcpy(r, h->stab, sizeof(r), cudaMemcpyDeviceToHost) != cudaSuccess) return THX_ERR_CUDA;
+  double rates[3];
+  for (int i = 0; i < 3; ++i) std::memcpy(&rates[i], &r[i], sizeof(double));
+  if (rates_out) std::memcpy(rates_out, rates, sizeof(rates));
+  const double total = std::max(rates[0], rates[1]) + rates[2];
+  if (!(total > 0.0)) return THX_ERR_NUMERICS;
+  *dt_out = cfl / total;
+  return THX_OK;
+}
+
+int thx_read_status(thx_handle h, uint32_t *flags, void *stream) {
+  if (!h || !flags) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned v = 0;
+  if (cudaMemcpyAsync(&v, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess) return THX_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return THX_ERR_CUDA;
+  if (cudaMemsetAsync(h->status, 0, sizeof(unsigned), s) != cudaSuccess) return THX_ERR_CUDA;
+  *flags = v;
+  return THX_OK;
+}
+
+int thx_rhs_profile(thx_handle h, const void *u, void *dudt, void *stream, double *ms) {
+  if (!h || !u || !dudt || !ms) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t ev[5];
+  for (int i = 0; i < 5; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) return THX_ERR_CUDA;
+  int st = h->mixed ? run_rhs<float>(h, (const float *)u, (float *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr, ev)
+                    : run_rhs<double>(h, (const double *)u, (double *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr, ev);
+  if (st == THX_OK && cudaEventSynchronize(ev[4]) != cudaSuccess) st = THX_ERR_CUDA;
+  for (int i = 0; i < 4 && st == THX_OK; ++i) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ev[i], ev[i + 1]) != cudaSuccess) st = THX_ERR_CUDA;
+    ms[i] = t;
+  }
+  for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+  return st;
+}
+
+int thx_describe(thx_handle h, char *buf, size_t len) {
+  if (!h || !buf || len == 0) return THX_ERR_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", h->desc.c_str());
+  return THX_OK;
+}
+
+}  // extern "C"

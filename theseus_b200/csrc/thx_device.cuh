@@ -1,0 +1,611 @@
+// thx_device.cuh -- pointwise device arithmetic of the DGSEM right-hand side:
+// ideal-gas model, logarithmic mean, two-point volume fluxes, Riemann
+// (surface) fluxes and the Navier-Stokes viscous flux.  Templated on the
+// arithmetic type R (double for the FP64 path, float for the FP32-mixed path).
+//
+// Formulas follow the reference's device functions (paths relative to the
+// reference project root); the per-node quantities that the reference
+// recomputes inside every pair (velocity, pressure, beta) are computed once per
+// node by the caller and passed in as NodeP, with identical arithmetic.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace thx {
+
+constexpr int MAXEQ = 5;
+
+// include/Physics.hpp:22-35, include/Transport.hpp, include/EOS.hpp
+template <typename R>
+struct GasT {
+  R gamma, gm1, gm1_inv, R_gas, cp, Pr_inv, mu, mu0, mu_bulk, T0, Ts;
+  R gm1_av_inv;   // 2/(gamma+gamma-2): Chandrashekar's averaged 1/(gamma-1)
+  R inv_gm1;      // 1/(gamma-1)
+  R cv;           // cp/gamma
+  int sutherland;
+};
+
+template <typename R> __device__ __forceinline__ R rsqrt_(R x);
+template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rlog(double x) { return log(x); }
+__device__ __forceinline__ float rlog(float x) { return logf(x); }
+__device__ __forceinline__ double rexp(double x) { return exp(x); }
+__device__ __forceinline__ float rexp(float x) { return expf(x); }
+template <typename R> __device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
+template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+
+// include/theseus_kernels.hpp:106-123.  In FP32 the series branch (equal
+// arguments, where the closed form cancels) is evaluated in FP64.
+__device__ __forceinline__ double log_mean(double x, double y) {
+  const double xi = y / x;
+  const double u = (xi * (xi - 2.0) + 1.0) / (xi * (xi + 2.0) + 1.0);
+  if (u < 1e-4) {
+    const double denom = 105.0 + u * (35.0 + u * (21.0 + 15.0 * u));
+    return (x + y) * 52.5 / denom;
+  }
+  return (y - x) / log(xi);
+}
+__device__ __forceinline__ float log_mean(float x, float y) {
+  const float xi = y / x;
+  const float u = (xi * (xi - 2.0f) + 1.0f) / (xi * (xi + 2.0f) + 1.0f);
+  if (u < 1e-4f) {
+    const double xd = x, yd = y;
+    const double xid = yd / xd;
+    const double ud = (xid * (xid - 2.0) + 1.0) / (xid * (xid + 2.0) + 1.0);
+    const double denom = 105.0 + ud * (35.0 + ud * (21.0 + 15.0 * ud));
+    return (float)((xd + yd) * 52.5 / denom);
+  }
+  return (y - x) / logf(xi);
+}
+
+// ---- gas functions on a conserved state q[DIM+2] -------------------------
+template <typename R, int DIM>
+__device__ __forceinline__ R ke_density(const R *q) {
+  R m2 = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
+  return R(0.5) * m2 / q[0];
+}
+template <typename R, int DIM>
+__device__ __forceinline__ R pressure(const GasT<R> &g, const R *q) {
+  return g.gm1 * (q[DIM + 1] - ke_density<R, DIM>(q));
+}
+template <typename R, int DIM>
+__device__ __forceinline__ R sound_speed(const GasT<R> &g, const R *q) {
+  return rsqrt_(g.gamma * pressure<R, DIM>(g, q) / q[0]);
+}
+template <typename R, int DIM>
+__device__ __forceinline__ R viscosity(const GasT<R> &g, const R *q) {
+  if (g.sutherland) {
+    const R T = pressure<R, DIM>(g, q) / (q[0] * g.R_gas);
+    const R Trel = T / g.T0;
+    const R T0pTs = g.T0 + g.Ts;
+    return g.mu0 * T0pTs * Trel * rsqrt_(Trel) / (T + g.Ts);
+  }
+  return g.mu;
+}
+
+// Per-node data used by the volume kernel: density, velocity, pressure and one
+// flux-specific auxiliary (beta = rho/(2p) for Chandrashekar, specific
+// enthalpy e + p/rho for Pirozzoli, total enthalpy (rhoE+p)/rho for central).
+template <typename R, int DIM>
+struct NodeP {
+  R rho, v[DIM], p, aux;
+};
+
+enum VolKind { VOL_CHANDRASHEKAR = 0, VOL_RANOCHA = 1, VOL_PIROZZOLI = 2, VOL_CENTRAL = 3 };
+
+template <typename R, int DIM, int VOL>
+__device__ __forceinline__ void node_prims(const GasT<R> &g, const R *q, R *out /*[DIM+3]*/) {
+  const R rho = q[0];
+  R v[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) v[d] = q[1 + d] / rho;
+  const R ke = ke_density<R, DIM>(q);
+  const R p = g.gm1 * (q[DIM + 1] - ke);
+  out[0] = rho;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) out[1 + d] = v[d];
+  out[DIM + 1] = p;
+  if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = R(0.5) * rho / p;
+  else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = (q[DIM + 1] - ke) / rho + p / rho;
+  else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * (R(1) / rho);
+  else out[DIM + 2] = R(0);
+}
+
+// ---- two-point volume fluxes (metric rows already averaged) --------------
+// include/ChandrashekarFlux.hpp:20-89
+template <typename R, int DIM>
+__device__ __forceinline__ void vol_chandrashekar(const GasT<R> &g, const R *a, const R *b,
+                                                  const R *met, R *F) {
+  const R rho1 = a[0], rho2 = b[0];
+  const R rho_ln = log_mean(rho1, rho2);
+  R mom_hat[DIM];
+  R h_hat = R(0), vn = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const R v1 = a[1 + d], v2 = b[1 + d];
+    const R vbar = R(0.5) * (v1 + v2);
+    vn += vbar * met[d];
+    mom_hat[d] = rho_ln * vbar;
+    h_hat += -R(0.25) * (v1 * v1 + v2 * v2) + vbar * vbar;
+  }
+  const R beta1 = a[DIM + 2], beta2 = b[DIM + 2];
+  const R beta_ln = log_mean(beta1, beta2);
+  const R p_hat = R(0.5) * (rho1 + rho2) / (beta1 + beta2);
+  h_hat += R(0.5) / beta_ln * g.gm1_av_inv + p_hat / rho_ln;
+  F[0] = rho_ln * vn;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom_hat[d] + p_hat * met[d];
+  F[DIM + 1] = rho_ln * vn * h_hat;
+}
+
+// include/RanochaFlux.hpp:20-79
+template <typename R, int DIM>
+__device__ __forceinline__ void vol_ranocha(const GasT<R> &g, const R *a, const R *b,
+                                            const R *met, R *F) {
+  const R rho1 = a[0], rho2 = b[0];
+  const R rho_ln = log_mean(rho1, rho2);
+  const R p1 = a[DIM + 1], p2 = b[DIM + 1];
+  const R pbar = R(0.5) * (p1 + p2);
+  R vbar[DIM];
+  R ke = R(0), vn = R(0), fe = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const R v1 = a[1 + d], v2 = b[1 + d];
+    vbar[d] = R(0.5) * (v1 + v2);
+    vn += vbar[d] * met[d];
+    ke += R(0.5) * (v1 * v2);
+    fe += (R(0.5) * (p1 * v2 + p2 * v1)) * met[d];
+  }
+  const R inv_beta_ln = (p1 * p2) / log_mean(rho1 * p2, rho2 * p1);
+  const R ie = inv_beta_ln * g.inv_gm1;
+  F[0] = rho_ln * vn;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_ln * vn * vbar[d] + pbar * met[d];
+  F[DIM + 1] = fe + rho_ln * (ie + ke) * vn;
+}
+
+// include/PirozzoliFlux.hpp:19-71
+template <typename R, int DIM>
+__device__ __forceinline__ void vol_pirozzoli(const GasT<R> &g, const R *a, const R *b,
+                                              const R *met, R *F) {
+  const R rho_mean = R(0.5) * (a[0] + b[0]);
+  const R pbar = R(0.5) * (a[DIM + 1] + b[DIM + 1]);
+  R vbar[DIM];
+  R ke_mean = R(0), vn = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const R v1 = a[1 + d], v2 = b[1 + d];
+    vbar[d] = R(0.5) * (v1 + v2);
+    vn += vbar[d] * met[d];
+    ke_mean += R(0.25) * ((v1 * v1) + (v2 * v2));
+  }
+  const R h_mean = R(0.5) * (a[DIM + 2] + b[DIM + 2]);
+  F[0] = rho_mean * vn;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_mean * vn * vbar[d] + pbar * met[d];
+  F[DIM + 1] = rho_mean * (h_mean + ke_mean) * vn;
+}
+
+// Central flux of HLL/LLF/Roe (include/HLLFlux.hpp:21-51): average of the
+// physical Euler fluxes contracted with the averaged metric.  qa/qb are the
+// conserved states, a/b the node data (aux = total enthalpy H).
+template <typename R, int DIM>
+__device__ __forceinline__ void vol_central(const R *qa, const R *qb, const R *a, const R *b,
+                                            const R *met, R *F) {
+  const R ia = R(1) / a[0], ib = R(1) / b[0];
+  R acc0 = R(0), accE = R(0);
+  R accm[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) accm[i] = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    acc0 += R(0.5) * (qa[1 + d] + qb[1 + d]) * met[d];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) {
+      R fa = qa[1 + i] * qa[1 + d] * ia, fb = qb[1 + i] * qb[1 + d] * ib;
+      if (i == d) { fa += a[DIM + 1]; fb += b[DIM + 1]; }
+      accm[i] += R(0.5) * (fa + fb) * met[d];
+    }
+    accE += R(0.5) * (qa[1 + d] * a[DIM + 2] + qb[1 + d] * b[DIM + 2]) * met[d];
+  }
+  F[0] = acc0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) F[1 + i] = accm[i];
+  F[DIM + 1] = accE;
+}
+
+// ---- surface fluxes on conserved states ----------------------------------
+template <typename R, int DIM>
+struct NState { R inv_rho, p, H; };
+
+template <typename R, int DIM>
+__device__ __forceinline__ NState<R, DIM> nstate(const GasT<R> &g, const R *q) {
+  NState<R, DIM> s;
+  s.inv_rho = R(1) / q[0];
+  s.p = pressure<R, DIM>(g, q);
+  s.H = (q[DIM + 1] + s.p) * s.inv_rho;
+  return s;
+}
+// include/NavierStokesFlux.hpp:64-103
+template <typename R, int DIM>
+__device__ __forceinline__ R normal_flux(const R *q, const NState<R, DIM> &s, const R *n, int eq) {
+  R r = R(0);
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const R m = q[1 + dir];
+    R pf;
+    if (eq == 0) pf = m;
+    else if (eq <= DIM) {
+      const int c = eq - 1;
+      pf = q[1 + c] * m * s.inv_rho;
+      if (c == dir) pf += s.p;
+    } else pf = m * s.H;
+    r += pf * n[dir];
+  }
+  return r;
+}
+
+// include/DissipationOperator.hpp:57-172
+template <typename R, int DIM>
+__device__ __forceinline__ void roe_dissipation(const GasT<R> &g, const R *q1, const R *q2,
+                                                const R *n, R *diss) {
+  const int E = DIM + 1;
+  R vn1 = R(0), vn2 = R(0), vn_roe = R(0), nor_mag = R(0);
+  const R rho1 = q1[0], rho2 = q2[0];
+  const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+  const R H1 = (q1[E] + p1) / rho1, H2 = (q2[E] + p2) / rho2;
+  R roe[DIM + 2];
+  const R ratio = rsqrt_(rho2 / rho1);
+  const R a = R(1) / (ratio + R(1));
+  const R b = a * ratio;
+  roe[0] = ratio * rho1;
+  roe[E] = a * H1 + b * H2;
+  R del_mom[DIM];
+  R ke = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    nor_mag += n[d] * n[d];
+    const R v1 = q1[1 + d] / rho1, v2 = q2[1 + d] / rho2;
+    del_mom[d] = v2 - v1;
+    roe[1 + d] = a * v1 + b * v2;
+    ke += R(0.5) * roe[1 + d] * roe[1 + d];
+    vn1 += v1 * n[d];
+    vn2 += v2 * n[d];
+    vn_roe += roe[1 + d] * n[d];
+  }
+  nor_mag = rsqrt_(nor_mag);
+  const R inm = R(1) / nor_mag;
+  vn1 *= inm;
+  vn2 *= inm;
+  vn_roe *= inm;
+  const R c_roe = rsqrt_((g.gamma - R(1)) * (roe[E] - ke));
+  const R c1 = rsqrt_(g.gamma * p1 / rho1), c2 = rsqrt_(g.gamma * p2 / rho2);
+  R e0, e2;
+  {
+    const R er = vn_roe - c_roe;
+    const R eps = rmax(R(0), rmax(er - (vn1 - c1), (vn2 - c2) - er));
+    e0 = (rabs(er) < eps) ? R(0.5) * (eps + (er * er) / eps) : rabs(er);
+  }
+  {
+    const R er = vn_roe + c_roe;
+    const R eps = rmax(R(0), rmax(er - (vn1 + c1), (vn2 + c2) - er));
+    e2 = (rabs(er) < eps) ? R(0.5) * (eps + (er * er) / eps) : rabs(er);
+  }
+  const R e1 = rabs(vn_roe);
+  const R del_rho = rho2 - rho1;
+  const R del_vn = vn2 - vn1;
+  const R del_p = p2 - p1;
+  const R ov_csq = R(1) / (c_roe * c_roe);
+  const R pov_csq = del_p * ov_csq;
+  const R rhoc_del_vn = roe[0] * del_vn * c_roe * ov_csq;
+  const R aVn = e1 * (del_rho - pov_csq);
+  const R aVn_rho = e1 * roe[0];
+  const R aL = R(0.5) * (e0 * (pov_csq - rhoc_del_vn));
+  const R aR = R(0.5) * (e2 * (pov_csq + rhoc_del_vn));
+  diss[0] = R(0.5) * (aVn + aL + aR);
+  R de = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    R dm = R(0.5) * (aVn * roe[1 + d] + aVn_rho * (del_mom[d] - n[d] * inm * del_vn));
+    dm += R(0.5) * (aL * (roe[1 + d] - n[d] * inm * c_roe) + aR * (roe[1 + d] + n[d] * inm * c_roe));
+    diss[1 + d] = dm;
+    de += R(0.5) * aVn_rho * (roe[1 + d] * del_mom[d]);
+  }
+  de -= R(0.5) * aVn_rho * vn_roe * del_vn;
+  de += R(0.5) * aVn * ke + R(0.5) * aL * (roe[E] - vn_roe * c_roe) +
+        R(0.5) * aR * (roe[E] + vn_roe * c_roe);
+  diss[E] = de;
+#pragma unroll
+  for (int e = 0; e < DIM + 2; ++e) diss[e] *= nor_mag;
+}
+
+// include/DissipationOperator.hpp:174-232
+template <typename R, int DIM>
+__device__ __forceinline__ void scalar_dissipation(const GasT<R> &g, const R *q1, const R *q2,
+                                                   const R *n, R *diss) {
+  const int E = DIM + 1;
+  const R rho1 = q1[0], rho2 = q2[0];
+  const R rho_mean = R(0.5) * (rho1 + rho2);
+  const R drho = rho2 - rho1;
+  const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+  R vn1 = R(0), vn2 = R(0), nor_mag = R(0), de = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    nor_mag += n[d] * n[d];
+    const R v1 = q1[1 + d] / rho1, v2 = q2[1 + d] / rho2;
+    const R dv = v2 - v1;
+    const R vbar = R(0.5) * (v1 + v2);
+    vn1 += v1 * n[d];
+    vn2 += v2 * n[d];
+    de += R(0.5) * drho * v1 * v2 + rho_mean * dv * vbar;
+  }
+  nor_mag = rsqrt_(nor_mag);
+  const R lmax = rmax(rabs(vn1) + rsqrt_(g.gamma * p1 / rho1) * nor_mag,
+                      rabs(vn2) + rsqrt_(g.gamma * p2 / rho2) * nor_mag);
+  const R beta1 = R(0.5) * rho1 / p1, beta2 = R(0.5) * rho2 / p2;
+  const R beta_ln = log_mean(beta1, beta2);
+  de += R(0.5) * drho * g.inv_gm1 / beta_ln + R(0.5) * rho_mean * g.inv_gm1 * (R(1) / beta2 - R(1) / beta1);
+  diss[0] = R(0.5) * lmax * drho;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) diss[1 + d] = R(0.5) * lmax * (q2[1 + d] - q1[1 + d]);
+  diss[E] = de * (R(0.5) * lmax);
+}
+
+enum SurfKind { SURF_CHANDRASHEKAR = 0, SURF_RANOCHA = 1, SURF_PIROZZOLI = 2, SURF_HLL = 3,
+                SURF_LLF = 4, SURF_ROE = 5 };
+
+template <typename R, int DIM, int SURF>
+__device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, const R *q2,
+                                             const R *n, R *F) {
+  constexpr int E = DIM + 1;
+  if (SURF == SURF_CHANDRASHEKAR) {
+    // include/ChandrashekarFlux.hpp:91-155
+    const R rho1 = q1[0], rho2 = q2[0];
+    const R rho_ln = log_mean(rho1, rho2);
+    R mom[DIM];
+    R hhat = R(0), vn = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const R v1 = q1[1 + d] / rho1, v2 = q2[1 + d] / rho2;
+      const R vbar = R(0.5) * (v1 + v2);
+      vn += vbar * n[d];
+      mom[d] = rho_ln * vbar;
+      hhat += -R(0.25) * (v1 * v1 + v2 * v2) + vbar * vbar;
+    }
+    const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+    const R beta1 = R(0.5) * rho1 / p1, beta2 = R(0.5) * rho2 / p2;
+    const R beta_ln = log_mean(beta1, beta2);
+    const R p_hat = R(0.5) * (rho1 + rho2) / (beta1 + beta2);
+    hhat += R(0.5) / beta_ln * g.gm1_av_inv + p_hat / rho_ln;
+    R diss[DIM + 2];
+    scalar_dissipation<R, DIM>(g, q1, q2, n, diss);
+    F[0] = rho_ln * vn - diss[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom[d] + p_hat * n[d] - diss[1 + d];
+    F[E] = rho_ln * vn * hhat - diss[E];
+  } else if (SURF == SURF_RANOCHA) {
+    // include/RanochaFlux.hpp:81-134
+    const R rho1 = q1[0], rho2 = q2[0];
+    const R rho_ln = log_mean(rho1, rho2);
+    const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+    const R pbar = R(0.5) * (p1 + p2);
+    R vbar[DIM];
+    R ke = R(0), vn = R(0), fe = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const R v1 = q1[1 + d] / rho1, v2 = q2[1 + d] / rho2;
+      vbar[d] = R(0.5) * (v1 + v2);
+      vn += vbar[d] * n[d];
+      ke += R(0.5) * (v1 * v2);
+      fe += (R(0.5) * (p1 * v2 + p2 * v1)) * n[d];
+    }
+    const R inv_beta_ln = (p1 * p2) / log_mean(rho1 * p2, rho2 * p1);
+    const R ie = inv_beta_ln * g.inv_gm1;
+    R diss[DIM + 2];
+    roe_dissipation<R, DIM>(g, q1, q2, n, diss);
+    F[0] = rho_ln * vn - diss[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[1 + d] = rho_ln * vn * vbar[d] + pbar * n[d] - diss[1 + d];
+    F[E] = fe + (rho_ln * (ie + ke) * vn - diss[E]);
+  } else if (SURF == SURF_PIROZZOLI) {
+    // include/PirozzoliFlux.hpp:73-120
+    const R rho1 = q1[0], rho2 = q2[0];
+    const R rho_mean = R(0.5) * (rho1 + rho2);
+    const R ke1 = ke_density<R, DIM>(q1), ke2 = ke_density<R, DIM>(q2);
+    const R p1 = g.gm1 * (q1[E] - ke1), p2 = g.gm1 * (q2[E] - ke2);
+    const R pbar = R(0.5) * (p1 + p2);
+    R vbar[DIM];
+    R ke_mean = R(0), vn = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const R v1 = q1[1 + d] / rho1, v2 = q2[1 + d] / rho2;
+      vbar[d] = R(0.5) * (v1 + v2);
+      vn += vbar[d] * n[d];
+      ke_mean += R(0.25) * ((v1 * v1) + (v2 * v2));
+    }
+    const R h_mean = R(0.5) * ((q1[E] - ke1) / rho1 + p1 / rho1 + (q2[E] - ke2) / rho2 + p2 / rho2);
+    R diss[DIM + 2];
+    roe_dissipation<R, DIM>(g, q1, q2, n, diss);
+    F[0] = rho_mean * vn - diss[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[1 + d] = rho_mean * vn * vbar[d] + pbar * n[d] - diss[1 + d];
+    F[E] = rho_mean * (h_mean + ke_mean) * vn - diss[E];
+  } else if (SURF == SURF_HLL) {
+    // include/HLLFlux.hpp:53-116
+    const NState<R, DIM> L = nstate<R, DIM>(g, q1), Rs = nstate<R, DIM>(g, q2);
+    R un1 = R(0), un2 = R(0), nn = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      un1 += (q1[1 + d] / q1[0]) * n[d];
+      un2 += (q2[1 + d] / q2[0]) * n[d];
+      nn += n[d] * n[d];
+    }
+    const R nm = rsqrt_(nn);
+    const R c1 = rsqrt_(g.gamma * L.p / q1[0]) * nm, c2 = rsqrt_(g.gamma * Rs.p / q2[0]) * nm;
+    const R sL1 = un1 - c1, sL2 = un2 - c2, sR1 = un1 + c1, sR2 = un2 + c2;
+    const R sL = (sL1 < sL2) ? sL1 : sL2;
+    const R sR = (sR1 > sR2) ? sR1 : sR2;
+#pragma unroll
+    for (int e = 0; e < DIM + 2; ++e) {
+      const R fn1 = normal_flux<R, DIM>(q1, L, n, e), fn2 = normal_flux<R, DIM>(q2, Rs, n, e);
+      if (sL >= R(0)) F[e] = fn1;
+      else if (sR <= R(0)) F[e] = fn2;
+      else F[e] = (sR * fn1 - sL * fn2 + sL * sR * (q2[e] - q1[e])) / (sR - sL);
+    }
+  } else if (SURF == SURF_LLF) {
+    // include/LaxFriedrichsFlux.hpp:188-211, include/NavierStokesFlux.hpp:16-41
+    const NState<R, DIM> L = nstate<R, DIM>(g, q1), Rs = nstate<R, DIM>(g, q2);
+    R vn1 = R(0), vn2 = R(0), nn = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      vn1 += (q1[1 + d] / q1[0]) * n[d];
+      vn2 += (q2[1 + d] / q2[0]) * n[d];
+      nn += n[d] * n[d];
+    }
+    const R nm = rsqrt_(nn);
+    const R lmax = rmax(rabs(vn1) + rsqrt_(g.gamma * L.p / q1[0]) * nm,
+                        rabs(vn2) + rsqrt_(g.gamma * Rs.p / q2[0]) * nm);
+#pragma unroll
+    for (int e = 0; e < DIM + 2; ++e) {
+      const R nl = normal_flux<R, DIM>(q1, L, n, e), nr = normal_flux<R, DIM>(q2, Rs, n, e);
+      F[e] = R(0.5) * (nl + nr) - R(0.5) * lmax * (q2[e] - q1[e]);
+    }
+  } else {
+    // include/RoeFlux.hpp:42-149
+    const NState<R, DIM> left = nstate<R, DIM>(g, q1), right = nstate<R, DIM>(g, q2);
+    R nm2 = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nm2 += n[d] * n[d];
+    const R nm = rsqrt_(nm2);
+    const R inv_nm = R(1) / nm;
+    const R rhoL = q1[0], rhoR = q2[0];
+    const R pL = left.p, pR = right.p;
+    const R rootL = rsqrt_(rhoL), rootR = rsqrt_(rhoR);
+    const R rsi = R(1) / (rootL + rootR);
+    const R rho_roe = rootL * rootR;
+    const R HL = (q1[E] + pL) / rhoL, HR = (q2[E] + pR) / rhoR;
+    const R H = (rootL * HL + rootR * HR) * rsi;
+    R u[DIM], du_t[DIM], nh[DIM];
+    R u2 = R(0), un = R(0), dun = R(0);
+    R du[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const R uL = q1[1 + d] / rhoL, uR = q2[1 + d] / rhoR;
+      nh[d] = n[d] * inv_nm;
+      u[d] = (rootL * uL + rootR * uR) * rsi;
+      du[d] = uR - uL;
+      u2 += u[d] * u[d];
+      un += u[d] * nh[d];
+      dun += du[d] * nh[d];
+    }
+    const R a2 = (g.gamma - R(1)) * (H - R(0.5) * u2);
+    const R a = rsqrt_(a2);
+    const R dp = pR - pL, drho = rhoR - rhoL;
+    const R am = R(0.5) * (dp - rho_roe * a * dun) / a2;
+    const R ap = R(0.5) * (dp + rho_roe * a * dun) / a2;
+    const R az = drho - dp / a2;
+    const R lm = rabs(un - a) * nm, lz = rabs(un) * nm, lp = rabs(un + a) * nm;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) du_t[d] = du[d] - dun * nh[d];
+    R diss[DIM + 2];
+    diss[0] = lm * am + lz * az + lp * ap;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      diss[1 + d] = lm * am * (u[d] - a * nh[d]) + lz * (az * u[d] + rho_roe * du_t[d]) +
+                    lp * ap * (u[d] + a * nh[d]);
+    R udt = R(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) udt += u[d] * du_t[d];
+    diss[E] = lm * am * (H - a * un) + lz * (R(0.5) * az * u2 + rho_roe * udt) + lp * ap * (H + a * un);
+#pragma unroll
+    for (int e = 0; e < DIM + 2; ++e) {
+      const R central = R(0.5) * (normal_flux<R, DIM>(q1, left, n, e) + normal_flux<R, DIM>(q2, right, n, e));
+      F[e] = central - R(0.5) * diss[e];
+    }
+  }
+}
+
+// ---- viscous flux: include/NavierStokesFlux.hpp:160-290 --------------------
+// dp[d*(DIM+2) + eq] = gradient of the primitive (rho, u, p) in direction d.
+// Returns vf[eq*DIM + dir]; the mass row is zero.
+template <typename R, int DIM>
+__device__ __forceinline__ void viscous_flux(const GasT<R> &g, const R *q, const R *dp, R *vf) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+  const R mu = viscosity<R, DIM>(g, q);
+  const R kappa = mu * g.cp * g.Pr_inv;
+  const R rho = q[0];
+  const R p = pressure<R, DIM>(g, q);
+  const R pressor = p / rho;
+  const R fac = g.gm1_inv / (g.cv * rho);
+  R div = R(0);
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) div += dp[i * NEQ + 1 + i];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) vf[d] = R(0);
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    R ef = kappa * (fac * (dp[dir * NEQ + E] - pressor * dp[dir * NEQ + 0]));
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) {
+      R tau;
+      if (mom == dir) tau = mu * (R(2) * dp[dir * NEQ + 1 + mom] - g.mu_bulk * div);
+      else tau = mu * (dp[dir * NEQ + 1 + mom] + dp[mom * NEQ + 1 + dir]);
+      vf[(1 + mom) * DIM + dir] = tau;
+    }
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) ef += (q[1 + mom] / rho) * vf[(1 + mom) * DIM + dir];
+    vf[E * DIM + dir] = ef;
+  }
+}
+
+// include/EOS.hpp:206-234: entropy variables (s_rho, beta*u, -beta), beta = rho/p
+template <typename R, int DIM>
+__device__ __forceinline__ void entropy_vars(const GasT<R> &g, const R *q, R *w) {
+  const R rho = q[0];
+  const R ke = ke_density<R, DIM>(q);
+  const R p = g.gm1 * (q[DIM + 1] - ke);
+  const R s = rlog(p) - g.gamma * rlog(rho);
+  const R beta = rho / p;
+  const R v2o2 = ke / rho;
+  w[0] = (g.gamma - s) / (g.gamma - R(1)) - beta * v2o2;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) w[1 + d] = beta * (q[1 + d] / rho);
+  w[DIM + 1] = -beta;
+}
+
+// include/EOS.hpp:236-263: gradient of entropy variables -> gradient of (rho,u,p)
+template <typename R, int DIM>
+__device__ __forceinline__ void grad_entropy_to_prim(const GasT<R> &g, const R *q, const R *dE, R *dP) {
+  constexpr int E = DIM + 1;
+  const R rho = q[0];
+  const R ke = ke_density<R, DIM>(q);
+  const R p = g.gm1 * (q[E] - ke);
+  const R ie = q[E] - ke;
+  R drho = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    dP[1 + d] = p / rho * (dE[1 + d] + (q[1 + d] / rho) * dE[E]);
+    drho += q[1 + d] * dP[1 + d];
+  }
+  drho = rho * dE[0] - dE[E] * (ke - ie) + rho * drho / p;
+  dP[0] = drho;
+  dP[E] = p / rho * (dP[0] + p * dE[E]);
+}
+
+// Local face index lf (0:x-,1:x+,2:y-,3:y+,4:z-,5:z+) and face point fp ->
+// element-local lexicographic node.
+template <int DIM>
+__device__ __forceinline__ int trace_node(int N, int lf, int fp) {
+  const int dir = lf >> 1;
+  const int pos = (lf & 1) ? N - 1 : 0;
+  if (DIM == 2) return dir == 0 ? pos + N * fp : fp + N * pos;
+  const int a = fp % N, b = fp / N;
+  if (dir == 0) return pos + N * (a + N * b);
+  if (dir == 1) return a + N * (pos + N * b);
+  return a + N * (b + N * pos);
+}
+
+}  // namespace thx

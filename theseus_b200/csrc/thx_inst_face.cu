@@ -1,0 +1,30 @@
+// thx_inst_face.cu -- instantiates the face-flux kernels of one
+// (precision, dimension) pair.  Compiled with -DTHX_PREC and -DTHX_DIM.
+#include "thx_launch.cuh"
+
+#define THX_CAT3(a, b, c) a##_##b##_##c
+#define THX_NAME(P, D) THX_CAT3(face_kernels, P, D)
+#define THX_TYPE2(P) FaceKernels##P
+#define THX_TYPE(P) THX_TYPE2(P)
+#define THX_RT2(P) PREC_T_##P
+#define THX_RT(P) THX_RT2(P)
+
+namespace thx {
+
+THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
+  using R = THX_RT(THX_PREC);
+  THX_TYPE(THX_PREC) k;
+#define THX_SET(S)                                             \
+  k.face[S][0] = &launch_face<R, THX_DIM, S, false>;           \
+  k.face[S][1] = &launch_face<R, THX_DIM, S, true>;
+  THX_SET(SURF_CHANDRASHEKAR)
+  THX_SET(SURF_RANOCHA)
+  THX_SET(SURF_PIROZZOLI)
+  THX_SET(SURF_HLL)
+  THX_SET(SURF_LLF)
+  THX_SET(SURF_ROE)
+#undef THX_SET
+  return k;
+}
+
+}  // namespace thx

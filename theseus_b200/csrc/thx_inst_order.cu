@@ -1,0 +1,35 @@
+// thx_inst_order.cu -- instantiates the volume, gradient and indicator kernels
+// of one (precision, dimension, order) triple.  Compiled once per triple with
+// -DTHX_PREC=<0 double|1 float> -DTHX_DIM=<2|3> -DTHX_N=<nodes per direction>.
+#include "thx_launch.cuh"
+
+#ifndef THX_PREC
+#error "THX_PREC must be defined"
+#endif
+
+#define THX_CAT4(a, b, c, d) a##_##b##_##c##_##d
+#define THX_NAME(P, D, N) THX_CAT4(order_kernels, P, D, N)
+#define THX_TYPE2(P) OrderKernels##P
+#define THX_TYPE(P) THX_TYPE2(P)
+#define THX_RT2(P) PREC_T_##P
+#define THX_RT(P) THX_RT2(P)
+
+namespace thx {
+
+THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
+  using R = THX_RT(THX_PREC);
+  THX_TYPE(THX_PREC) k;
+  k.vol[VOL_CHANDRASHEKAR][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, false>;
+  k.vol[VOL_CHANDRASHEKAR][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, true>;
+  k.vol[VOL_RANOCHA][0] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, false>;
+  k.vol[VOL_RANOCHA][1] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, true>;
+  k.vol[VOL_PIROZZOLI][0] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, false>;
+  k.vol[VOL_PIROZZOLI][1] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, true>;
+  k.vol[VOL_CENTRAL][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false>;
+  k.vol[VOL_CENTRAL][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true>;
+  k.grad = &launch_grad<R, THX_DIM, THX_N>;
+  k.blend = &launch_blend<R, THX_DIM, THX_N>;
+  return k;
+}
+
+}  // namespace thx

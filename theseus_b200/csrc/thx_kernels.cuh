@@ -1,0 +1,779 @@
+// thx_kernels.cuh -- CUDA kernels of the DGSEM right-hand side on sm_100a.
+//
+// Layouts (all in HBM, R = double or float):
+//   state / rate     u[eq][elem][node]      (MFEM byNODES L-vector, node lexicographic)
+//   gradients        g[c][eq][elem][node]   (primitive gradients, NS only)
+//   face fluxes      fs[face][eq][fp]       (unweighted F*, inviscid minus viscous)
+//   geometry         jac[e*jac_es + n*jac_ns], metric block of DIM*DIM per node
+//                    at met[e*met_es + n*met_ns]; strides are 0 where the host
+//                    found the factor constant (exactly) over nodes/elements.
+//
+// Kernel structure per right-hand side:
+//   NS only : grad_kernel   element-local BR1 gradient of entropy variables with
+//             the interior-face lift, converted to primitive gradients.
+//   always  : face_kernel   one thread per face point: F*(u-,u+,n) (- n.avg(F_v)).
+//   always  : volume_kernel one CTA per EPB elements: flux differencing with every
+//             symmetric pair evaluated once, optional subcell-FV blend, viscous
+//             divergence, surface lift from fs; writes dudt once.
+#pragma once
+#include "thx_device.cuh"
+
+namespace thx {
+
+template <int DIM, int N>
+struct Shape {
+  static constexpr int ND = DIM == 2 ? N * N : N * N * N;
+  static constexpr int NFP = DIM == 2 ? N : N * N;
+  static constexpr int NEQ = DIM + 2;
+  static constexpr int EPB = (256 / ND) > 0 ? 256 / ND : 1;
+  static constexpr int THREADS = ((EPB * ND + 31) / 32) * 32;
+  static constexpr int NP = N * (N - 1) / 2;  // pairs per line
+  static constexpr int NLINE = ND / N;
+  static constexpr int PAIRS = NLINE * NP;     // pairs per element and direction
+  static constexpr int NPRIM = DIM + 3;
+};
+
+// Node index of position `pos` on tensor line `line` along direction dir.
+template <int DIM, int N>
+__device__ __forceinline__ int line_node(int dir, int line, int pos) {
+  if (DIM == 2) return dir == 0 ? pos + N * line : line + N * pos;
+  if (dir == 0) return pos + N * line;
+  if (dir == 1) return (line % N) + N * (pos + N * (line / N));
+  return line + N * N * pos;
+}
+template <int DIM, int N>
+__device__ __forceinline__ void node_coords(int n, int *c) {
+  c[0] = n % N;
+  c[1] = (n / N) % N;
+  c[2] = DIM == 3 ? n / (N * N) : 0;
+}
+template <int DIM, int N>
+__device__ __forceinline__ int line_of(int dir, const int *c) {
+  if (DIM == 2) return dir == 0 ? c[1] : c[0];
+  if (dir == 0) return c[1] + N * c[2];
+  if (dir == 1) return c[0] + N * c[2];
+  return c[0] + N * c[1];
+}
+// Face point of a node on a face normal to `dir` (same order as trace_node).
+template <int DIM, int N>
+__device__ __forceinline__ int face_point(int dir, const int *c) {
+  if (DIM == 2) return dir == 0 ? c[1] : c[0];
+  if (dir == 0) return c[1] + N * c[2];
+  if (dir == 1) return c[0] + N * c[2];
+  return c[0] + N * c[1];
+}
+template <int N>
+__device__ __forceinline__ int pair_index(int lo, int hi) {
+  return lo * (N - 1) - (lo * (lo - 1)) / 2 + (hi - lo - 1);
+}
+template <int N>
+__device__ __forceinline__ void pair_decode(int k, int &a, int &b) {
+  a = 0;
+#pragma unroll
+  for (int s = 0; s < N - 1; ++s) {
+    if (k >= N - 1 - a) { k -= N - 1 - a; ++a; }
+  }
+  b = a + 1 + k;
+}
+
+// Status bits written by kernels (read by thx_read_status).
+enum : unsigned { STATUS_NONPOSITIVE = 1u, STATUS_NONFINITE = 2u };
+
+template <typename R>
+struct VolArgs {
+  const R *u;
+  R *du;
+  int ne;
+  const R *jac;
+  long long jac_es, jac_ns;
+  const R *met;
+  long long met_es, met_ns;
+  const int *elem_face;   // [e][2*DIM] = 2*face + side
+  const R *fstar;         // [f][eq][fp]
+  const R *wm, *wp;       // lift weights
+  long long w_fs, w_ps;
+  const R *grad;          // NS primitive gradients
+  const double *alpha;    // per-element blending coefficient or nullptr
+  const R *sub[3];        // subcell metrics (reference layout), element stride sub_es
+  long long sub_es[3];
+  int fv_flux;            // SurfKind for the subcell FV fluxes
+  GasT<R> gas;
+  const R *ops;           // [Dhat2 N*N | Dhat N*N | w N]
+  // fused SSP-RK3 stage (stage==0: plain dudt)
+  int stage;
+  double dt;
+  double *um;             // FP64 master state (read every stage, written by stage 3)
+  double *y;              // FP64 stage state (written by stages 1 and 2)
+  float *yf;              // FP32 working copy of the next RHS input (mixed mode) or nullptr
+  unsigned *status;
+};
+
+// Surface flux with a run-time selector (used on subcell faces).
+template <typename R, int DIM>
+__device__ __noinline__ void surface_flux_rt(int kind, const GasT<R> &g, const R *q1, const R *q2,
+                                             const R *n, R *F) {
+  switch (kind) {
+    case SURF_CHANDRASHEKAR: surface_flux<R, DIM, SURF_CHANDRASHEKAR>(g, q1, q2, n, F); break;
+    case SURF_RANOCHA: surface_flux<R, DIM, SURF_RANOCHA>(g, q1, q2, n, F); break;
+    case SURF_PIROZZOLI: surface_flux<R, DIM, SURF_PIROZZOLI>(g, q1, q2, n, F); break;
+    case SURF_HLL: surface_flux<R, DIM, SURF_HLL>(g, q1, q2, n, F); break;
+    case SURF_ROE: surface_flux<R, DIM, SURF_ROE>(g, q1, q2, n, F); break;
+    default: surface_flux<R, DIM, SURF_LLF>(g, q1, q2, n, F); break;
+  }
+}
+
+template <typename R, int DIM, int N, int VOL, bool NS>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+volume_kernel(const VolArgs<R> a) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = S::NPRIM, PAIRS = S::PAIRS;
+  constexpr int MB = DIM * DIM;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded to 64)
+  R *sPrim = sOps + 64;                                   // [EPB][NPRIM][ND]
+  R *sQ = sPrim + EPB * NPRIM * ND;                       // [EPB][NEQ][ND]
+  R *sMet = sQ + EPB * NEQ * ND;                          // [EPB][ND][MB]
+  R *sFB = sMet + EPB * ND * MB;                          // [EPB][PAIRS][NEQ] (aliased by FV rate)
+  R *sFv = sFB + EPB * PAIRS * NEQ;                       // [EPB][DIM][NEQ][ND] (NS)
+
+  const int tid = threadIdx.x;
+  const int e0 = blockIdx.x * EPB;
+  const long long L = (long long)a.ne * ND;
+  for (int i = tid; i < 2 * N * N + N; i += blockDim.x) sOps[i] = a.ops[i];
+  const R *sD2 = sOps;
+  const R *sDh = sOps + N * N;
+  const R *sW = sOps + 2 * N * N;
+
+  // stage states, node data and metric
+  const int el = tid / ND, n = tid % ND;
+  const int e = e0 + el;
+  const bool active = (el < EPB) && (e < a.ne);
+  if (active) {
+    R q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    R pr[NPRIM];
+    node_prims<R, DIM, VOL>(a.gas, q, pr);
+#pragma unroll
+    for (int k = 0; k < NPRIM; ++k) sPrim[(el * NPRIM + k) * ND + n] = pr[k];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+    if (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))) atomicOr(a.status, STATUS_NONPOSITIVE);
+    const R *mp = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
+#pragma unroll
+    for (int k = 0; k < MB; ++k) sMet[(el * ND + n) * MB + k] = mp[k];
+  }
+  __syncthreads();
+
+  int c[3];
+  node_coords<DIM, N>(n, c);
+  R rate[NEQ];
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) rate[k] = R(0);
+
+#pragma unroll 1
+  for (int dir = 0; dir < DIM; ++dir) {
+    // pair phase: every symmetric pair once, in (lower, upper) order
+    for (int t = tid; t < EPB * PAIRS; t += blockDim.x) {
+      const int pel = t / PAIRS, pidx = t % PAIRS;
+      if (e0 + pel >= a.ne) continue;
+      const int line = pidx / S::NP;
+      int pa, pb;
+      pair_decode<N>(pidx % S::NP, pa, pb);
+      const int na = line_node<DIM, N>(dir, line, pa), nb = line_node<DIM, N>(dir, line, pb);
+      R A[NPRIM], B[NPRIM], met[DIM], F[NEQ];
+#pragma unroll
+      for (int k = 0; k < NPRIM; ++k) {
+        A[k] = sPrim[(pel * NPRIM + k) * ND + na];
+        B[k] = sPrim[(pel * NPRIM + k) * ND + nb];
+      }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        met[d] = R(0.5) * (sMet[(pel * ND + na) * MB + dir * DIM + d] + sMet[(pel * ND + nb) * MB + dir * DIM + d]);
+      if (VOL == VOL_CHANDRASHEKAR) vol_chandrashekar<R, DIM>(a.gas, A, B, met, F);
+      else if (VOL == VOL_RANOCHA) vol_ranocha<R, DIM>(a.gas, A, B, met, F);
+      else if (VOL == VOL_PIROZZOLI) vol_pirozzoli<R, DIM>(a.gas, A, B, met, F);
+      else {
+        R QA[NEQ], QB[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) {
+          QA[k] = sQ[(pel * NEQ + k) * ND + na];
+          QB[k] = sQ[(pel * NEQ + k) * ND + nb];
+        }
+        vol_central<R, DIM>(QA, QB, A, B, met, F);
+      }
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) sFB[(pel * PAIRS + pidx) * NEQ + k] = F[k];
+    }
+    __syncthreads();
+    // node phase: rate_i += sum_m Dhat2(i,m) F(i,m) in m order
+    if (active) {
+      const int me = c[dir];
+      const int line = line_of<DIM, N>(dir, c);
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        if (m == me) continue;
+        const int lo = m < me ? m : me, hi = m < me ? me : m;
+        const int pidx = line * S::NP + pair_index<N>(lo, hi);
+        const R coef = sD2[me * N + m];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) rate[k] += coef * sFB[(el * PAIRS + pidx) * NEQ + k];
+      }
+    }
+    __syncthreads();
+  }
+
+  R du[NEQ];
+  R J = R(1);
+  if (active) {
+    J = a.jac[(long long)e * a.jac_es + (long long)n * a.jac_ns];
+    const R s = R(-1) / J;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) du[k] = s * rate[k];
+  }
+
+  // subcell finite-volume blend (include/DGSEMIntegrator.hpp:338-483,
+  // include/EulerOperator_impl.hpp:134-152)
+  if (a.alpha != nullptr) {
+    bool any = false;
+    for (int k = 0; k < EPB; ++k)
+      if (e0 + k < a.ne && a.alpha[e0 + k] > 1e-16) any = true;
+    if (any) {
+      R *sRfv = sFB;  // [EPB][NEQ][ND]
+#pragma unroll 1
+      for (int dir = 0; dir < DIM; ++dir) {
+        for (int t = tid; t < EPB * S::NLINE; t += blockDim.x) {
+          const int lel = t / S::NLINE, line = t % S::NLINE;
+          const int le = e0 + lel;
+          if (le >= a.ne || !(a.alpha[le] > 1e-16)) continue;
+          const R *sub = a.sub[dir] + (long long)le * a.sub_es[dir];
+          R s1[NEQ], s2[NEQ], fn[NEQ], dus[NEQ];
+          int id1 = line_node<DIM, N>(dir, line, 0);
+#pragma unroll
+          for (int k = 0; k < NEQ; ++k) { dus[k] = R(0); s1[k] = sQ[(lel * NEQ + k) * ND + id1]; }
+          for (int i = 0; i < N; ++i) {
+            R Ji = a.jac[(long long)le * a.jac_es + (long long)id1 * a.jac_ns];
+            if (i < N - 1) {
+              const int id2 = line_node<DIM, N>(dir, line, i + 1);
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) s2[k] = sQ[(lel * NEQ + k) * ND + id2];
+              R nrm[DIM];
+#pragma unroll
+              for (int d = 0; d < DIM; ++d) nrm[d] = sub[id2 * DIM + d];
+              surface_flux_rt<R, DIM>(a.fv_flux, a.gas, s1, s2, nrm, fn);
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) dus[k] -= fn[k];
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) dus[k] /= (Ji * sW[i]);
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) {
+                R &dst = sRfv[(lel * NEQ + k) * ND + id1];
+                dst = dir == 0 ? dus[k] : dst + dus[k];
+              }
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) { dus[k] = fn[k]; s1[k] = s2[k]; }
+              id1 = id2;
+            } else {
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) dus[k] /= (Ji * sW[N - 1]);
+#pragma unroll
+              for (int k = 0; k < NEQ; ++k) {
+                R &dst = sRfv[(lel * NEQ + k) * ND + id1];
+                dst = dir == 0 ? dus[k] : dst + dus[k];
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+      if (active) {
+        const double al = a.alpha[e];
+        if (al > 1e-16) {
+          const R af = (R)al, ad = (R)(1.0 - al);
+#pragma unroll
+          for (int k = 0; k < NEQ; ++k) du[k] = ad * du[k] + af * sRfv[(el * NEQ + k) * ND + n];
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  if (NS) {
+    // contravariant viscous flux per node (include/DGSEMIntegrator.hpp:486-524)
+    if (active) {
+      R q[NEQ], dp[DIM * NEQ], vf[NEQ * DIM];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) q[k] = sQ[(el * NEQ + k) * ND + n];
+#pragma unroll
+      for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) dp[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + (long long)e * ND + n];
+      viscous_flux<R, DIM>(a.gas, q, dp, vf);
+      const R *row = sMet + (el * ND + n) * MB;
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir)
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) {
+          R f = R(0);
+#pragma unroll
+          for (int pd = 0; pd < DIM; ++pd) f += row[dir * DIM + pd] * vf[k * DIM + pd];
+          sFv[((el * DIM + dir) * NEQ + k) * ND + n] = f;
+        }
+    }
+    __syncthreads();
+    // weak-form divergence with Dhat (include/DGSEMIntegrator.hpp:526-622)
+    if (active) {
+      R dv[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) dv[k] = R(0);
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir) {
+        const int me = c[dir];
+        const int line = line_of<DIM, N>(dir, c);
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+          const int s = line_node<DIM, N>(dir, line, l);
+          const R co = sDh[me * N + l];
+#pragma unroll
+          for (int k = 0; k < NEQ; ++k) dv[k] += co * sFv[((el * DIM + dir) * NEQ + k) * ND + s];
+        }
+      }
+      const R sc = R(1) / J;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) du[k] += sc * dv[k];
+    }
+  }
+
+  if (!active) return;
+  // surface lift: faces summed first, then added (restr_f transpose; +=)
+  {
+    R acc[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) acc[k] = R(0);
+    bool any = false;
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+      const int me = c[dir];
+      if (me != 0 && me != N - 1) continue;
+      const int lf = 2 * dir + (me == N - 1 ? 1 : 0);
+      const int fs = a.elem_face[e * 2 * DIM + lf];
+      if (fs < 0) continue;
+      const int f = fs >> 1, side = fs & 1;
+      const int fp = face_point<DIM, N>(dir, c);
+      const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
+      const R w = side == 0 ? -a.wm[wi] : a.wp[wi];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) acc[k] += w * a.fstar[((long long)f * NEQ + k) * S::NFP + fp];
+      any = true;
+    }
+    if (any) {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) du[k] += acc[k];
+    }
+  }
+  const long long base = (long long)e * ND + n;
+  if (a.stage == 0) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) a.du[k * L + base] = du[k];
+  } else {
+    // fused SSP-RK3 stage in the arithmetic order of mfem::RK3SSPSolver::Step
+    const double dt = a.dt;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      const long long i = k * L + base;
+      const double kk = (double)du[k];
+      double y;
+      if (a.stage == 1) {
+        y = a.um[i] + dt * kk;
+        a.y[i] = y;
+      } else if (a.stage == 2) {
+        y = a.y[i] + dt * kk;
+        y = 0.75 * a.um[i] + 0.25 * y;
+        a.y[i] = y;
+      } else {
+        y = a.y[i] + dt * kk;
+        y = (1.0 / 3.0) * a.um[i] + (2.0 / 3.0) * y;
+        a.um[i] = y;
+      }
+      if (a.yf) a.yf[i] = (float)y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename R>
+struct FaceArgs {
+  const R *u;
+  int ne, nf, N;
+  const int *face_elem, *face_lface;
+  const R *normal;
+  long long n_fs, n_ps;
+  const R *grad;
+  R *fstar;
+  GasT<R> gas;
+};
+
+template <typename R, int DIM, int SURF, bool NS>
+__global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
+  constexpr int NEQ = DIM + 2;
+  const int N = a.N;
+  const int nfp = DIM == 2 ? N : N * N;
+  const int nd = DIM == 2 ? N * N : N * N * N;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)a.nf * nfp) return;
+  const int f = (int)(t / nfp), fp = (int)(t % nfp);
+  const long long L = (long long)a.ne * nd;
+  const int em = a.face_elem[2 * f], ep = a.face_elem[2 * f + 1];
+  const long long im = (long long)em * nd + trace_node<DIM>(N, a.face_lface[2 * f], fp);
+  const long long ip = (long long)ep * nd + trace_node<DIM>(N, a.face_lface[2 * f + 1], fp);
+  R qm[NEQ], qp[NEQ], nrm[DIM], F[NEQ];
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) { qm[k] = a.u[k * L + im]; qp[k] = a.u[k * L + ip]; }
+  const R *np = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) nrm[d] = np[d];
+  surface_flux<R, DIM, SURF>(a.gas, qm, qp, nrm, F);
+  if (NS) {
+    // include/DGSEMIntegrator.hpp:261-316
+    R gm[DIM * NEQ], gp[DIM * NEQ], vm[NEQ * DIM], vp[NEQ * DIM];
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        gm[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + im];
+        gp[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + ip];
+      }
+    viscous_flux<R, DIM>(a.gas, qm, gm, vm);
+    viscous_flux<R, DIM>(a.gas, qp, gp, vp);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) F[k] -= nrm[d] * (R(0.5) * (vm[k * DIM + d] + vp[k * DIM + d]));
+  }
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) a.fstar[((long long)f * NEQ + k) * nfp + fp] = F[k];
+}
+
+// ---------------------------------------------------------------------------
+template <typename R>
+struct GradArgs {
+  const R *u;
+  R *grad;
+  int ne;
+  const R *jac;
+  long long jac_es, jac_ns;
+  const R *met;
+  long long met_es, met_ns;
+  const int *elem_face, *face_elem, *face_lface;
+  const R *normal;
+  long long n_fs, n_ps;
+  const R *wm, *wp;
+  long long w_fs, w_ps;
+  const R *D;  // N*N
+  GasT<R> gas;
+};
+
+// BR1 gradient (include/NSOperator_impl.hpp:11-159,194-517;
+// include/DGSEMIntegrator.hpp:764-850,1011-1044)
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded to 64)
+  R *sS = sD + 64;                           // [EPB][NEQ][ND]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N * N; i += blockDim.x) sD[i] = a.D[i];
+  const int el = tid / ND, n = tid % ND;
+  const int e = blockIdx.x * EPB + el;
+  const bool active = (el < EPB) && (e < a.ne);
+  const long long L = (long long)a.ne * ND;
+  R q[NEQ];
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    R w[NEQ];
+    entropy_vars<R, DIM>(a.gas, q, w);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sS[(el * NEQ + k) * ND + n] = w[k];
+  }
+  __syncthreads();
+  if (!active) return;
+  int c[3];
+  node_coords<DIM, N>(n, c);
+  R dref[DIM][NEQ];
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const int me = c[dir];
+    const int line = line_of<DIM, N>(dir, c);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) dref[dir][k] = R(0);
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const int s = line_node<DIM, N>(dir, line, l);
+      const R co = sD[me * N + l];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) dref[dir][k] += sS[(el * NEQ + k) * ND + s] * co;
+    }
+  }
+  const R invJ = R(1) / a.jac[(long long)e * a.jac_es + (long long)n * a.jac_ns];
+  const R *adj = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
+  R adjr[DIM * DIM];
+#pragma unroll
+  for (int k = 0; k < DIM * DIM; ++k) adjr[k] = adj[k];
+  R g[DIM][NEQ];
+#pragma unroll
+  for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      R s = dref[0][k] * adjr[0 * DIM + cc];
+#pragma unroll
+      for (int dir = 1; dir < DIM; ++dir) s += dref[dir][k] * adjr[dir * DIM + cc];
+      g[cc][k] = invJ * s;
+    }
+  // interior-face lift: w * 0.5 (S+ - S-) n_c, faces summed then added
+  {
+    R acc[DIM][NEQ];
+    bool any = false;
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) acc[cc][k] = R(0);
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+      const int me = c[dir];
+      if (me != 0 && me != N - 1) continue;
+      const int lf = 2 * dir + (me == N - 1 ? 1 : 0);
+      const int fs = a.elem_face[e * 2 * DIM + lf];
+      if (fs < 0) continue;
+      const int f = fs >> 1, side = fs & 1;
+      const int fp = face_point<DIM, N>(dir, c);
+      const int eo = a.face_elem[2 * f + 1 - side];
+      const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
+      R qo[NEQ], so[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) qo[k] = a.u[k * L + (long long)eo * ND + no];
+      entropy_vars<R, DIM>(a.gas, qo, so);
+      const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
+      const R w = side == 0 ? a.wm[wi] : a.wp[wi];
+      const R *nr = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        const R sown = sS[(el * NEQ + k) * ND + n];
+        const R jump = side == 0 ? R(0.5) * (so[k] - sown) : R(0.5) * (sown - so[k]);
+#pragma unroll
+        for (int cc = 0; cc < DIM; ++cc) acc[cc][k] += w * (jump * nr[cc]);
+      }
+      any = true;
+    }
+    if (any) {
+#pragma unroll
+      for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) g[cc][k] += acc[cc][k];
+    }
+  }
+#pragma unroll
+  for (int cc = 0; cc < DIM; ++cc) {
+    R dP[NEQ];
+    grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dP);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) a.grad[((long long)cc * NEQ + k) * L + (long long)e * ND + n] = dP[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persson-Peraire indicator (include/RHSOperator_impl.hpp:355-527): modal
+// energy of p*rho with the tensor-product Legendre transform applied by sum
+// factorisation (V^-1 = V1^-1 (x) V1^-1 (x) V1^-1).
+template <typename R>
+struct BlendArgs {
+  const R *u;
+  int ne;
+  const double *vinv;  // N*N, row = degree
+  GasT<R> gas;
+  double threshold, sharpness, alpha_min, alpha_max;
+  double *alpha, *eta;
+};
+
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const BlendArgs<R> a) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
+  __shared__ double sV[N * N];
+  __shared__ double sA[EPB * ND], sB[EPB * ND];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N * N; i += blockDim.x) sV[i] = a.vinv[i];
+  const int el = tid / ND, n = tid % ND;
+  const int e = blockIdx.x * EPB + el;
+  const bool active = (el < EPB) && (e < a.ne);
+  const long long L = (long long)a.ne * ND;
+  if (active) {
+    R q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    sA[el * ND + n] = (double)(pressure<R, DIM>(a.gas, q) * q[0]);
+  }
+  __syncthreads();
+  int c[3];
+  node_coords<DIM, N>(n, c);
+  // contract direction by direction: after pass d, index c[d] is a mode degree
+  double *src = sA, *dst = sB;
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    if (active) {
+      const int line = line_of<DIM, N>(dir, c);
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < N; ++l) s += sV[c[dir] * N + l] * src[el * ND + line_node<DIM, N>(dir, line, l)];
+      dst[el * ND + n] = s;
+    }
+    __syncthreads();
+    double *t = src; src = dst; dst = t;
+  }
+  // deterministic per-element sums in mode order
+  if (active && n == 0) {
+    double mm = 0.0, m1 = 0.0, m2 = 0.0;
+    for (int m = 0; m < ND; ++m) {
+      int cm[3];
+      node_coords<DIM, N>(m, cm);
+      int mx = cm[0];
+#pragma unroll
+      for (int d = 1; d < DIM; ++d) mx = cm[d] > mx ? cm[d] : mx;
+      const double mode = src[el * ND + m];
+      const double sq = mode * mode;
+      mm += sq;
+      if (mx <= N - 2) m1 += sq;
+      if (mx <= N - 3) m2 += sq;
+    }
+    const double eps = 1.0e-30;
+    double val = 0.0;
+    if (mm > eps) {
+      val = 1.0 - m1 / mm;
+      if (m1 > eps) val = fmax(val, 1.0 - m2 / m1);
+      else val = 1.0;
+    }
+    const double et = fmin(fmax(val, 0.0), 1.0);
+    double al = 1.0 / (1.0 + exp(-a.sharpness * (et - a.threshold) / a.threshold));
+    if (al < a.alpha_min) al = 0.0;
+    else if (al > 1.0 - a.alpha_min) al = 1.0;
+    a.alpha[e] = fmin(al, a.alpha_max);
+    if (a.eta) a.eta[e] = et;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SSP-RK3 stage updates (mfem::RK3SSPSolver::Step order) for the unfused path.
+template <typename R>
+__global__ void rk_stage_kernel(int stage, long long n, double dt, const R *k, double *um,
+                                double *y, float *yf) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double kk = (double)k[i];
+    double v;
+    if (stage == 1) { v = um[i] + dt * kk; y[i] = v; }
+    else if (stage == 2) { v = y[i] + dt * kk; v = 0.75 * um[i] + 0.25 * v; y[i] = v; }
+    else { v = y[i] + dt * kk; v = (1.0 / 3.0) * um[i] + (2.0 / 3.0) * v; um[i] = v; }
+    if (yf) yf[i] = (float)v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stability rates (include/RHSOperator_impl.hpp:10-174) reduced on device.
+struct StabArgs {
+  const double *u;
+  int ne, N;
+  const double *jac;
+  long long jac_es, jac_ns;
+  const double *met;
+  long long met_es, met_ns;
+  const int *face_elem, *face_lface;
+  int nf;
+  const double *normal;
+  long long n_fs, n_ps;
+  const double *wm, *wp;
+  long long w_fs, w_ps;
+  GasT<double> gas;
+  double adv_scale, dif_scale, surf_scale;
+  int viscous;
+  unsigned long long *out;  // [3] as ordered bit patterns of non-negative doubles
+};
+
+template <int DIM>
+__global__ void stability_kernel(const StabArgs a) {
+  constexpr int NEQ = DIM + 2;
+  const int N = a.N;
+  const int nd = DIM == 2 ? N * N : N * N * N;
+  const int nfp = DIM == 2 ? N : N * N;
+  const long long L = (long long)a.ne * nd;
+  const long long nface_pts = (long long)a.nf * nfp;
+  double adv = 0.0, dif = 0.0, sur = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < L + nface_pts; t += stride) {
+    if (t < L) {
+      const long long e = t / nd, n = t % nd;
+      double q[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + t];
+      const double ij = 1.0 / a.jac[e * a.jac_es + n * a.jac_ns];
+      const double *M = a.met + e * a.met_es + n * a.met_ns;
+      const double snd = sound_speed<double, DIM>(a.gas, q);
+      double ds = 0.0, mss = 0.0;
+#pragma unroll
+      for (int rd = 0; rd < DIM; ++rd) {
+        double vdm = 0.0, mn2 = 0.0;
+#pragma unroll
+        for (int pd = 0; pd < DIM; ++pd) {
+          const double v = M[rd * DIM + pd];
+          vdm += (q[1 + pd] / q[0]) * v;
+          mn2 += v * v;
+        }
+        ds += (fabs(vdm) + snd * sqrt(mn2)) * ij;
+        mss += mn2 * ij * ij;
+      }
+      adv = fmax(adv, a.adv_scale * ds);
+      if (a.viscous) {
+        const double mu = viscosity<double, DIM>(a.gas, q);
+        const double lon = (2.0 - a.gas.mu_bulk) * mu;
+        const double md = fmax(mu, lon) / q[0];
+        const double td = (mu * a.gas.cp * a.gas.Pr_inv) * a.gas.gamma / (q[0] * a.gas.cp);
+        dif = fmax(dif, a.dif_scale * fmax(md, td) * mss);
+      }
+    } else {
+      const long long fpt = t - L;
+      const int f = (int)(fpt / nfp), fp = (int)(fpt % nfp);
+      const long long im = (long long)a.face_elem[2 * f] * nd + trace_node<DIM>(N, a.face_lface[2 * f], fp);
+      const long long ip = (long long)a.face_elem[2 * f + 1] * nd + trace_node<DIM>(N, a.face_lface[2 * f + 1], fp);
+      double qm[NEQ], qp[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) { qm[k] = a.u[k * L + im]; qp[k] = a.u[k * L + ip]; }
+      const double *nr = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
+      double n2 = 0.0, vm = 0.0, vp = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        n2 += nr[d] * nr[d];
+        vm += (qm[1 + d] / qm[0]) * nr[d];
+        vp += (qp[1 + d] / qp[0]) * nr[d];
+      }
+      const double nm = sqrt(n2);
+      const double ws = fmax(fabs(vm) + sound_speed<double, DIM>(a.gas, qm) * nm,
+                             fabs(vp) + sound_speed<double, DIM>(a.gas, qp) * nm);
+      const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
+      sur = fmax(sur, ws * fmax(fabs(a.wm[wi]), fabs(a.wp[wi])) * a.surf_scale);
+    }
+  }
+  // warp reduce then one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    adv = fmax(adv, __shfl_xor_sync(0xffffffffu, adv, o));
+    dif = fmax(dif, __shfl_xor_sync(0xffffffffu, dif, o));
+    sur = fmax(sur, __shfl_xor_sync(0xffffffffu, sur, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&a.out[0], (unsigned long long)__double_as_longlong(adv));
+    atomicMax(&a.out[1], (unsigned long long)__double_as_longlong(sur));
+    atomicMax(&a.out[2], (unsigned long long)__double_as_longlong(dif));
+  }
+}
+
+}  // namespace thx
