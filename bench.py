@@ -198,6 +198,9 @@ def run_ours(args):
         dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                  device_id=torch.device("cuda", local))
         dist = dist_
+    if args.n != WORKLOAD["mesh"][0]:
+        WORKLOAD["mesh"] = [args.n] * 3
+        WORKLOAD["workload"] = f"ns_tgv_{args.n}^3_p4"
     m, u = build_case()
     prec = "fp32" if args.precision == "fp32" else "fp64"
     op = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"], surface_flux=WORKLOAD["surface_flux"],
@@ -273,7 +276,8 @@ def run_ours(args):
                 "phase_ms": {k: float(v) for k, v in zip(names, phases)},
                 "algorithmic_bytes": {k: int(v) for k, v in algo.items()}}
     # FP64 pipe view of the flux-differencing kernel: pairs x F_pair flops
-    pairs = m.num_elements * 3 * 25 * 10
+    N = m.order + 1
+    pairs = m.num_elements * 3 * N * N * (N * (N - 1) // 2)
     roofline["volume_pair_evals_per_s"] = pairs / (phases[3] * 1e-3)
 
     # FP32-mixed companion number and its error against FP64
@@ -330,6 +334,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

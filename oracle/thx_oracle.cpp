@@ -1454,7 +1454,7 @@ int orc_estimate_dt(const thx_geometry *g, const thx_config *cfg, const double *
     for (int fp = 0; fp < c.nfp; ++fp) {
       const size_t nm = (size_t)em * nd + trace_node(c, lm, fp);
       const size_t np = (size_t)ep * nd + trace_node(c, lp, fp);
-      double qm[MAXEQ], qp[MAXEQ];
+      double qm[MAXEQ] = {0}, qp[MAXEQ] = {0};
       for (int k = 0; k < neq; ++k) { qm[k] = u[k * L + nm]; qp[k] = u[k * L + np]; }
       const double *nr = g->face_normal + ((size_t)f * c.nfp + fp) * dim;
       double n2 = 0, vm = 0, vp = 0;

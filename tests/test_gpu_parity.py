@@ -28,6 +28,8 @@ def gpu_rhs(mesh, u, **kw):
 
 
 def oracle_rhs(mesh, u, ns=False, **kw):
+    if "numerical_flux" in kw:
+        kw["volume_flux"] = kw.pop("numerical_flux")
     cfg = T.make_config(flow="ns" if ns else "euler", **kw)
     return O.rhs(oracle_mesh(mesh), cfg, u, nthreads=4, want_alpha=True)
 

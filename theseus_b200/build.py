@@ -48,6 +48,12 @@ def _stale(obj, src):
 
 def _compile(job):
     obj, src, defs = job
+    # The FP64 path keeps every multiply and add separately rounded, like the
+    # reference's CPU builds (-ffp-contract=off), so that it reproduces the CPU
+    # right-hand side to round-off even where the result cancels strongly.
+    # The FP32-mixed units may contract to FMA.
+    if "-DTHX_PREC=1" not in defs:
+        defs = defs + ["--fmad=false"]
     cmd = [NVCC] + ARCH + FLAGS + defs + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [NVCC] + FLAGS + defs + ["-x", "cu", "-c", src, "-o", obj] + ARCH

@@ -31,6 +31,8 @@ struct Shape {
   static constexpr int NLINE = ND / N;
   static constexpr int PAIRS = NLINE * NP;     // pairs per element and direction
   static constexpr int NPRIM = DIM + 3;
+  static constexpr int OPS = ((2 * N * N + N + 7) / 8) * 8;  // Dhat2 | Dhat | w, padded
+  static constexpr int DPAD = ((N * N + 7) / 8) * 8;
 };
 
 // Node index of position `pos` on tensor line `line` along direction dir.
@@ -129,8 +131,8 @@ volume_kernel(const VolArgs<R> a) {
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = S::NPRIM, PAIRS = S::PAIRS;
   constexpr int MB = DIM * DIM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded to 64)
-  R *sPrim = sOps + 64;                                   // [EPB][NPRIM][ND]
+  R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded)
+  R *sPrim = sOps + S::OPS;                               // [EPB][NPRIM][ND]
   R *sQ = sPrim + EPB * NPRIM * ND;                       // [EPB][NEQ][ND]
   R *sMet = sQ + EPB * NEQ * ND;                          // [EPB][ND][MB]
   R *sFB = sMet + EPB * ND * MB;                          // [EPB][PAIRS][NEQ] (aliased by FV rate)
@@ -480,8 +482,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const Grad
   using S = Shape<DIM, N>;
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded to 64)
-  R *sS = sD + 64;                           // [EPB][NEQ][ND]
+  R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded)
+  R *sS = sD + S::DPAD;                      // [EPB][NEQ][ND]
   const int tid = threadIdx.x;
   for (int i = tid; i < N * N; i += blockDim.x) sD[i] = a.D[i];
   const int el = tid / ND, n = tid % ND;

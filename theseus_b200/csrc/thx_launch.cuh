@@ -16,7 +16,7 @@ template <typename R> using BlendLaunch = cudaError_t (*)(const BlendArgs<R> &, 
 template <typename R, int DIM, int N, bool NS>
 constexpr size_t volume_smem_bytes() {
   using S = Shape<DIM, N>;
-  return sizeof(R) * (64 + (size_t)S::EPB * (S::NPRIM * S::ND + S::NEQ * S::ND + S::ND * DIM * DIM +
+  return sizeof(R) * (S::OPS + (size_t)S::EPB * (S::NPRIM * S::ND + S::NEQ * S::ND + S::ND * DIM * DIM +
                                              S::PAIRS * S::NEQ + (NS ? DIM * S::NEQ * S::ND : 0)));
 }
 
@@ -47,7 +47,7 @@ cudaError_t launch_face(const FaceArgs<R> &a, cudaStream_t s) {
 template <typename R, int DIM, int N>
 cudaError_t launch_grad(const GradArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
-  constexpr size_t smem = sizeof(R) * (64 + (size_t)S::EPB * S::NEQ * S::ND);
+  constexpr size_t smem = sizeof(R) * (S::DPAD + (size_t)S::EPB * S::NEQ * S::ND);
   if (prepare)
     return cudaFuncSetAttribute(grad_kernel<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem);
