@@ -113,16 +113,18 @@ def peaks():
 
 
 def bytes_per_phase(m, elem_size=8):
-    """Algorithmic HBM bytes of each kernel for one RHS (compressed geometry):
-    gradient: read u, write grad; face: read both traces of u and grad, write F*;
-    volume: read u, grad, F* once, write dudt."""
+    """Algorithmic HBM bytes of each kernel for one RHS (geometry stored once):
+    gradient: read u, write the physical viscous flux (dim x (neq-1) per node);
+    face: read both traces of u and of the viscous flux, write F*;
+    volume: read u, the viscous flux and F* once, write dudt."""
     nodes = m.num_nodes
     neq, dim = m.neq, m.dim
+    nv = dim * (neq - 1)
     fpts = m.num_faces * m.nfp
     s = elem_size
-    grad = nodes * neq * s + nodes * dim * neq * s
-    face = fpts * (2 * neq + 2 * dim * neq + neq) * s
-    vol = nodes * neq * s * 2 + nodes * dim * neq * s + fpts * neq * s
+    grad = nodes * (neq + nv) * s
+    face = fpts * (2 * neq + 2 * nv + neq) * s
+    vol = nodes * (2 * neq + nv) * s + fpts * neq * s
     return {"blend": nodes * neq * s, "grad": grad, "face": face, "volume": vol}
 
 

@@ -134,7 +134,7 @@ struct thx_operator_s {
   float *jac32 = nullptr, *met32 = nullptr, *nrm32 = nullptr, *wm32 = nullptr, *wp32 = nullptr;
   float *sub32[3] = {nullptr, nullptr, nullptr}, *ops32 = nullptr, *D32 = nullptr;
   int *face_elem = nullptr, *face_lface = nullptr, *elem_face = nullptr;
-  void *fstar = nullptr, *grad = nullptr;
+  void *fstar = nullptr, *vflux = nullptr;  // face fluxes; NS physical viscous flux
   double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
   unsigned *status = nullptr;
   unsigned long long *stab = nullptr;
@@ -172,15 +172,16 @@ struct DeviceGuard {
 
 bool pick_order_kernels(thx_operator_s *h, int vk) {
   const bool ns = h->ns;
+  const bool bl = h->blend;
 #define THX_PICK(P, D, NN)                                                  \
   if (h->dim == D && h->N == NN) {                                          \
     auto k = order_kernels_##P##_##D##_##NN();                              \
     if (P == 0) {                                                           \
-      h->vol64 = reinterpret_cast<VolLaunch<double>>(k.vol[vk][ns ? 1 : 0]); \
+      h->vol64 = reinterpret_cast<VolLaunch<double>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad64 = reinterpret_cast<GradLaunch<double>>(k.grad);             \
       h->blend64 = reinterpret_cast<BlendLaunch<double>>(k.blend);          \
     } else {                                                                \
-      h->vol32 = reinterpret_cast<VolLaunch<float>>(k.vol[vk][ns ? 1 : 0]); \
+      h->vol32 = reinterpret_cast<VolLaunch<float>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad32 = reinterpret_cast<GradLaunch<float>>(k.grad);              \
       h->blend32 = reinterpret_cast<BlendLaunch<float>>(k.blend);           \
     }                                                                       \
@@ -354,12 +355,12 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h)
     float *p;
     if ((st = dev_alloc(&p, fsz, A))) return st;
     h->fstar = p;
-    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * h->neq * h->L, A))) return st; h->grad = p; }
+    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * (h->neq - 1) * h->L, A))) return st; h->vflux = p; }
   } else {
     double *p;
     if ((st = dev_alloc(&p, fsz, A))) return st;
     h->fstar = p;
-    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * h->neq * h->L, A))) return st; h->grad = p; }
+    if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * (h->neq - 1) * h->L, A))) return st; h->vflux = p; }
   }
   if ((st = dev_alloc(&h->status, 1, A))) return st;
   if ((st = dev_alloc(&h->stab, 3, A))) return st;
@@ -473,10 +474,10 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     if ((ce = blendk(h, tag)(b, s)) != cudaSuccess) return THX_ERR_CUDA;
   }
   if (ev) cudaEventRecord(ev[1], s);
-  R *gradp = reinterpret_cast<R *>(h->grad);
+  R *vfl = reinterpret_cast<R *>(h->vflux);
   if (h->ns) {
     GradArgs<R> a;
-    a.u = u; a.grad = gradp; a.ne = h->ne;
+    a.u = u; a.vflux = vfl; a.ne = h->ne;
     a.jac = G.jac; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
     a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
     a.elem_face = h->elem_face; a.face_elem = h->face_elem; a.face_lface = h->face_lface;
@@ -492,7 +493,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     a.u = u; a.ne = h->ne; a.nf = h->nf; a.N = h->N;
     a.face_elem = h->face_elem; a.face_lface = h->face_lface;
     a.normal = G.nrm; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
-    a.grad = gradp; a.fstar = fst; a.gas = g;
+    a.vflux = vfl; a.fstar = fst; a.gas = g;
     if ((ce = facek(h, tag)(a, s)) != cudaSuccess) return THX_ERR_CUDA;
   }
   if (ev) cudaEventRecord(ev[3], s);
@@ -503,7 +504,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
     a.elem_face = h->elem_face; a.fstar = fst;
     a.wm = G.wm; a.wp = G.wp; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
-    a.grad = gradp;
+    a.vflux = vfl;
     a.alpha = h->blend ? h->alpha : nullptr;
     for (int d = 0; d < 3; ++d) { a.sub[d] = G.sub[d]; a.sub_es[d] = h->lay.sub_es[d]; }
     a.fv_flux = h->cfg.fv_flux;

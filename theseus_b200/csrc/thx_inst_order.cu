@@ -19,14 +19,22 @@ namespace thx {
 THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   using R = THX_RT(THX_PREC);
   THX_TYPE(THX_PREC) k;
-  k.vol[VOL_CHANDRASHEKAR][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, false>;
-  k.vol[VOL_CHANDRASHEKAR][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, true>;
-  k.vol[VOL_RANOCHA][0] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, false>;
-  k.vol[VOL_RANOCHA][1] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, true>;
-  k.vol[VOL_PIROZZOLI][0] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, false>;
-  k.vol[VOL_PIROZZOLI][1] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, true>;
-  k.vol[VOL_CENTRAL][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false>;
-  k.vol[VOL_CENTRAL][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true>;
+  k.vol[VOL_CHANDRASHEKAR][0][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, false, false>;
+  k.vol[VOL_CHANDRASHEKAR][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, false, true>;
+  k.vol[VOL_CHANDRASHEKAR][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, true, false>;
+  k.vol[VOL_CHANDRASHEKAR][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR, true, true>;
+  k.vol[VOL_RANOCHA][0][0] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, false, false>;
+  k.vol[VOL_RANOCHA][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, false, true>;
+  k.vol[VOL_RANOCHA][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, true, false>;
+  k.vol[VOL_RANOCHA][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_RANOCHA, true, true>;
+  k.vol[VOL_PIROZZOLI][0][0] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, false, false>;
+  k.vol[VOL_PIROZZOLI][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, false, true>;
+  k.vol[VOL_PIROZZOLI][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, true, false>;
+  k.vol[VOL_PIROZZOLI][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_PIROZZOLI, true, true>;
+  k.vol[VOL_CENTRAL][0][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false, false>;
+  k.vol[VOL_CENTRAL][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false, true>;
+  k.vol[VOL_CENTRAL][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, false>;
+  k.vol[VOL_CENTRAL][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, true>;
   k.grad = &launch_grad<R, THX_DIM, THX_N>;
   k.blend = &launch_blend<R, THX_DIM, THX_N>;
   return k;

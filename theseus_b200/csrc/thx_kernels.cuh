@@ -2,7 +2,8 @@
 //
 // Layouts (all in HBM, R = double or float):
 //   state / rate     u[eq][elem][node]      (MFEM byNODES L-vector, node lexicographic)
-//   gradients        g[c][eq][elem][node]   (primitive gradients, NS only)
+//   viscous flux     fv[d][eq-1][elem][node] (physical viscous flux, NS only;
+//                    its mass row is identically zero and is not stored)
 //   face fluxes      fs[face][eq][fp]       (unweighted F*, inviscid minus viscous)
 //   geometry         jac[e*jac_es + n*jac_ns], metric block of DIM*DIM per node
 //                    at met[e*met_es + n*met_ns]; strides are 0 where the host
@@ -10,7 +11,8 @@
 //
 // Kernel structure per right-hand side:
 //   NS only : grad_kernel   element-local BR1 gradient of entropy variables with
-//             the interior-face lift, converted to primitive gradients.
+//             the interior-face lift, converted to primitive gradients and on to
+//             the physical viscous flux, which is what the other kernels read.
 //   always  : face_kernel   one thread per face point: F*(u-,u+,n) (- n.avg(F_v)).
 //   always  : volume_kernel one CTA per EPB elements: flux differencing with every
 //             symmetric pair evaluated once, optional subcell-FV blend, viscous
@@ -94,7 +96,7 @@ struct VolArgs {
   const R *fstar;         // [f][eq][fp]
   const R *wm, *wp;       // lift weights
   long long w_fs, w_ps;
-  const R *grad;          // NS primitive gradients
+  const R *vflux;         // NS physical viscous flux [dir][eq-1][elem][node]
   const double *alpha;    // per-element blending coefficient or nullptr
   const R *sub[3];        // subcell metrics (reference layout), element stride sub_es
   long long sub_es[3];
@@ -124,19 +126,24 @@ __device__ __noinline__ void surface_flux_rt(int kind, const GasT<R> &g, const R
   }
 }
 
-template <typename R, int DIM, int N, int VOL, bool NS>
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
 volume_kernel(const VolArgs<R> a) {
   using S = Shape<DIM, N>;
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = S::NPRIM, PAIRS = S::PAIRS;
   constexpr int MB = DIM * DIM;
+  constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // [ops | prim | pair fluxes | state (NEEDQ) | metric]; the viscous flux of the
+  // NS phase reuses the prim + pair-flux region, the FV rate the pair fluxes.
   R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded)
   R *sPrim = sOps + S::OPS;                               // [EPB][NPRIM][ND]
-  R *sQ = sPrim + EPB * NPRIM * ND;                       // [EPB][NEQ][ND]
-  R *sMet = sQ + EPB * NEQ * ND;                          // [EPB][ND][MB]
-  R *sFB = sMet + EPB * ND * MB;                          // [EPB][PAIRS][NEQ] (aliased by FV rate)
-  R *sFv = sFB + EPB * PAIRS * NEQ;                       // [EPB][DIM][NEQ][ND] (NS)
+  R *sFB = sPrim + EPB * NPRIM * ND;                      // [EPB][PAIRS][NEQ]
+  R *sQ = sFB + EPB * PAIRS * NEQ;                        // [EPB][NEQ][ND] if NEEDQ
+  R *sMet = sQ + (NEEDQ ? EPB * NEQ * ND : 0);            // per node or once per element
+  R *sFv = sPrim;                                         // [EPB][DIM][NEQ-1][ND] (NS)
+  const int mns = a.met_ns != 0 ? MB : 0;                 // metric node stride in smem
+  const int mbk = a.met_ns != 0 ? ND * MB : MB;           // metric element block in smem
 
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * EPB;
@@ -158,12 +165,16 @@ volume_kernel(const VolArgs<R> a) {
     node_prims<R, DIM, VOL>(a.gas, q, pr);
 #pragma unroll
     for (int k = 0; k < NPRIM; ++k) sPrim[(el * NPRIM + k) * ND + n] = pr[k];
+    if (NEEDQ) {
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+      for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+    }
     if (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))) atomicOr(a.status, STATUS_NONPOSITIVE);
-    const R *mp = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
+    if (mns != 0 || n == 0) {
+      const R *mp = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
 #pragma unroll
-    for (int k = 0; k < MB; ++k) sMet[(el * ND + n) * MB + k] = mp[k];
+      for (int k = 0; k < MB; ++k) sMet[el * mbk + n * mns + k] = mp[k];
+    }
   }
   __syncthreads();
 
@@ -191,7 +202,7 @@ volume_kernel(const VolArgs<R> a) {
       }
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
-        met[d] = R(0.5) * (sMet[(pel * ND + na) * MB + dir * DIM + d] + sMet[(pel * ND + nb) * MB + dir * DIM + d]);
+        met[d] = R(0.5) * (sMet[pel * mbk + na * mns + dir * DIM + d] + sMet[pel * mbk + nb * mns + dir * DIM + d]);
       if (VOL == VOL_CHANDRASHEKAR) vol_chandrashekar<R, DIM>(a.gas, A, B, met, F);
       else if (VOL == VOL_RANOCHA) vol_ranocha<R, DIM>(a.gas, A, B, met, F);
       else if (VOL == VOL_PIROZZOLI) vol_pirozzoli<R, DIM>(a.gas, A, B, met, F);
@@ -236,7 +247,7 @@ volume_kernel(const VolArgs<R> a) {
 
   // subcell finite-volume blend (include/DGSEMIntegrator.hpp:338-483,
   // include/EulerOperator_impl.hpp:134-152)
-  if (a.alpha != nullptr) {
+  if (BLEND && a.alpha != nullptr) {
     bool any = false;
     for (int k = 0; k < EPB; ++k)
       if (e0 + k < a.ne && a.alpha[e0 + k] > 1e-16) any = true;
@@ -302,32 +313,33 @@ volume_kernel(const VolArgs<R> a) {
 
   if (NS) {
     // contravariant viscous flux per node (include/DGSEMIntegrator.hpp:486-524)
+    // from the physical viscous flux that grad_kernel stored; the mass row of
+    // the viscous flux is zero and is not stored.
+    constexpr int NV = NEQ - 1;
     if (active) {
-      R q[NEQ], dp[DIM * NEQ], vf[NEQ * DIM];
+      R vf[NV * DIM];
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) q[k] = sQ[(el * NEQ + k) * ND + n];
+      for (int pd = 0; pd < DIM; ++pd)
 #pragma unroll
-      for (int cc = 0; cc < DIM; ++cc)
-#pragma unroll
-        for (int k = 0; k < NEQ; ++k) dp[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + (long long)e * ND + n];
-      viscous_flux<R, DIM>(a.gas, q, dp, vf);
-      const R *row = sMet + (el * ND + n) * MB;
+        for (int k = 0; k < NV; ++k)
+          vf[k * DIM + pd] = a.vflux[((long long)pd * NV + k) * L + (long long)e * ND + n];
+      const R *row = sMet + el * mbk + n * mns;
 #pragma unroll
       for (int dir = 0; dir < DIM; ++dir)
 #pragma unroll
-        for (int k = 0; k < NEQ; ++k) {
+        for (int k = 0; k < NV; ++k) {
           R f = R(0);
 #pragma unroll
           for (int pd = 0; pd < DIM; ++pd) f += row[dir * DIM + pd] * vf[k * DIM + pd];
-          sFv[((el * DIM + dir) * NEQ + k) * ND + n] = f;
+          sFv[((el * DIM + dir) * NV + k) * ND + n] = f;
         }
     }
     __syncthreads();
     // weak-form divergence with Dhat (include/DGSEMIntegrator.hpp:526-622)
     if (active) {
-      R dv[NEQ];
+      R dv[NV];
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) dv[k] = R(0);
+      for (int k = 0; k < NV; ++k) dv[k] = R(0);
 #pragma unroll
       for (int dir = 0; dir < DIM; ++dir) {
         const int me = c[dir];
@@ -337,12 +349,12 @@ volume_kernel(const VolArgs<R> a) {
           const int s = line_node<DIM, N>(dir, line, l);
           const R co = sDh[me * N + l];
 #pragma unroll
-          for (int k = 0; k < NEQ; ++k) dv[k] += co * sFv[((el * DIM + dir) * NEQ + k) * ND + s];
+          for (int k = 0; k < NV; ++k) dv[k] += co * sFv[((el * DIM + dir) * NV + k) * ND + s];
         }
       }
       const R sc = R(1) / J;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) du[k] += sc * dv[k];
+      for (int k = 0; k < NV; ++k) du[1 + k] += sc * dv[k];
     }
   }
 
@@ -410,7 +422,7 @@ struct FaceArgs {
   const int *face_elem, *face_lface;
   const R *normal;
   long long n_fs, n_ps;
-  const R *grad;
+  const R *vflux;
   R *fstar;
   GasT<R> gas;
 };
@@ -436,21 +448,17 @@ __global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
   for (int d = 0; d < DIM; ++d) nrm[d] = np[d];
   surface_flux<R, DIM, SURF>(a.gas, qm, qp, nrm, F);
   if (NS) {
-    // include/DGSEMIntegrator.hpp:261-316
-    R gm[DIM * NEQ], gp[DIM * NEQ], vm[NEQ * DIM], vp[NEQ * DIM];
+    // include/DGSEMIntegrator.hpp:261-316: F* -= n . avg(F_v), with the physical
+    // viscous flux of both traces as stored by grad_kernel (mass row zero)
+    constexpr int NV = NEQ - 1;
 #pragma unroll
-    for (int cc = 0; cc < DIM; ++cc)
+    for (int k = 0; k < NV; ++k)
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) {
-        gm[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + im];
-        gp[cc * NEQ + k] = a.grad[((long long)cc * NEQ + k) * L + ip];
+      for (int d = 0; d < DIM; ++d) {
+        const R vm = a.vflux[((long long)d * NV + k) * L + im];
+        const R vp = a.vflux[((long long)d * NV + k) * L + ip];
+        F[1 + k] -= nrm[d] * (R(0.5) * (vm + vp));
       }
-    viscous_flux<R, DIM>(a.gas, qm, gm, vm);
-    viscous_flux<R, DIM>(a.gas, qp, gp, vp);
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k)
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) F[k] -= nrm[d] * (R(0.5) * (vm[k * DIM + d] + vp[k * DIM + d]));
   }
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) a.fstar[((long long)f * NEQ + k) * nfp + fp] = F[k];
@@ -460,7 +468,7 @@ __global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
 template <typename R>
 struct GradArgs {
   const R *u;
-  R *grad;
+  R *vflux;   // physical viscous flux [dir][eq-1][elem][node] (mass row omitted)
   int ne;
   const R *jac;
   long long jac_es, jac_ns;
@@ -575,13 +583,19 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const Grad
         for (int k = 0; k < NEQ; ++k) g[cc][k] += acc[cc][k];
     }
   }
+  // entropy gradient -> primitive gradient, then the physical viscous flux
+  // (include/NavierStokesFlux.hpp:160-290) that the face and volume kernels use
+  R dp[DIM * NEQ];
 #pragma unroll
-  for (int cc = 0; cc < DIM; ++cc) {
-    R dP[NEQ];
-    grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dP);
+  for (int cc = 0; cc < DIM; ++cc) grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dp + cc * NEQ);
+  R vf[NEQ * DIM];
+  viscous_flux<R, DIM>(a.gas, q, dp, vf);
+  constexpr int NV = NEQ - 1;
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) a.grad[((long long)cc * NEQ + k) * L + (long long)e * ND + n] = dP[k];
-  }
+  for (int d = 0; d < DIM; ++d)
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+      a.vflux[((long long)d * NV + k) * L + (long long)e * ND + n] = vf[(1 + k) * DIM + d];
 }
 
 // ---------------------------------------------------------------------------

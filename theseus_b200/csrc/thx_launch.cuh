@@ -13,24 +13,29 @@ template <typename R> using FaceLaunch = cudaError_t (*)(const FaceArgs<R> &, cu
 template <typename R> using GradLaunch = cudaError_t (*)(const GradArgs<R> &, cudaStream_t, int prepare);
 template <typename R> using BlendLaunch = cudaError_t (*)(const BlendArgs<R> &, cudaStream_t);
 
-template <typename R, int DIM, int N, bool NS>
-constexpr size_t volume_smem_bytes() {
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+constexpr size_t volume_smem_bytes(bool metric_per_node) {
   using S = Shape<DIM, N>;
-  return sizeof(R) * (S::OPS + (size_t)S::EPB * (S::NPRIM * S::ND + S::NEQ * S::ND + S::ND * DIM * DIM +
-                                             S::PAIRS * S::NEQ + (NS ? DIM * S::NEQ * S::ND : 0)));
+  constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
+  constexpr size_t region = (size_t)S::EPB * (S::NPRIM * S::ND + S::PAIRS * S::NEQ);
+  constexpr size_t visc = NS ? (size_t)S::EPB * DIM * (S::NEQ - 1) * S::ND : 0;
+  const size_t met = (size_t)S::EPB * (metric_per_node ? S::ND * DIM * DIM : DIM * DIM);
+  return sizeof(R) * (S::OPS + (region > visc ? region : visc) +
+                      (NEEDQ ? (size_t)S::EPB * S::NEQ * S::ND : 0) + met);
 }
 
-template <typename R, int DIM, int N, int VOL, bool NS>
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 cudaError_t launch_volume(const VolArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
   static_assert(S::PAIRS >= S::ND, "subcell FV rate aliases the pair-flux buffer");
-  constexpr size_t smem = volume_smem_bytes<R, DIM, N, NS>();
   if (prepare)
-    return cudaFuncSetAttribute(volume_kernel<R, DIM, N, VOL, NS>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaFuncSetAttribute(volume_kernel<R, DIM, N, VOL, NS, BLEND>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)volume_smem_bytes<R, DIM, N, VOL, NS, BLEND>(true));
   if (a.ne <= 0) return cudaSuccess;
+  const size_t smem = volume_smem_bytes<R, DIM, N, VOL, NS, BLEND>(a.met_ns != 0);
   const int grid = (a.ne + S::EPB - 1) / S::EPB;
-  volume_kernel<R, DIM, N, VOL, NS><<<grid, S::THREADS, smem, s>>>(a);
+  volume_kernel<R, DIM, N, VOL, NS, BLEND><<<grid, S::THREADS, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -66,8 +71,8 @@ cudaError_t launch_blend(const BlendArgs<R> &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-struct OrderKernels0 { VolLaunch<double> vol[4][2]; GradLaunch<double> grad; BlendLaunch<double> blend; };
-struct OrderKernels1 { VolLaunch<float> vol[4][2]; GradLaunch<float> grad; BlendLaunch<float> blend; };
+struct OrderKernels0 { VolLaunch<double> vol[4][2][2]; GradLaunch<double> grad; BlendLaunch<double> blend; };
+struct OrderKernels1 { VolLaunch<float> vol[4][2][2]; GradLaunch<float> grad; BlendLaunch<float> blend; };
 struct FaceKernels0 { FaceLaunch<double> face[6][2]; };
 struct FaceKernels1 { FaceLaunch<float> face[6][2]; };
 
