@@ -139,7 +139,9 @@ volume_kernel(const VolArgs<R> a) {
   R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded)
   R *sPrim = sOps + S::OPS;                               // [EPB][NPRIM][ND]
   R *sFB = sPrim + EPB * NPRIM * ND;                      // [EPB][PAIRS][NEQ]
-  R *sQ = sFB + EPB * PAIRS * NEQ;                        // [EPB][NEQ][ND] if NEEDQ
+  constexpr int REGION = EPB * (NPRIM * ND + PAIRS * NEQ);
+  constexpr int VISC = NS ? EPB * DIM * (NEQ - 1) * ND : 0;
+  R *sQ = sPrim + (REGION > VISC ? REGION : VISC);        // [EPB][NEQ][ND] if NEEDQ
   R *sMet = sQ + (NEEDQ ? EPB * NEQ * ND : 0);            // per node or once per element
   R *sFv = sPrim;                                         // [EPB][DIM][NEQ-1][ND] (NS)
   const int mns = a.met_ns != 0 ? MB : 0;                 // metric node stride in smem
