@@ -57,7 +57,8 @@ typedef enum {
   THX_FLUX_HLL = 3,           /* include/HLLFlux.hpp:53-116 */
   THX_FLUX_LLF = 4,           /* include/LaxFriedrichsFlux.hpp:54-77 */
   THX_FLUX_ROE = 5,           /* include/RoeFlux.hpp:42-149 */
-  THX_FLUX_COUNT = 6
+  THX_FLUX_LTEEC = 6,         /* include/LTEECFlux.hpp:11-99 (LTE Helmholtz gas only) */
+  THX_FLUX_COUNT = 7
 } thx_flux;
 
 typedef enum {
@@ -95,6 +96,9 @@ typedef struct {
   double alpha_min;          /* 0.001 */
   double sharpness;          /* 9.21024 (include/RHSOperator.hpp:33) */
   double modal_threshold;    /* <= 0: 0.5*10^(-1.8 p^0.25) (include/RHSOperator.hpp:64) */
+  double state_offset[5];    /* FP32-mixed only: constant reference state u_ref (rho, rho*u_0..,
+                                rho*E) subtracted from the FP32 working copy; pressure enters
+                                the momentum fluxes as p - p(u_ref).  Zeros: plain FP32 copy. */
 } thx_config;
 
 /* Mesh and geometric factors, in the layout of the reference's device cache
@@ -127,6 +131,28 @@ typedef struct {
   const double *face_wminus;
   const double *face_wplus;
 } thx_geometry;
+
+/* LTE Helmholtz gas table in the reference's six-plane layout
+ * (include/LTEHelmholtzTable.hpp:13-35, include/LTETable.hpp:56-71), host
+ * pointers: planes[p][j][i] with p = H, H_rho, H_T, H_rhoT, mu, lambda (physical
+ * derivatives), i the density and j the temperature sample; inverse[j][i] is the
+ * temperature guess at (rho_grid[i], e_grid[j]). */
+typedef struct {
+  int32_t nx;                /* density samples */
+  int32_t ny;                /* temperature (and energy) samples */
+  const double *rho_grid;    /* [nx], increasing */
+  const double *T_grid;      /* [ny], increasing */
+  const double *e_grid;      /* [ny], increasing */
+  const double *planes;      /* [6][ny][nx] */
+  const double *inverse;     /* [ny][nx] */
+} thx_lte_table;
+
+/* Synthetic ideal-dissociating gas (Lighthill): molecular gas constant R,
+ * characteristic density rho_d, dissociation temperature theta_d; transport
+ * mu = mu0 (T/T0)^0.7, lambda = mu 4R(1+alpha)/Pr. */
+typedef struct {
+  double R, rho_d, theta_d, mu0, T0, Pr;
+} thx_idg_params;
 
 typedef struct thx_operator_s *thx_handle;
 
@@ -167,11 +193,38 @@ int thx_lgl(int np, double *x, double *w);
  * MakeRHSOperator (include/SimFactory_impl.hpp:63-488). */
 int thx_create(const thx_geometry *geom, const thx_config *cfg,
                thx_handle *out);
+
+/* The same operator on the LTE Helmholtz gas (include/LTEGasModel.hpp:339
+ * LTEHelmholtzGas, include/LTEHelmholtzGasEOS.hpp:10-172) with the LTEEC flux
+ * on volume and faces (cfg->volume_flux == cfg->surface_flux == THX_FLUX_LTEEC),
+ * FP64, no blending; Euler or Navier-Stokes (transport from the table's mu and
+ * lambda planes, include/LTETransport.hpp:19-66).  The table (host pointers)
+ * is copied to the device.  Every right-hand side recovers T(rho, e) once per
+ * node by the reference's Newton iteration (include/LTEHelmholtzEOS.hpp:158-223);
+ * a failed recovery sets THX_STATUS_EOS.  Replaces MakeRHSOperator with the
+ * LTE gas selected (include/SimFactory_impl.hpp:63-488). */
+int thx_create_lte(const thx_geometry *geom, const thx_config *cfg,
+                   const thx_lte_table *table, thx_handle *out);
+
+/* Energy grid and inverse table of a forward Helmholtz table: e_grid[ny]
+ * uniform over [e_min - pad, e_max + pad], inverse[j][i] = T(rho_i, e_j) by
+ * bisection -- the part of HelmholtzTable::Build that does not need PLATO
+ * (include/LTEHelmholtzTableBuilder.hpp:131-218).  Host arrays. */
+int thx_lte_inverse_table(int nx, int ny, const double *rho_grid, const double *T_grid,
+                          const double *planes, double *e_grid, double *inverse);
+
+/* Forward planes of the synthetic ideal-dissociating-gas table on log-spaced
+ * grids (include/LTETable.hpp:95-103): rho_grid[nx] over 10^[lr0, lr1],
+ * T_grid[ny] over 10^[lt0, lt1], planes[6][ny][nx].  Host arrays. */
+int thx_lte_idg_table(const thx_idg_params *gas, int nx, int ny, double lr0, double lr1,
+                      double lt0, double lt1, double *rho_grid, double *T_grid, double *planes);
+
 int thx_destroy(thx_handle h);
 
-/* dudt = L(u).  u and dudt are device L-vectors (byNODES).  For
- * THX_PRECISION_FP64 they hold double; for THX_PRECISION_FP32_MIXED they hold
- * float (the FP32 working copy).  Replaces RHSOperator<PhysicsT>::Mult
+/* dudt = L(u).  u and dudt are device FP64 L-vectors (byNODES) in both
+ * precisions; in THX_PRECISION_FP32_MIXED the state is narrowed to the FP32
+ * working copy (u - state_offset), the right-hand side is evaluated in FP32 and
+ * widened back.  Replaces RHSOperator<PhysicsT>::Mult
  * (include/RHSOperator_impl.hpp:719-793). */
 int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream);
 
@@ -195,8 +248,12 @@ int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev,
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out,
                     double *rates_out /* [3]: advective, surface, diffusive */);
 
-/* Device status word of the last evaluations (non-finite or non-positive
- * density/pressure seen).  Reading it synchronises the stream. */
+/* Device status word of the evaluations since the last read, a bitwise OR of
+ * THX_STATUS_* flags.  Reading it synchronises the stream and clears it. */
+#define THX_STATUS_NONPOSITIVE 1u  /* non-positive density or pressure seen */
+#define THX_STATUS_NONFINITE 2u    /* non-finite value seen */
+#define THX_STATUS_LAUNCH 4u       /* a kernel got too little shared memory and did nothing */
+#define THX_STATUS_EOS 8u          /* LTE temperature recovery failed or left the table */
 int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
 
 /* Diagnostics of the configured kernels (for roofline bookkeeping). */

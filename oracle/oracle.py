@@ -254,3 +254,85 @@ def ref_rhs(mesh, cfg, u, alpha=None):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+# ---- LTE Helmholtz gas ----------------------------------------------------
+class LteTableStruct(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("rho_grid", D), ("T_grid", D),
+                ("e_grid", D), ("planes", D), ("inverse", D)]
+
+
+class IdgParams(C.Structure):
+    _fields_ = [("R", C.c_double), ("rho_d", C.c_double), ("theta_d", C.c_double),
+                ("mu0", C.c_double), ("T0", C.c_double), ("Pr", C.c_double)]
+
+
+# Config 4's table: O2-like ideal dissociating gas on 256 x 512 log-spaced samples
+IDG_O2 = dict(R=8.314462618 / 0.0319988, rho_d=1.5e5, theta_d=59500.0, mu0=1.9e-5, T0=273.15,
+              Pr=0.71)
+GRID_CONFIG4 = dict(nx=256, ny=512, log_rho=(-6.0, 1.0), log_T=(2.3, 4.3))
+
+
+class LteTable:
+    """Oracle-built LTE table (forward planes + inverse table), kept alive for ctypes."""
+
+    def __init__(self, nx, ny, log_rho, log_T, params=None):
+        p = IdgParams(**(params or IDG_O2))
+        self.params = p
+        self.nx, self.ny = nx, ny
+        self.rho = np.zeros(nx)
+        self.T = np.zeros(ny)
+        self.planes = np.zeros((6, ny, nx))
+        self.e = np.zeros(ny)
+        self.inv = np.zeros((ny, nx))
+        _check(lib().orc_lte_idg_table(C.byref(p), nx, ny, C.c_double(log_rho[0]), C.c_double(log_rho[1]),
+                                       C.c_double(log_T[0]), C.c_double(log_T[1]), _dp(self.rho),
+                                       _dp(self.T), _dp(self.planes)), "orc_lte_idg_table")
+        _check(lib().orc_lte_inverse_table(nx, ny, _dp(self.rho), _dp(self.T), _dp(self.planes),
+                                           _dp(self.e), _dp(self.inv)), "orc_lte_inverse_table")
+
+    def struct(self):
+        s = LteTableStruct(self.nx, self.ny, _dp(self.rho), _dp(self.T), _dp(self.e),
+                           _dp(self.planes), _dp(self.inv))
+        self._s = s
+        return s
+
+
+def lte_point(table, rho, T, use_ref=False):
+    out = np.zeros(7)
+    fn = ref().ref_lte_point if use_ref else lib().orc_lte_point
+    _check(fn(C.byref(table.struct()), C.c_double(rho), C.c_double(T), _dp(out)), "lte_point")
+    return out
+
+
+def lte_temperature(table, rho, e, use_ref=False):
+    T, st = C.c_double(), C.c_int()
+    fn = ref().ref_lte_temperature if use_ref else lib().orc_lte_temperature
+    fn(C.byref(table.struct()), C.c_double(rho), C.c_double(e), C.byref(T), C.byref(st))
+    return T.value, st.value
+
+
+def lte_flux(table, cfg, dim, face, q1, q2, d1, d2, use_ref=False):
+    F = np.zeros(dim + 2)
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (q1, q2, d1, d2)]
+    if use_ref:
+        st = ref().ref_lte_flux(C.byref(table.struct()), C.byref(cfg), int(dim), int(face),
+                                *[_dp(a) for a in arrs], _dp(F))
+    else:
+        st = lib().orc_lte_flux(C.byref(table.struct()), int(dim), int(face), *[_dp(a) for a in arrs], _dp(F))
+    _check(st, "lte_flux")
+    return F
+
+
+def rhs_lte(mesh, cfg, table, u, nthreads=1, use_ref=False):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    du = np.zeros_like(u)
+    if use_ref:
+        x, w, Dm, Dh, Dh2 = operators(mesh.order)
+        st = ref().ref_rhs_lte(C.byref(mesh.struct()), C.byref(cfg), C.byref(table.struct()), _dp(Dm),
+                               _dp(Dh), _dp(Dh2), _dp(w), _dp(u), _dp(du))
+    else:
+        st = lib().orc_rhs_lte(C.byref(mesh.struct()), C.byref(cfg), C.byref(table.struct()), _dp(u),
+                               _dp(du), int(nthreads))
+    _check(st, "rhs_lte")
+    return du

@@ -14,6 +14,8 @@
 #include "RoeFlux.hpp"
 #include "HLLFlux.hpp"
 #include "LaxFriedrichsFlux.hpp"
+#include "LTEGasModel.hpp"
+#include "LTEECFlux.hpp"
 
 #include "theseus_b200.h"
 
@@ -54,14 +56,42 @@ struct PairFlux {
 };
 
 // Duck-typed context, the pattern of tests/viscous_volume_tests.cpp:9-17.
-struct Ctx {
+template <class GasT, class FluxT>
+struct CtxT {
   int dim, num_equations, ndof_scalar_el, Np_x, Np_y, Np_z, num_face_points;
   bool axisymmetric = false;
-  Gas gas;
-  PairFlux iflux;
+  GasT gas;
+  FluxT iflux;
   const double *D_d, *Dhat_d, *Dhat2_d, *subcell_weights_d;
   int iface_idx(int side, int fp, int eq) const {
     return (side * num_equations + eq) * num_face_points + fp;
+  }
+};
+using Ctx = CtxT<Gas, PairFlux>;
+using LteGas = Theseus::LTEHelmholtzGas;
+using LteCtx = CtxT<LteGas, Theseus::LTEECFlux::InviscidFlux>;
+
+// The reference's table data from the oracle's arrays.
+struct LteData {
+  Theseus::HelmholtzTable::Data data;
+  Theseus::HelmholtzTable::Layout layout;
+  explicit LteData(const thx_lte_table *t) {
+    layout.nx = t->nx;
+    layout.ny = t->ny;
+    auto fill = [](mfem::Vector &v, const double *src, int n) {
+      v.SetSize(n);
+      for (int i = 0; i < n; ++i) v[i] = src[i];
+    };
+    fill(data.rho_grid, t->rho_grid, t->nx);
+    fill(data.T_grid, t->T_grid, t->ny);
+    fill(data.e_grid, t->e_grid, t->ny);
+    fill(data.lte_table, t->planes, 6 * t->nx * t->ny);
+    fill(data.inv_table, t->inverse, t->nx * t->ny);
+  }
+  LteGas gas(const thx_config &c, int dim) const {
+    Theseus::PhysicsConstants phys(c.gamma, c.Pr, c.R_gas, c.mu, c.mu0);
+    phys.mu_bulk = c.mu_bulk;
+    return LteGas(phys, Theseus::StateLayout(dim, 1), Theseus::HelmholtzTable::HostView(data, layout));
   }
 };
 
@@ -90,65 +120,21 @@ int trace_node(int dim, int N, int lf, int fp) {
 
 }  // namespace
 
-extern "C" {
-
-int ref_volume_flux(int flux, const thx_config *cfg, int dim, const double *q1, const double *q2,
-                    const double *m1, const double *m2, double *F) {
-  Gas g = make_gas(*cfg, dim);
-  PairFlux pf;
-  pf.vol = flux;
-  pf.ComputeVolumeFlux(g, q1, q2, m1, m2, F);
-  return 0;
-}
-
-int ref_face_flux(int flux, const thx_config *cfg, int dim, const double *qm, const double *qp,
-                  const double *n, double *F) {
-  Gas g = make_gas(*cfg, dim);
-  PairFlux pf;
-  pf.surf = flux;
-  pf.ComputeFaceFlux(g, qm, qp, n, F);
-  return 0;
-}
-
-int ref_entropy_vars(const thx_config *cfg, int dim, const double *q, double *w) {
-  Gas g = make_gas(*cfg, dim);
-  Theseus::PointStateView S{q};
-  Theseus::PointStateViewRW E{w};
-  g.entropy_state(S, E);
-  return 0;
-}
-
-int ref_viscous_flux(const thx_config *cfg, int dim, const double *q, const double *dprim,
-                     double *vf_out) {
-  Gas g = make_gas(*cfg, dim);
-  double vf[Theseus::MAXEQ][Theseus::MAXDIM];
-  const int neq = dim + 2;
-  Theseus::NavierStokesFlux::ComputeViscousFluxKernel(g, q, dprim, dprim + neq,
-                                                     dim > 2 ? dprim + 2 * neq : dprim, vf);
-  for (int e = 0; e < neq; ++e)
-    for (int d = 0; d < dim; ++d) vf_out[e * dim + d] = vf[e][d];
-  return 0;
-}
-
+namespace {
 // Full RHS on a byNODES L-vector, driving the reference point kernels.
 //  D, Dhat, Dhat2: [i*Np+l] operator arrays; w: LGL weights on [0,1]
 //  alpha: per-element blending coefficient (NULL = no blending)
 //  sub_xi/eta/zeta: subcell metrics in the reference layout
-int ref_rhs(const thx_geometry *geo, const thx_config *cfg, const double *D, const double *Dhat,
-            const double *Dhat2, const double *w, const double *alpha, const double *sub_xi,
-            const double *sub_eta, const double *sub_zeta, const double *u, double *dudt) {
+template <class C>
+int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_config *cfg,
+             const double *alpha, const double *sub_xi, const double *sub_eta,
+             const double *sub_zeta, const double *u, double *dudt) {
   const int dim = geo->dim, N = geo->order + 1;
   const int nd = dim == 2 ? N * N : N * N * N;
   const int nfp = dim == 2 ? N : N * N;
   const int neq = dim + 2, ne = geo->num_elements, nf = geo->num_faces;
   const size_t L = (size_t)ne * nd;
   const bool ns = cfg->flow_model == THX_FLOW_NAVIER_STOKES;
-  Ctx ctx{dim, neq, nd, N, N, dim > 2 ? N : 1, nfp, false, make_gas(*cfg, dim), PairFlux{},
-          D, Dhat, Dhat2, w};
-  ctx.iflux.vol = cfg->volume_flux;
-  ctx.iflux.surf = cfg->surface_flux;
-  Ctx fvctx = ctx;
-  fvctx.iflux.surf = cfg->fv_flux;
 
   // E-vector [e][eq][node] (restr_v->Mult)
   std::vector<double> Ue((size_t)neq * L), dUe((size_t)neq * L, 0.0), dUfv((size_t)neq * nd);
@@ -288,6 +274,115 @@ int ref_rhs(const thx_geometry *geo, const thx_config *cfg, const double *D, con
   }
   for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += acc[i];
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_volume_flux(int flux, const thx_config *cfg, int dim, const double *q1, const double *q2,
+                    const double *m1, const double *m2, double *F) {
+  Gas g = make_gas(*cfg, dim);
+  PairFlux pf;
+  pf.vol = flux;
+  pf.ComputeVolumeFlux(g, q1, q2, m1, m2, F);
+  return 0;
+}
+
+int ref_face_flux(int flux, const thx_config *cfg, int dim, const double *qm, const double *qp,
+                  const double *n, double *F) {
+  Gas g = make_gas(*cfg, dim);
+  PairFlux pf;
+  pf.surf = flux;
+  pf.ComputeFaceFlux(g, qm, qp, n, F);
+  return 0;
+}
+
+int ref_entropy_vars(const thx_config *cfg, int dim, const double *q, double *w) {
+  Gas g = make_gas(*cfg, dim);
+  Theseus::PointStateView S{q};
+  Theseus::PointStateViewRW E{w};
+  g.entropy_state(S, E);
+  return 0;
+}
+
+int ref_viscous_flux(const thx_config *cfg, int dim, const double *q, const double *dprim,
+                     double *vf_out) {
+  Gas g = make_gas(*cfg, dim);
+  double vf[Theseus::MAXEQ][Theseus::MAXDIM];
+  const int neq = dim + 2;
+  Theseus::NavierStokesFlux::ComputeViscousFluxKernel(g, q, dprim, dprim + neq,
+                                                     dim > 2 ? dprim + 2 * neq : dprim, vf);
+  for (int e = 0; e < neq; ++e)
+    for (int d = 0; d < dim; ++d) vf_out[e * dim + d] = vf[e][d];
+  return 0;
+}
+
+int ref_rhs(const thx_geometry *geo, const thx_config *cfg, const double *D, const double *Dhat,
+            const double *Dhat2, const double *w, const double *alpha, const double *sub_xi,
+            const double *sub_eta, const double *sub_zeta, const double *u, double *dudt) {
+  const int dim = geo->dim, N = geo->order + 1;
+  const int nd = dim == 2 ? N * N : N * N * N;
+  const int nfp = dim == 2 ? N : N * N;
+  Ctx ctx{dim, dim + 2, nd, N, N, dim > 2 ? N : 1, nfp, false, make_gas(*cfg, dim), PairFlux{},
+          D, Dhat, Dhat2, w};
+  ctx.iflux.vol = cfg->volume_flux;
+  ctx.iflux.surf = cfg->surface_flux;
+  Ctx fvctx = ctx;
+  fvctx.iflux.surf = cfg->fv_flux;
+  return rhs_impl(ctx, fvctx, geo, cfg, alpha, sub_xi, sub_eta, sub_zeta, u, dudt);
+}
+
+// The same driver with the reference's LTE Helmholtz gas and LTEEC flux.
+int ref_rhs_lte(const thx_geometry *geo, const thx_config *cfg, const thx_lte_table *t,
+                const double *D, const double *Dhat, const double *Dhat2, const double *w,
+                const double *u, double *dudt) {
+  const int dim = geo->dim, N = geo->order + 1;
+  const int nd = dim == 2 ? N * N : N * N * N;
+  const int nfp = dim == 2 ? N : N * N;
+  LteData data(t);
+  LteCtx ctx{dim, dim + 2, nd, N, N, dim > 2 ? N : 1, nfp, false, data.gas(*cfg, dim),
+             Theseus::LTEECFlux::InviscidFlux{}, D, Dhat, Dhat2, w};
+  try {
+    return rhs_impl(ctx, ctx, geo, cfg, nullptr, nullptr, nullptr, nullptr, u, dudt);
+  } catch (const std::exception &) {
+    return THX_ERR_NUMERICS;
+  }
+}
+
+int ref_lte_point(const thx_lte_table *t, double rho, double T, double *out) {
+  LteData data(t);
+  const auto tables = Theseus::HelmholtzTable::HostView(data.data, data.layout);
+  const auto s = Theseus::HelmholtzEOS::At(tables, rho, T);
+  if (!s.valid) return THX_ERR_NUMERICS;
+  out[0] = s.pressure(); out[1] = s.energy(); out[2] = s.gibbs(); out[3] = s.cv();
+  out[4] = s.sound_speed_squared();
+  out[5] = s.transport<Theseus::HelmholtzTable::Layout::mu_idx>(tables);
+  out[6] = s.transport<Theseus::HelmholtzTable::Layout::lambda_idx>(tables);
+  return THX_OK;
+}
+
+int ref_lte_temperature(const thx_lte_table *t, double rho, double e, double *T, int *status) {
+  LteData data(t);
+  const auto tables = Theseus::HelmholtzTable::HostView(data.data, data.layout);
+  const auto r = Theseus::HelmholtzEOS::TemperatureFromEnergy(tables, rho, e);
+  *T = r.temperature;
+  *status = (int)r.status;
+  return THX_OK;
+}
+
+int ref_lte_flux(const thx_lte_table *t, const thx_config *cfg, int dim, int face,
+                 const double *q1, const double *q2, const double *d1, const double *d2,
+                 double *F) {
+  LteData data(t);
+  const LteGas gas = data.gas(*cfg, dim);
+  try {
+    if (face) Theseus::LTEECFlux::ComputeFaceFluxKernel(gas, q1, q2, d1, F);
+    else Theseus::LTEECFlux::ComputeVolumeFluxKernel(gas, q1, q2, d1, d2, F);
+  } catch (const std::exception &) {
+    return THX_ERR_NUMERICS;
+  }
+  return THX_OK;
 }
 
 }  // extern "C"

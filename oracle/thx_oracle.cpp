@@ -17,10 +17,13 @@
 #include "../include/theseus_b200.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
+
+#include "lte_oracle.h"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -37,7 +40,16 @@ struct Gas {
   int dim;
   double gamma, gm1, gm1_inv, R, cp, Pr_inv, mu, mu0, mu_bulk, T0, Ts;
   bool sutherland;
+  const lte::Table *lte = nullptr;       // LTE Helmholtz gas when set
+  std::atomic<int> *bad = nullptr;       // failed temperature recoveries
 };
+
+static inline lte::Eval lte_state(const Gas &g, const double *q) {
+  bool bad = false;
+  lte::Eval s = lte::evaluate_state(*g.lte, g.dim, q, &bad);
+  if (bad && g.bad) g.bad->fetch_add(1);
+  return s;
+}
 
 static Gas make_gas(const thx_config &c, int dim) {
   Gas g;
@@ -81,8 +93,9 @@ static inline double sound_speed(const Gas &g, const double *q) {
 static inline double temperature(const Gas &g, const double *q) {
   return pressure(g, q) / (q[0] * g.R);
 }
-// include/Transport.hpp:26-40
+// include/Transport.hpp:26-40; LTE: include/LTETransport.hpp:33-65 (table planes)
 static inline double viscosity(const Gas &g, const double *q) {
+  if (g.lte) return lte_state(g, q).transport(*g.lte, 4);
   if (g.sutherland) {
     const double T = temperature(g, q);
     const double Trel = T / g.T0;
@@ -93,20 +106,36 @@ static inline double viscosity(const Gas &g, const double *q) {
 }
 // include/Transport.hpp:50-57
 static inline double conductivity(const Gas &g, const double *q) {
+  if (g.lte) return lte_state(g, q).transport(*g.lte, 5);
   return viscosity(g, q) * g.cp * g.Pr_inv;
 }
 // include/EOS.hpp:159-173
 static inline void grad_temperature(const Gas &g, const double *q,
                                     const double *grho, const double *gp,
                                     double *gT) {
+  if (g.lte) {  // include/LTEHelmholtzGasEOS.hpp:133-142
+    for (int i = 0; i < g.dim; ++i) gT[i] = gp[i];
+    return;
+  }
   const double rho = q[0];
   const double pressor = pressure(g, q) / rho;
   const double cv = g.cp / g.gamma;
   const double fac = g.gm1_inv / (cv * rho);
   for (int i = 0; i < g.dim; ++i) gT[i] = fac * (gp[i] - pressor * grho[i]);
 }
-// include/EOS.hpp:206-234
+// include/EOS.hpp:206-234; LTE: include/LTEHelmholtzGasEOS.hpp:144-157
 static inline void entropy_vars(const Gas &g, const double *q, double *w) {
+  if (g.lte) {
+    const lte::Eval s = lte_state(g, q);
+    const double beta = 1 / s.T;
+    double m2 = 0.0;
+    for (int d = 0; d < g.dim; ++d) m2 += q[1 + d] * q[1 + d];
+    const double kinetic = (0.5 * m2 / q[0]) / q[0];
+    w[0] = beta * (s.gibbs() - kinetic);
+    for (int d = 0; d < g.dim; ++d) w[1 + d] = beta * (q[1 + d] / q[0]);
+    w[g.dim + 1] = -beta;
+    return;
+  }
   const double p = pressure(g, q);
   const double rho = q[0];
   const double s = std::log(p) - g.gamma * std::log(rho);
@@ -122,6 +151,14 @@ static inline void entropy_vars(const Gas &g, const double *q, double *w) {
 static inline void grad_entropy_to_prim(const Gas &g, const double *q,
                                         const double *dE, double *dP) {
   const int dim = g.dim, E = dim + 1;
+  if (g.lte) {
+    // include/LTEHelmholtzGasEOS.hpp:159-172: the energy slot holds grad T
+    const double t = lte_state(g, q).T;
+    dP[0] = 0.0;
+    for (int d = 0; d < dim; ++d) dP[1 + d] = t * dE[1 + d] + t * (q[1 + d] / q[0]) * dE[E];
+    dP[E] = t * t * dE[E];
+    return;
+  }
   const double ke = ke_density(g, q);
   const double p = pressure(g, q);
   const double rho = q[0];
@@ -588,8 +625,24 @@ typedef void (*VolFn)(const Gas &, const double *, const double *, const double 
                       const double *, double *);
 typedef void (*FaceFn)(const Gas &, const double *, const double *, const double *, double *);
 
+// LTEEC (include/LTEECFlux.hpp:86-99): volume form with the averaged metric,
+// face form with the Lax dissipation; needs the LTE Helmholtz gas.
+static void vol_lteec(const Gas &g, const double *q1, const double *q2, const double *m1,
+                      const double *m2, double *F) {
+  bool bad = false;
+  lte::lteec(*g.lte, g.dim, false, q1, q2, m1, m2, F, &bad);
+  if (bad && g.bad) g.bad->fetch_add(1);
+}
+static void face_lteec(const Gas &g, const double *q1, const double *q2, const double *n,
+                       double *F) {
+  bool bad = false;
+  lte::lteec(*g.lte, g.dim, true, q1, q2, n, n, F, &bad);
+  if (bad && g.bad) g.bad->fetch_add(1);
+}
+
 static VolFn vol_fn(int f) {
   switch (f) {
+    case THX_FLUX_LTEEC: return vol_lteec;
     case THX_FLUX_CHANDRASHEKAR: return vol_chandrashekar;
     case THX_FLUX_RANOCHA: return vol_ranocha;
     case THX_FLUX_PIROZZOLI: return vol_pirozzoli;
@@ -599,6 +652,7 @@ static VolFn vol_fn(int f) {
 }
 static FaceFn face_fn(int f) {
   switch (f) {
+    case THX_FLUX_LTEEC: return face_lteec;
     case THX_FLUX_CHANDRASHEKAR: return face_chandrashekar;
     case THX_FLUX_RANOCHA: return face_ranocha;
     case THX_FLUX_PIROZZOLI: return face_pirozzoli;
@@ -1555,6 +1609,66 @@ int orc_subcell_metrics(const thx_geometry *g, const thx_config *cfg, double *xi
   if (eta && !c.sub_eta.empty()) std::memcpy(eta, c.sub_eta.data(), sizeof(double) * c.sub_eta.size());
   if (zeta && !c.sub_zeta.empty()) std::memcpy(zeta, c.sub_zeta.data(), sizeof(double) * c.sub_zeta.size());
   return THX_OK;
+}
+
+// ---- LTE Helmholtz gas ------------------------------------------------------
+static lte::Table lte_view(const thx_lte_table *t) {
+  lte::Table v;
+  v.nx = t->nx; v.ny = t->ny; v.rho = t->rho_grid; v.T = t->T_grid; v.e = t->e_grid;
+  v.planes = t->planes; v.inv = t->inverse;
+  return v;
+}
+
+int orc_lte_idg_table(const thx_idg_params *p, int nx, int ny, double lr0, double lr1, double lt0,
+                      double lt1, double *rho, double *T, double *planes) {
+  if (!p || nx < 2 || ny < 2 || !rho || !T || !planes) return THX_ERR_INVALID_ARGUMENT;
+  lte::IDG g{p->R, p->rho_d, p->theta_d, p->mu0, p->T0, p->Pr};
+  lte::idg_table(g, nx, ny, lr0, lr1, lt0, lt1, rho, T, planes);
+  return THX_OK;
+}
+
+int orc_lte_inverse_table(int nx, int ny, const double *rho, const double *T, const double *planes,
+                          double *egrid, double *inv) {
+  if (nx < 2 || ny < 2) return THX_ERR_INVALID_ARGUMENT;
+  return lte::inverse_table(nx, ny, rho, T, planes, egrid, inv) ? THX_OK : THX_ERR_NUMERICS;
+}
+
+// out: p, e, gibbs, cv, c^2, mu, lambda at (rho, T)
+int orc_lte_point(const thx_lte_table *t, double rho, double T, double *out) {
+  const lte::Table v = lte_view(t);
+  const lte::Eval s = lte::at(v, rho, T);
+  if (!s.valid) return THX_ERR_NUMERICS;
+  out[0] = s.pressure(); out[1] = s.energy(); out[2] = s.gibbs(); out[3] = s.cv();
+  out[4] = s.c2(); out[5] = s.transport(v, 4); out[6] = s.transport(v, 5);
+  return THX_OK;
+}
+
+int orc_lte_temperature(const thx_lte_table *t, double rho, double e, double *T, int *status) {
+  const lte::Table v = lte_view(t);
+  *T = lte::temperature(v, rho, e, status);
+  return THX_OK;
+}
+
+int orc_lte_flux(const thx_lte_table *t, int dim, int face, const double *q1, const double *q2,
+                 const double *d1, const double *d2, double *F) {
+  const lte::Table v = lte_view(t);
+  bool bad = false;
+  lte::lteec(v, dim, face != 0, q1, q2, d1, d2, F, &bad);
+  return bad ? THX_ERR_NUMERICS : THX_OK;
+}
+
+int orc_rhs_lte(const thx_geometry *g, const thx_config *cfg, const thx_lte_table *t,
+                const double *u, double *dudt, int nthreads) {
+  Disc c;
+  int st = setup(c, g, cfg);
+  if (st) return st;
+  const lte::Table v = lte_view(t);
+  std::atomic<int> bad{0};
+  c.gas.lte = &v;
+  c.gas.bad = &bad;
+  st = rhs(c, u, dudt, nthreads < 1 ? 1 : nthreads, nullptr, nullptr);
+  if (st) return st;
+  return bad.load() ? THX_ERR_NUMERICS : THX_OK;
 }
 
 int orc_max_threads(void) {

@@ -103,5 +103,49 @@ def pointwise():
     print("pointwise", len(rows))
 
 
+def lte():
+    """Reference LTE Helmholtz RHS (LTEEC, Euler and Navier-Stokes) on a 64x128
+    synthetic ideal-dissociating-gas table rebuilt by the oracle from its
+    parameters, plus reference point evaluations, recoveries and fluxes."""
+    tab = O.LteTable(64, 128, (-6.0, 1.0), (2.3, 4.3))
+    for name, flow, order, n in [("lte_euler_tgv_p2", "euler", 2, (3, 3, 2)),
+                                 ("lte_ns_tgv_p3", "ns", 3, (2, 2, 2))]:
+        m = O.box_mesh(3, order, n, (0.0,) * 3, (2 * np.pi,) * 3)
+        cfg = make_config(flow=flow, volume_flux="lteec", surface_flux="lteec", mu=1e-4)
+        u = cases.lte_taylor_green(m.coords)
+        du = O.rhs_lte(m, cfg, tab, u, use_ref=True)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), order=order, n=np.array(n),
+                            cfg=np.frombuffer(bytes(cfg), dtype=np.uint8), u=u, dudt=du,
+                            table=np.array([64, 128, -6.0, 1.0, 2.3, 4.3]))
+        print(name, du.shape)
+    rng = np.random.default_rng(7)
+    pts, recs, fl = [], [], []
+    cfg = make_config(volume_flux="lteec", surface_flux="lteec")
+    for k in range(12):
+        rho = 10 ** rng.uniform(-5.5, 0.5)
+        T = 10 ** rng.uniform(2.4, 4.2)
+        v = O.lte_point(tab, rho, T, use_ref=True)
+        pts.append([rho, T] + list(v))
+        Tr, st = O.lte_temperature(tab, rho, v[1], use_ref=True)
+        recs.append([rho, v[1], Tr, st])
+    for k in range(8):
+        def st():
+            rho = 0.01 * (1 + 0.2 * rng.random())
+            T = 3000.0 * (1 + 0.3 * rng.random())
+            u = rng.uniform(-300, 300, 3)
+            e = O.lte_point(tab, rho, T)[1]
+            return np.array([rho, rho * u[0], rho * u[1], rho * u[2], rho * e + 0.5 * rho * (u @ u)])
+        q1, q2 = st(), st()
+        d1, d2 = rng.uniform(-1, 1, 3), rng.uniform(-1, 1, 3)
+        for face in (0, 1):
+            F = O.lte_flux(tab, cfg, 3, face, q1, q2, d1, d2, use_ref=True)
+            fl.append(np.concatenate([[face], q1, q2, d1, d2, F]))
+    np.savez_compressed(os.path.join(HERE, "lte_pointwise.npz"), points=np.array(pts),
+                        recoveries=np.array(recs), fluxes=np.array(fl),
+                        table=np.array([64, 128, -6.0, 1.0, 2.3, 4.3]))
+    print("lte_pointwise", len(pts), len(fl))
+
+
 if __name__ == "__main__":
     pointwise()
+    lte()

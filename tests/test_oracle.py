@@ -25,11 +25,17 @@ def rel_l2(a, b):
 
 
 def load_cfg(raw):
-    return Config.from_buffer_copy(raw.tobytes())
+    """Configuration bytes stored with a fixture; fields added later stay zero."""
+    import ctypes
+    cfg = Config()
+    b = raw.tobytes()
+    ctypes.memmove(ctypes.addressof(cfg), b, min(len(b), ctypes.sizeof(cfg)))
+    return cfg
 
 
 @pytest.mark.parametrize("path", sorted(p for p in glob.glob(os.path.join(GOLD, "*.npz"))
-                                        if not p.endswith("pointwise.npz")))
+                                        if not p.endswith("pointwise.npz")
+                                        and not os.path.basename(p).startswith("lte_")))
 def test_oracle_matches_reference_golden(path):
     z = np.load(path)
     m = O.box_mesh(int(z["dim"]), int(z["order"]), tuple(z["n"]), tuple(z["lo"]), tuple(z["hi"]))
@@ -150,3 +156,70 @@ def test_rk3_conserves_and_threads_agree():
     mass0 = (u[0] * wq * m.jac).sum()
     mass1 = (a[0] * wq * m.jac).sum()
     assert abs(mass1 - mass0) <= 1e-13 * abs(mass0)
+
+
+# ---- LTE Helmholtz gas -----------------------------------------------------
+def _table(spec):
+    return O.LteTable(int(spec[0]), int(spec[1]), (spec[2], spec[3]), (spec[4], spec[5]))
+
+
+@pytest.mark.parametrize("name", ["lte_euler_tgv_p2", "lte_ns_tgv_p3"])
+def test_lte_rhs_matches_reference_golden(name):
+    z = np.load(os.path.join(GOLD, name + ".npz"))
+    tab = _table(z["table"])
+    m = O.box_mesh(3, int(z["order"]), tuple(z["n"]), (0.0,) * 3, (2 * np.pi,) * 3)
+    du = O.rhs_lte(m, load_cfg(z["cfg"]), tab, z["u"], nthreads=2)
+    assert rel_l2(du, z["dudt"]).max() <= 1e-12
+
+
+def test_lte_pointwise_golden():
+    z = np.load(os.path.join(GOLD, "lte_pointwise.npz"))
+    tab = _table(z["table"])
+    for row in z["points"]:
+        v = O.lte_point(tab, row[0], row[1])
+        assert np.allclose(v, row[2:], rtol=1e-13, atol=0)
+    for rho, e, T, st in z["recoveries"]:
+        Tr, s = O.lte_temperature(tab, rho, e)
+        assert s == st and abs(Tr - T) <= 1e-12 * T
+    cfg = make_config(volume_flux="lteec", surface_flux="lteec")
+    for row in z["fluxes"]:
+        face = int(row[0])
+        q1, q2, d1, d2, F = row[1:6], row[6:11], row[11:14], row[14:17], row[17:22]
+        got = O.lte_flux(tab, cfg, 3, face, q1, q2, d1, d2)
+        assert np.allclose(got, F, rtol=1e-12, atol=1e-12 * np.abs(F).max())
+
+
+def test_lte_table_is_the_ideal_dissociating_gas():
+    """Table planes reproduce p = rho R T (1+alpha), e = 3RT + alpha R theta_d, and the
+    inverse table inverts e(rho, T) (include/LTEHelmholtzTableBuilder.hpp:131-218)."""
+    tab = O.LteTable(32, 64, (-6.0, 1.0), (2.3, 4.3))
+    R, rd, th = O.IDG_O2["R"], O.IDG_O2["rho_d"], O.IDG_O2["theta_d"]
+    for i in (0, 7, 31):
+        for j in (0, 20, 63):
+            rho, T = tab.rho[i], tab.T[j]
+            K = rd / rho * np.exp(-th / T)
+            a = 2.0 / (1.0 + np.sqrt(1.0 + 4.0 / K))
+            p = rho * rho * tab.planes[1, j, i]
+            e = tab.planes[0, j, i] - T * tab.planes[2, j, i]
+            assert abs(p - rho * R * T * (1 + a)) <= 1e-12 * p
+            assert abs(e - (3 * R * T + a * R * th)) <= 1e-10 * abs(e)
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        rho = 10 ** rng.uniform(-5.9, 0.9)
+        T = 10 ** rng.uniform(2.31, 4.29)
+        e = O.lte_point(tab, rho, T)[1]
+        Tr, st = O.lte_temperature(tab, rho, e)
+        assert st == 0 and abs(Tr - T) <= 1e-8 * T
+
+
+def test_product_lte_tables_equal_oracle_tables():
+    """The library's table builders (synthetic gas planes, energy grid and
+    inverse table) reproduce the oracle's bit for bit."""
+    import theseus_b200 as T
+    for nx, ny, lr, lt in [(64, 128, (-6.0, 1.0), (2.3, 4.3)), (33, 47, (-4.0, 0.5), (2.5, 4.0))]:
+        o = O.LteTable(nx, ny, lr, lt)
+        p = T.HelmholtzTable.ideal_dissociating_gas(nx, ny, lr, lt, **O.IDG_O2)
+        for a in ("rho", "T", "planes", "e", "inv"):
+            assert np.array_equal(getattr(p, a), getattr(o, a)), a
+        q = T.HelmholtzTable(o.rho, o.T, o.planes)  # inverse rebuilt from the forward planes
+        assert np.array_equal(q.e, o.e) and np.array_equal(q.inv, o.inv)

@@ -18,9 +18,10 @@ import os
 
 import numpy as np
 
-from ._abi import (Config, Geometry, make_config, flux_id, FLUX, FLUX_NAMES,  # noqa: F401
-                   FLOW_EULER, FLOW_NAVIER_STOKES, PRECISION_FP64, PRECISION_FP32_MIXED,
-                   THX_OK)
+from ._abi import (Config, Geometry, LteTable, IdgParams, make_config, flux_id,  # noqa: F401
+                   FLUX, FLUX_NAMES, FLOW_EULER, FLOW_NAVIER_STOKES, PRECISION_FP64,
+                   PRECISION_FP32_MIXED, THX_OK, STATUS_NONPOSITIVE, STATUS_NONFINITE,
+                   STATUS_LAUNCH, STATUS_EOS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtheseus_b200.so")
@@ -46,6 +47,11 @@ def library():
         lib.thx_version.restype = C.c_char_p
         lib.thx_status_string.restype = C.c_char_p
         lib.thx_create.argtypes = [C.POINTER(Geometry), C.POINTER(Config), C.POINTER(C.c_void_p)]
+        lib.thx_create_lte.argtypes = [C.POINTER(Geometry), C.POINTER(Config), C.POINTER(LteTable),
+                                       C.POINTER(C.c_void_p)]
+        lib.thx_lte_idg_table.argtypes = [C.POINTER(IdgParams), C.c_int, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, _D, _D, _D]
+        lib.thx_lte_inverse_table.argtypes = [C.c_int, C.c_int, _D, _D, _D, _D, _D]
         lib.thx_destroy.argtypes = [C.c_void_p]
         lib.thx_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.thx_rk3_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
@@ -142,6 +148,52 @@ def lgl(np_):
     return x, w
 
 
+class HelmholtzTable:
+    """LTE Helmholtz gas table (include/LTEHelmholtzTable.hpp:13-35): host numpy
+    arrays rho_grid[nx], T_grid[ny], planes[6][ny][nx] (H, H_rho, H_T, H_rhoT, mu,
+    lambda), plus the energy grid and inverse table, which Build() derives when
+    they are not given (include/LTEHelmholtzTableBuilder.hpp:131-218)."""
+
+    def __init__(self, rho_grid, T_grid, planes, e_grid=None, inverse=None):
+        self.rho = np.ascontiguousarray(rho_grid, np.float64)
+        self.T = np.ascontiguousarray(T_grid, np.float64)
+        self.nx, self.ny = self.rho.size, self.T.size
+        self.planes = np.ascontiguousarray(planes, np.float64).reshape(6, self.ny, self.nx)
+        self.e = None if e_grid is None else np.ascontiguousarray(e_grid, np.float64)
+        self.inv = None if inverse is None else np.ascontiguousarray(inverse, np.float64).reshape(
+            self.ny, self.nx)
+        if self.e is None or self.inv is None:
+            self.Build()
+
+    def Build(self):
+        self.e = np.zeros(self.ny)
+        self.inv = np.zeros((self.ny, self.nx))
+        _check(library().thx_lte_inverse_table(self.nx, self.ny, self.rho.ctypes.data_as(_D),
+                                               self.T.ctypes.data_as(_D),
+                                               self.planes.ctypes.data_as(_D),
+                                               self.e.ctypes.data_as(_D),
+                                               self.inv.ctypes.data_as(_D)), "thx_lte_inverse_table")
+        return self
+
+    @classmethod
+    def ideal_dissociating_gas(cls, nx, ny, log_rho, log_T, R, rho_d, theta_d, mu0, T0, Pr):
+        """Synthetic table of Lighthill's ideal dissociating gas on log-spaced grids."""
+        p = IdgParams(R, rho_d, theta_d, mu0, T0, Pr)
+        rho, T, planes = np.zeros(nx), np.zeros(ny), np.zeros((6, ny, nx))
+        _check(library().thx_lte_idg_table(C.byref(p), nx, ny, float(log_rho[0]), float(log_rho[1]),
+                                           float(log_T[0]), float(log_T[1]),
+                                           rho.ctypes.data_as(_D), T.ctypes.data_as(_D),
+                                           planes.ctypes.data_as(_D)), "thx_lte_idg_table")
+        return cls(rho, T, planes)
+
+    def struct(self):
+        s = LteTable(self.nx, self.ny, self.rho.ctypes.data_as(_D), self.T.ctypes.data_as(_D),
+                     self.e.ctypes.data_as(_D), self.planes.ctypes.data_as(_D),
+                     self.inv.ctypes.data_as(_D))
+        self._s = s
+        return s
+
+
 def _stream_ptr(stream):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
@@ -155,7 +207,7 @@ class RHSOperator:
     flow = "euler"
 
     def __init__(self, mesh, numerical_flux="chandrashekar", surface_flux=None, fv_flux="llf",
-                 blending=False, precision="fp64", device=None, **physics):
+                 blending=False, precision="fp64", device=None, gas=None, **physics):
         import torch
         if not torch.cuda.is_available():
             raise THXError("no CUDA device: the DGSEM operator has no CPU fallback")
@@ -164,12 +216,20 @@ class RHSOperator:
                                surface_flux=surface_flux, fv_flux=fv_flux, blending=blending,
                                precision=precision, **physics)
         self.mixed = self.cfg.precision == PRECISION_FP32_MIXED
-        self.dtype = torch.float32 if self.mixed else torch.float64
+        # the ABI state is FP64 in both precisions (FP32-mixed narrows internally)
+        self.dtype = torch.float64
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.gas = gas
         h = C.c_void_p()
         with torch.cuda.device(self.device):
-            _check(library().thx_create(C.byref(mesh.struct()), C.byref(self.cfg), C.byref(h)),
-                   "thx_create")
+            if gas is None:
+                _check(library().thx_create(C.byref(mesh.struct()), C.byref(self.cfg), C.byref(h)),
+                       "thx_create")
+            else:
+                if not isinstance(gas, HelmholtzTable):
+                    raise THXError("gas must be a HelmholtzTable (or None for the ideal gas)")
+                _check(library().thx_create_lte(C.byref(mesh.struct()), C.byref(self.cfg),
+                                                C.byref(gas.struct()), C.byref(h)), "thx_create_lte")
         self._h = h
 
     def __del__(self):
@@ -271,13 +331,22 @@ class NSOperator(RHSOperator):
     flow = "navier-stokes"
 
 
-def MakeRHSOperator(runtime, mesh, device=None):
+def MakeRHSOperator(runtime, mesh, device=None, table=None):
     """Selection by the reference's runtime JSON keys (include/SimFactory_impl.hpp:63-488):
-    flow_model, numerical_flux, gamma, Pr, R_gas, mu; plus the keys this library adds to
-    decouple the volume and surface fluxes (surface_flux, fv_flux), blending and precision."""
+    flow_model, numerical_flux, gas_model, gamma, Pr, R_gas, mu; plus the keys this library
+    adds to decouple the volume and surface fluxes (surface_flux, fv_flux), blending and
+    precision.  gas_model "lte"/"lte_helmholtz" needs `table` (a HelmholtzTable)."""
     flow = str(runtime.get("flow_model", "euler")).lower()
     viscous = flow.startswith(("visc", "nav", "cns", "ns"))
     gas = str(runtime.get("gas_model", "cpg")).lower()
+    if gas in ("lte", "lte_helmholtz", "helmholtz"):
+        if table is None:
+            raise THXError("gas_model 'lte' needs a HelmholtzTable (table=...)")
+        cls = NSOperator if viscous else EulerOperator
+        phys = {k: runtime[k] for k in ("Pr", "mu") if k in runtime}
+        return cls(mesh, numerical_flux=runtime.get("numerical_flux", "lteec"),
+                   surface_flux=runtime.get("surface_flux", "lteec"), device=device, gas=table,
+                   **phys)
     if gas not in ("", "cpg", "ideal", "ideal_gas"):
         raise THXError(f"gas_model '{gas}' is not built in this library")
     cls = NSOperator if viscous else EulerOperator

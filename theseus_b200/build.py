@@ -17,14 +17,19 @@ LIB = os.path.join(HERE, "libtheseus_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-O3",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-O3",
          "--expt-relaxed-constexpr", "-I", SRC, "-I", INCLUDE]
 ORDERS = (3, 4, 5, 6)
 
 
 def units():
     """(object name, source, extra defines) of every translation unit."""
-    u = [("thx_api.o", "thx_api.cu", []), ("thx_host.o", "thx_host.cpp", [])]
+    u = [("thx_api.o", "thx_api.cu", []), ("thx_host.o", "thx_host.cpp", []),
+         ("thx_lte_host.o", "thx_lte_host.cpp", [])]
+    for dim in (2, 3):
+        u.append((f"lte_face_{dim}.o", "thx_inst_lte.cu", [f"-DTHX_DIM={dim}"]))
+        for n in ORDERS:
+            u.append((f"lte_{dim}_{n}.o", "thx_inst_lte.cu", [f"-DTHX_DIM={dim}", f"-DTHX_N={n}"]))
     for prec in (0, 1):
         for dim in (2, 3):
             u.append((f"face_{prec}_{dim}.o", "thx_inst_face.cu", [f"-DTHX_PREC={prec}", f"-DTHX_DIM={dim}"]))
@@ -78,10 +83,13 @@ def build(verbose=False, jobs=None):
         with ThreadPoolExecutor(jobs) as ex:
             list(ex.map(_compile, todo))
     if todo or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs
+        # link beside the library and rename: a reader never sees a partial file
+        tmp = LIB + ".partial"
+        cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+        os.replace(tmp, LIB)
     return LIB
 
 

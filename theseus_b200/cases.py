@@ -79,3 +79,35 @@ def perturbed_uniform(shape_eq_e_nd, dim, seed=0, amp=0.1, gamma=1.4):
     vel = [c + amp * rng.uniform(-1, 1, (ne, nd)) for c in (0.3, -0.2, 0.1)[:dim]]
     p = 1.0 + amp * rng.uniform(-1, 1, (ne, nd))
     return conserved(rho, vel, p, gamma)
+
+
+# O2-like ideal dissociating gas of the LTE benchmark table (gas constant of
+# the molecule, characteristic density, dissociation temperature).
+IDG_O2 = dict(R=8.314462618 / 0.0319988, rho_d=1.5e5, theta_d=59500.0)
+
+
+def idg_energy(rho, T, R, rho_d, theta_d):
+    """Specific internal energy of the ideal dissociating gas, e = 3RT + alpha R theta_d,
+    alpha^2/(1-alpha) = (rho_d/rho) exp(-theta_d/T)."""
+    K = (rho_d / rho) * np.exp(-theta_d / T)
+    alpha = 2.0 / (1.0 + np.sqrt(1.0 + 4.0 / K))
+    return 3.0 * R * T + alpha * R * theta_d
+
+
+def lte_taylor_green(coords, rho0=0.01, T0=3000.0, U0=300.0, dT=0.05, gas=None):
+    """Taylor-Green velocity field (include/StateInit.hpp:139-161 shape) on a uniform
+    density, with the temperature carrying the TGV pressure pattern:
+    T = T0 (1 + dT/16 (cos 2x + cos 2y)(cos 2z + 2))."""
+    g = gas or IDG_O2
+    x, y, z = coords[0], coords[1], coords[2]
+    u = U0 * np.sin(x) * np.cos(y) * np.cos(z)
+    v = -U0 * np.cos(x) * np.sin(y) * np.cos(z)
+    w = np.zeros_like(x)
+    T = T0 * (1.0 + dT / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0))
+    rho = rho0 * np.ones_like(x)
+    e = idg_energy(rho, T, g["R"], g["rho_d"], g["theta_d"])
+    out = np.empty((5,) + x.shape)
+    out[0] = rho
+    out[1], out[2], out[3] = rho * u, rho * v, rho * w
+    out[4] = rho * e + 0.5 * rho * (u * u + v * v + w * w)
+    return out

@@ -2,7 +2,7 @@
 // device, kernel selection, right-hand side, fused SSP-RK3 steps, stability
 // estimate and status.  No CPU fallback exists: without a CUDA device every
 // compute entry point returns THX_ERR_NO_DEVICE.
-#include "thx_launch.cuh"
+#include "thx_operator.cuh"
 #include "thx_host.h"
 
 #include <algorithm>
@@ -16,12 +16,6 @@
 using namespace thx;
 
 namespace {
-
-struct Layout {
-  long long jac_es = 0, jac_ns = 0, met_es = 0, met_ns = 0;
-  long long n_fs = 0, n_ps = 0, w_fs = 0, w_ps = 0;
-  long long sub_es[3] = {0, 0, 0};
-};
 
 // Pack a [outer][inner][block] array, dropping the outer and/or inner
 // dimension where every entry is bitwise equal along it.
@@ -56,8 +50,21 @@ void pack_strided(const double *src, long long outer, long long inner, int block
 }
 
 template <typename R>
-GasT<R> make_gas(const thx_config &c) {
+GasT<R> make_gas(const thx_config &c, int dim) {
   GasT<R> g;
+  for (int k = 0; k < 5; ++k) g.qref[k] = R(0);
+  g.ke_ref = R(0);
+  g.p_ref = R(0);
+  if (IsF32<R>::value) {
+    // reference state of the FP32 working copy and its pressure
+    double m2 = 0.0;
+    for (int d = 0; d < dim; ++d) m2 += c.state_offset[1 + d] * c.state_offset[1 + d];
+    const double rho = c.state_offset[0];
+    const double ke = rho > 0.0 ? 0.5 * m2 / rho : 0.0;
+    for (int k = 0; k < dim + 2; ++k) g.qref[k] = (R)c.state_offset[k];
+    g.ke_ref = (R)ke;
+    g.p_ref = (R)((c.gamma - 1.0) * (c.state_offset[dim + 1] - ke));
+  }
   const double gm1 = c.gamma - 1.0;
   const double gm1_inv = 1.0 / gm1;
   const double cp = (c.gamma * gm1_inv) * c.R_gas;
@@ -79,24 +86,53 @@ GasT<R> make_gas(const thx_config &c) {
   return g;
 }
 
+// Operator whose buffers are being allocated on this thread: in pool mode
+// (batch engine) allocations are stream-ordered on its set-up stream.
+thread_local thx_operator_s *t_alloc_owner = nullptr;
+
+struct AllocOwner {
+  explicit AllocOwner(thx_operator_s *h) { t_alloc_owner = h; }
+  ~AllocOwner() { t_alloc_owner = nullptr; }
+};
+
+bool pool_mode() { return t_alloc_owner && t_alloc_owner->pool; }
+
 template <typename T>
 int dev_alloc(T **p, size_t n, std::vector<void *> &track) {
   *p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) {
+  const cudaError_t e = pool_mode()
+      ? cudaMallocFromPoolAsync((void **)p, n * sizeof(T), t_alloc_owner->pool, t_alloc_owner->setup_stream)
+      : cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
     cudaGetLastError();
+    *p = nullptr;
     return THX_ERR_OUT_OF_MEMORY;
   }
   track.push_back(*p);
   return THX_OK;
 }
 
+// Host-to-device copy of set-up data; stream-ordered in pool mode (pageable
+// sources are staged before the call returns).
+int to_device(void *dst, const void *src, size_t bytes) {
+  const cudaError_t e = pool_mode()
+      ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, t_alloc_owner->setup_stream)
+      : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? THX_OK : THX_ERR_CUDA;
+}
+
+int dev_zero(void *dst, size_t bytes) {
+  const cudaError_t e = pool_mode() ? cudaMemsetAsync(dst, 0, bytes, t_alloc_owner->setup_stream)
+                                    : cudaMemset(dst, 0, bytes);
+  return e == cudaSuccess ? THX_OK : THX_ERR_CUDA;
+}
+
 template <typename T>
 int upload(T **p, const T *src, size_t n, std::vector<void *> &track) {
   int st = dev_alloc(p, n, track);
   if (st) return st;
-  if (cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return THX_ERR_CUDA;
-  return THX_OK;
+  return to_device(*p, src, n * sizeof(T));
 }
 
 int upload_both(const std::vector<double> &h, double **d64, float **d32, bool want32,
@@ -114,47 +150,6 @@ int upload_both(const std::vector<double> &h, double **d64, float **d32, bool wa
 
 }  // namespace
 
-namespace thx {
-__global__ void convert_f64_f32(long long n, const double *src, float *dst) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    dst[i] = (float)src[i];
-}
-}  // namespace thx
-
-struct thx_operator_s {
-  int device = 0;
-  thx_config cfg{};
-  int dim = 0, order = 0, N = 0, nd = 0, nfp = 0, neq = 0, ne = 0, nf = 0;
-  long long L = 0;
-  bool mixed = false, ns = false, blend = false;
-  Layout lay;
-  double *jac64 = nullptr, *met64 = nullptr, *nrm64 = nullptr, *wm64 = nullptr, *wp64 = nullptr;
-  double *sub64[3] = {nullptr, nullptr, nullptr}, *ops64 = nullptr, *D64 = nullptr;
-  float *jac32 = nullptr, *met32 = nullptr, *nrm32 = nullptr, *wm32 = nullptr, *wp32 = nullptr;
-  float *sub32[3] = {nullptr, nullptr, nullptr}, *ops32 = nullptr, *D32 = nullptr;
-  int *face_elem = nullptr, *face_lface = nullptr, *elem_face = nullptr;
-  void *fstar = nullptr, *vflux = nullptr;  // face fluxes; NS physical viscous flux
-  double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
-  unsigned *status = nullptr;
-  unsigned long long *stab = nullptr;
-  double *y = nullptr;
-  float *yf = nullptr;
-  VolLaunch<double> vol64 = nullptr;
-  GradLaunch<double> grad64 = nullptr;
-  BlendLaunch<double> blend64 = nullptr;
-  FaceLaunch<double> face64 = nullptr;
-  VolLaunch<float> vol32 = nullptr;
-  GradLaunch<float> grad32 = nullptr;
-  BlendLaunch<float> blend32 = nullptr;
-  FaceLaunch<float> face32 = nullptr;
-  GasT<double> g64;
-  GasT<float> g32;
-  double threshold = 0.0;
-  double adv_scale = 0.0, dif_scale = 0.0, surf_scale = 0.0;
-  std::vector<void *> allocs;
-  std::string desc;
-};
 
 namespace {
 
@@ -198,6 +193,25 @@ bool pick_order_kernels(thx_operator_s *h, int vk) {
   return false;
 }
 
+bool pick_lte_kernels(thx_operator_s *h) {
+  const int ns = h->ns ? 1 : 0;
+#define THX_PICK_LTE(P, D, NN)                      \
+  if (h->dim == D && h->N == NN) {                  \
+    const LteKernels k = lte_kernels_##D##_##NN();  \
+    h->vol64 = k.vol[ns];                           \
+    h->grad64 = k.grad;                             \
+    found = true;                                   \
+  }
+  bool found = false;
+  THX_FOR_ORDERS(THX_PICK_LTE, 0, 2)
+  THX_FOR_ORDERS(THX_PICK_LTE, 0, 3)
+#undef THX_PICK_LTE
+  if (!found) return false;
+  const LteFaceKernels f = h->dim == 2 ? lte_face_kernels_2() : lte_face_kernels_3();
+  h->face64 = f.face[ns];
+  return true;
+}
+
 void pick_face_kernels(thx_operator_s *h) {
   const int s = h->cfg.surface_flux, ns = h->ns ? 1 : 0;
   if (!h->mixed) {
@@ -210,7 +224,10 @@ void pick_face_kernels(thx_operator_s *h) {
 }
 
 void free_all(thx_operator_s *h) {
-  for (void *p : h->allocs) cudaFree(p);
+  for (void *p : h->allocs) {
+    if (h->pool) cudaFreeAsync(p, h->setup_stream);
+    else cudaFree(p);
+  }
   h->allocs.clear();
 }
 
@@ -270,7 +287,9 @@ void subcell_element(int dim, int N, const double *metric_el, const double *D, c
           }
 }
 
-int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h) {
+int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
+                const thx_lte_table *table = nullptr) {
+  AllocOwner owner(h);
   h->cfg = *cfg;
   h->dim = g->dim;
   h->order = g->order;
@@ -284,19 +303,44 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h)
   h->mixed = cfg->precision == THX_PRECISION_FP32_MIXED;
   h->ns = cfg->flow_model == THX_FLOW_NAVIER_STOKES;
   h->blend = cfg->blending != 0;
-  h->g64 = make_gas<double>(*cfg);
-  h->g32 = make_gas<float>(*cfg);
+  h->g64 = make_gas<double>(*cfg, g->dim);
+  h->g32 = make_gas<float>(*cfg, g->dim);
+  for (int k = 0; k < 5; ++k) h->off.v[k] = (k < g->dim + 2) ? cfg->state_offset[k] : 0.0;
   const int vk = (cfg->volume_flux == THX_FLUX_CHANDRASHEKAR) ? VOL_CHANDRASHEKAR
                : (cfg->volume_flux == THX_FLUX_RANOCHA)     ? VOL_RANOCHA
                : (cfg->volume_flux == THX_FLUX_PIROZZOLI)   ? VOL_PIROZZOLI
                                                             : VOL_CENTRAL;
-  if (!pick_order_kernels(h, vk)) return THX_ERR_UNSUPPORTED;
-  pick_face_kernels(h);
+  h->lte = table != nullptr;
+  if (h->lte) {
+    if (!pick_lte_kernels(h)) return THX_ERR_UNSUPPORTED;
+  } else {
+    if (!pick_order_kernels(h, vk)) return THX_ERR_UNSUPPORTED;
+    pick_face_kernels(h);
+  }
   const bool full = cfg->geometry_layout == 1;
   const int dim = h->dim, N = h->N, nd = h->nd, nfp = h->nfp, MB = dim * dim;
   const bool w32 = h->mixed;
   auto &A = h->allocs;
   int st;
+  if (h->lte) {
+    // device copy of the table; node temperatures
+    const size_t nx = (size_t)table->nx, ny = (size_t)table->ny;
+    double *rho = nullptr, *T = nullptr, *e = nullptr, *planes = nullptr, *inv = nullptr;
+    if ((st = upload(&rho, table->rho_grid, nx, A))) return st;
+    if ((st = upload(&T, table->T_grid, ny, A))) return st;
+    if ((st = upload(&e, table->e_grid, ny, A))) return st;
+    if ((st = upload(&planes, table->planes, 6 * nx * ny, A))) return st;
+    if ((st = upload(&inv, table->inverse, nx * ny, A))) return st;
+    h->g64.lte.nx = table->nx;
+    h->g64.lte.ny = table->ny;
+    h->g64.lte.rho = rho;
+    h->g64.lte.T = T;
+    h->g64.lte.e = e;
+    h->g64.lte.planes = planes;
+    h->g64.lte.inv = inv;
+    if ((st = dev_alloc(&h->Tn, (size_t)h->L, A))) return st;
+    h->g64.Tn = h->Tn;
+  }
   // geometry
   std::vector<double> tmp;
   pack_strided(g->jac, h->ne, nd, 1, full, tmp, h->lay.jac_es, h->lay.jac_ns);
@@ -364,11 +408,11 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h)
   }
   if ((st = dev_alloc(&h->status, 1, A))) return st;
   if ((st = dev_alloc(&h->stab, 3, A))) return st;
-  if (cudaMemset(h->status, 0, sizeof(unsigned)) != cudaSuccess) return THX_ERR_CUDA;
+  if ((st = dev_zero(h->status, sizeof(unsigned)))) return st;
   if ((st = dev_alloc(&h->alpha, h->ne, A))) return st;
   if ((st = dev_alloc(&h->eta, h->ne, A))) return st;
-  if (cudaMemset(h->alpha, 0, sizeof(double) * h->ne) != cudaSuccess) return THX_ERR_CUDA;
-  if (cudaMemset(h->eta, 0, sizeof(double) * h->ne) != cudaSuccess) return THX_ERR_CUDA;
+  if ((st = dev_zero(h->alpha, sizeof(double) * h->ne))) return st;
+  if ((st = dev_zero(h->eta, sizeof(double) * h->ne))) return st;
   // blending: modal transform and subcell metrics
   h->threshold = cfg->modal_threshold > 0 ? cfg->modal_threshold
                                           : 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->order, 0.25));
@@ -424,10 +468,11 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h)
   if (ce != cudaSuccess) { cudaGetLastError(); return THX_ERR_CUDA; }
   char buf[512];
   std::snprintf(buf, sizeof(buf),
-                "dim=%d p=%d ne=%d nf=%d flow=%s vol=%d surf=%d fv=%d blend=%d prec=%s "
+                "dim=%d p=%d ne=%d nf=%d flow=%s gas=%s vol=%d surf=%d fv=%d blend=%d prec=%s "
                 "layout jac(%lld,%lld) met(%lld,%lld) nrm(%lld,%lld) w(%lld,%lld) sub(%lld)",
-                dim, h->order, h->ne, h->nf, h->ns ? "ns" : "euler", cfg->volume_flux,
-                cfg->surface_flux, cfg->fv_flux, cfg->blending, h->mixed ? "fp32-mixed" : "fp64",
+                dim, h->order, h->ne, h->nf, h->ns ? "ns" : "euler", h->lte ? "lte" : "ideal",
+                cfg->volume_flux, cfg->surface_flux, cfg->fv_flux, cfg->blending,
+                h->mixed ? "fp32-mixed" : "fp64",
                 h->lay.jac_es, h->lay.jac_ns, h->lay.met_es, h->lay.met_ns, h->lay.n_fs, h->lay.n_ps,
                 h->lay.w_fs, h->lay.w_ps, h->lay.sub_es[0]);
   h->desc = buf;
@@ -455,65 +500,92 @@ FaceLaunch<float> facek(thx_operator_s *h, float *) { return h->face32; }
 const GasT<double> &gas(thx_operator_s *h, double *) { return h->g64; }
 const GasT<float> &gas(thx_operator_s *h, float *) { return h->g32; }
 
-// One right-hand side: [indicator] [gradient] face fluxes, volume+lift.
-// stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
+}  // namespace
+
+namespace thx {
+
+template <typename R>
+void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double *um, double *y,
+             float *yf, GradArgs<R> &ga, FaceArgs<R> &fa, VolArgs<R> &va) {
+  R *tag = nullptr;
+  const Geo<R> G = geo(h, tag);
+  const GasT<R> &g = gas(h, tag);
+  R *vfl = reinterpret_cast<R *>(h->vflux);
+  R *fst = reinterpret_cast<R *>(h->fstar);
+  ga = GradArgs<R>{};
+  ga.u = u; ga.vflux = vfl; ga.ne = h->ne;
+  ga.jac = G.jac; ga.jac_es = h->lay.jac_es; ga.jac_ns = h->lay.jac_ns;
+  ga.met = G.met; ga.met_es = h->lay.met_es; ga.met_ns = h->lay.met_ns;
+  ga.elem_face = h->elem_face; ga.face_elem = h->face_elem; ga.face_lface = h->face_lface;
+  ga.normal = G.nrm; ga.n_fs = h->lay.n_fs; ga.n_ps = h->lay.n_ps;
+  ga.wm = G.wm; ga.wp = G.wp; ga.w_fs = h->lay.w_fs; ga.w_ps = h->lay.w_ps;
+  ga.D = G.D; ga.gas = g; ga.status = h->status;
+  fa = FaceArgs<R>{};
+  fa.u = u; fa.ne = h->ne; fa.nf = h->nf; fa.N = h->N;
+  fa.face_elem = h->face_elem; fa.face_lface = h->face_lface;
+  fa.normal = G.nrm; fa.n_fs = h->lay.n_fs; fa.n_ps = h->lay.n_ps;
+  fa.vflux = vfl; fa.fstar = fst; fa.gas = g;
+  va = VolArgs<R>{};
+  va.u = u; va.du = du; va.ne = h->ne;
+  va.jac = G.jac; va.jac_es = h->lay.jac_es; va.jac_ns = h->lay.jac_ns;
+  va.met = G.met; va.met_es = h->lay.met_es; va.met_ns = h->lay.met_ns;
+  va.elem_face = h->elem_face; va.fstar = fst;
+  va.wm = G.wm; va.wp = G.wp; va.w_fs = h->lay.w_fs; va.w_ps = h->lay.w_ps;
+  va.vflux = vfl;
+  va.alpha = h->blend ? h->alpha : nullptr;
+  for (int d = 0; d < 3; ++d) { va.sub[d] = G.sub[d]; va.sub_es[d] = h->lay.sub_es[d]; }
+  va.fv_flux = h->cfg.fv_flux;
+  va.gas = g;
+  va.ops = G.ops;
+  va.stage = stage; va.dt = dt; va.um = um; va.y = y; va.yf = yf;
+  for (int k = 0; k < 5; ++k) va.off[k] = IsF32<R>::value ? h->off.v[k] : 0.0;
+  va.status = h->status;
+}
+
+template void op_args<double>(thx_operator_s *, const double *, double *, int, double, double *,
+                              double *, float *, GradArgs<double> &, FaceArgs<double> &,
+                              VolArgs<double> &);
+template void op_args<float>(thx_operator_s *, const float *, float *, int, double, double *,
+                             double *, float *, GradArgs<float> &, FaceArgs<float> &,
+                             VolArgs<float> &);
+
+}  // namespace thx
+
+namespace {
+
+// One right-hand side: [T recovery] [indicator] [gradient] face fluxes,
+// volume+lift.  stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
 template <typename R>
 int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
             double *um, double *y, float *yf, cudaEvent_t *ev = nullptr) {
   R *tag = nullptr;
   if (ev) cudaEventRecord(ev[0], s);
-  const Geo<R> G = geo(h, tag);
-  const GasT<R> &g = gas(h, tag);
-  cudaError_t ce;
+  GradArgs<R> ga;
+  FaceArgs<R> fa;
+  VolArgs<R> va;
+  op_args<R>(h, u, du, stage, dt, um, y, yf, ga, fa, va);
+  if constexpr (!IsF32<R>::value) {
+    if (h->lte) {
+      cudaError_t te = h->dim == 2
+          ? launch_lte_temperature<2>(u, h->L, h->g64.lte, h->Tn, h->status, s)
+          : launch_lte_temperature<3>(u, h->L, h->g64.lte, h->Tn, h->status, s);
+      if (te != cudaSuccess) return THX_ERR_CUDA;
+    }
+  }
   if (h->blend) {
     BlendArgs<R> b;
-    b.u = u; b.ne = h->ne; b.vinv = h->vinv; b.gas = g;
+    b.u = u; b.ne = h->ne; b.vinv = h->vinv; b.gas = gas(h, tag);
     b.threshold = h->threshold; b.sharpness = h->cfg.sharpness;
     b.alpha_min = h->cfg.alpha_min; b.alpha_max = h->cfg.alpha_max;
     b.alpha = h->alpha; b.eta = h->eta;
-    if ((ce = blendk(h, tag)(b, s)) != cudaSuccess) return THX_ERR_CUDA;
+    if (blendk(h, tag)(b, s) != cudaSuccess) return THX_ERR_CUDA;
   }
   if (ev) cudaEventRecord(ev[1], s);
-  R *vfl = reinterpret_cast<R *>(h->vflux);
-  if (h->ns) {
-    GradArgs<R> a;
-    a.u = u; a.vflux = vfl; a.ne = h->ne;
-    a.jac = G.jac; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
-    a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
-    a.elem_face = h->elem_face; a.face_elem = h->face_elem; a.face_lface = h->face_lface;
-    a.normal = G.nrm; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
-    a.wm = G.wm; a.wp = G.wp; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
-    a.D = G.D; a.gas = g;
-    if ((ce = gradk(h, tag)(a, s, 0)) != cudaSuccess) return THX_ERR_CUDA;
-  }
+  if (h->ns && gradk(h, tag)(ga, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[2], s);
-  R *fst = reinterpret_cast<R *>(h->fstar);
-  {
-    FaceArgs<R> a;
-    a.u = u; a.ne = h->ne; a.nf = h->nf; a.N = h->N;
-    a.face_elem = h->face_elem; a.face_lface = h->face_lface;
-    a.normal = G.nrm; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
-    a.vflux = vfl; a.fstar = fst; a.gas = g;
-    if ((ce = facek(h, tag)(a, s)) != cudaSuccess) return THX_ERR_CUDA;
-  }
+  if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[3], s);
-  {
-    VolArgs<R> a;
-    a.u = u; a.du = du; a.ne = h->ne;
-    a.jac = G.jac; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
-    a.met = G.met; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
-    a.elem_face = h->elem_face; a.fstar = fst;
-    a.wm = G.wm; a.wp = G.wp; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
-    a.vflux = vfl;
-    a.alpha = h->blend ? h->alpha : nullptr;
-    for (int d = 0; d < 3; ++d) { a.sub[d] = G.sub[d]; a.sub_es[d] = h->lay.sub_es[d]; }
-    a.fv_flux = h->cfg.fv_flux;
-    a.gas = g;
-    a.ops = G.ops;
-    a.stage = stage; a.dt = dt; a.um = um; a.y = y; a.yf = yf;
-    a.status = h->status;
-    if ((ce = volk(h, tag)(a, s, 0)) != cudaSuccess) return THX_ERR_CUDA;
-  }
+  if (volk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[4], s);
   return THX_OK;
 }
@@ -528,6 +600,50 @@ int check_device() {
 }
 
 }  // namespace
+
+namespace {
+
+// Narrow the FP64 state to the FP32 working copy (mixed mode).
+int to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
+  const long long n = h->L * h->neq;
+  int st;
+  if (!h->yf && (st = dev_alloc(&h->yf, (size_t)n, h->allocs))) return st;
+  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  to_working<<<grid, 256, 0, s>>>(h->L, h->neq, u, h->yf, h->off);
+  return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
+}
+
+int rhs_mixed(thx_operator_s *h, const double *u, double *dudt, cudaStream_t s, cudaEvent_t *ev) {
+  const long long n = h->L * h->neq;
+  int st;
+  if (!h->kf && (st = dev_alloc(&h->kf, (size_t)n, h->allocs))) return st;
+  if ((st = to_working_copy(h, u, s))) return st;
+  if ((st = run_rhs<float>(h, h->yf, h->kf, s, 0, 0.0, nullptr, nullptr, nullptr, ev))) return st;
+  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  widen<<<grid, 256, 0, s>>>(n, h->kf, dudt);
+  return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
+}
+
+}  // namespace
+
+namespace thx {
+
+int op_create(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
+              const thx_lte_table *table) {
+  try {
+    return create_impl(g, cfg, h, table);
+  } catch (...) {
+    return THX_ERR_OUT_OF_MEMORY;
+  }
+}
+
+void op_free(thx_operator_s *h) { free_all(h); }
+
+int op_to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
+  return to_working_copy(h, u, s);
+}
+
+}  // namespace thx
 
 extern "C" {
 
@@ -583,6 +699,10 @@ int thx_create(const thx_geometry *g, const thx_config *cfg, thx_handle *out) {
       !(cfg->gamma > 1.0) || !(cfg->Pr > 0.0))
     return THX_ERR_INVALID_ARGUMENT;
   if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
+  // the LTEEC flux needs the LTE Helmholtz gas (thx_create_lte)
+  if (cfg->volume_flux == THX_FLUX_LTEEC || cfg->surface_flux == THX_FLUX_LTEEC ||
+      cfg->fv_flux == THX_FLUX_LTEEC)
+    return THX_ERR_UNSUPPORTED;
   int st = check_device();
   if (st) return st;
   thx_operator_s *h = new (std::nothrow) thx_operator_s();
@@ -590,6 +710,54 @@ int thx_create(const thx_geometry *g, const thx_config *cfg, thx_handle *out) {
   cudaGetDevice(&h->device);
   try {
     st = create_impl(g, cfg, h);
+  } catch (...) {
+    st = THX_ERR_OUT_OF_MEMORY;
+  }
+  if (st) {
+    free_all(h);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return THX_OK;
+}
+
+int thx_create_lte(const thx_geometry *g, const thx_config *cfg, const thx_lte_table *table,
+                   thx_handle *out) {
+  if (!g || !cfg || !table || !out) return THX_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (g->dim < 2 || g->dim > 3 || g->order < 1 || g->num_elements <= 0 || g->num_faces < 0 ||
+      !g->jac || !g->metric || (g->num_faces > 0 && (!g->face_elem || !g->face_lface ||
+                                                     !g->face_normal || !g->face_wminus ||
+                                                     !g->face_wplus)))
+    return THX_ERR_INVALID_ARGUMENT;
+  if ((cfg->flow_model != THX_FLOW_EULER && cfg->flow_model != THX_FLOW_NAVIER_STOKES) ||
+      !(cfg->Pr > 0.0))
+    return THX_ERR_INVALID_ARGUMENT;
+  // the LTE gas is served by the LTEEC flux on volume and faces, in FP64,
+  // without subcell blending
+  if (cfg->volume_flux != THX_FLUX_LTEEC || cfg->surface_flux != THX_FLUX_LTEEC ||
+      cfg->precision != THX_PRECISION_FP64 || cfg->blending)
+    return THX_ERR_UNSUPPORTED;
+  if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
+  if (table->nx < 2 || table->ny < 2 || !table->rho_grid || !table->T_grid || !table->e_grid ||
+      !table->planes || !table->inverse)
+    return THX_ERR_INVALID_ARGUMENT;
+  // grids strictly increasing (the cell search bisects them)
+  const double *grids[3] = {table->rho_grid, table->T_grid, table->e_grid};
+  const int counts[3] = {table->nx, table->ny, table->ny};
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < counts[k]; ++i)
+      if (!std::isfinite(grids[k][i]) || (i > 0 && !(grids[k][i] > grids[k][i - 1])))
+        return THX_ERR_INVALID_ARGUMENT;
+  if ((long long)table->nx * table->ny > (1LL << 26)) return THX_ERR_INVALID_ARGUMENT;
+  int st = check_device();
+  if (st) return st;
+  thx_operator_s *h = new (std::nothrow) thx_operator_s();
+  if (!h) return THX_ERR_OUT_OF_MEMORY;
+  cudaGetDevice(&h->device);
+  try {
+    st = create_impl(g, cfg, h, table);
   } catch (...) {
     st = THX_ERR_OUT_OF_MEMORY;
   }
@@ -617,8 +785,7 @@ int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream) {
   DeviceGuard dg(h->device);
   if (!dg.ok) return THX_ERR_CUDA;
   cudaStream_t s = (cudaStream_t)stream;
-  if (h->mixed)
-    return run_rhs<float>(h, (const float *)u, (float *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr);
+  if (h->mixed) return rhs_mixed(h, (const double *)u, (double *)dudt, s, nullptr);
   return run_rhs<double>(h, (const double *)u, (double *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr);
 }
 
@@ -630,11 +797,7 @@ int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream) 
   const long long n = h->L * h->neq;
   int st;
   if (!h->y && (st = dev_alloc(&h->y, (size_t)n, h->allocs))) return st;
-  if (h->mixed && !h->yf && (st = dev_alloc(&h->yf, (size_t)n, h->allocs))) return st;
-  if (h->mixed) {
-    convert_f64_f32<<<(int)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, s>>>(n, u, h->yf);
-    if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
-  }
+  if (h->mixed && (st = to_working_copy(h, u, s))) return st;
   for (int step = 0; step < nsteps; ++step) {
     if (h->mixed) {
       for (int stage = 1; stage <= 3; ++stage)
@@ -661,6 +824,7 @@ int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev, 
 
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, double *rates_out) {
   if (!h || !u || !dt_out) return THX_ERR_INVALID_ARGUMENT;
+  if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
   DeviceGuard dg(h->device);
   if (!dg.ok) return THX_ERR_CUDA;
   StabArgs a;
@@ -711,7 +875,7 @@ int thx_rhs_profile(thx_handle h, const void *u, void *dudt, void *stream, doubl
   cudaEvent_t ev[5];
   for (int i = 0; i < 5; ++i)
     if (cudaEventCreate(&ev[i]) != cudaSuccess) return THX_ERR_CUDA;
-  int st = h->mixed ? run_rhs<float>(h, (const float *)u, (float *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr, ev)
+  int st = h->mixed ? rhs_mixed(h, (const double *)u, (double *)dudt, s, ev)
                     : run_rhs<double>(h, (const double *)u, (double *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr, ev);
   if (st == THX_OK && cudaEventSynchronize(ev[4]) != cudaSuccess) st = THX_ERR_CUDA;
   for (int i = 0; i < 4 && st == THX_OK; ++i) {

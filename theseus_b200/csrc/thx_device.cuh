@@ -6,10 +6,12 @@
 // Formulas follow the reference's device functions (paths relative to the
 // reference project root); the per-node quantities that the reference
 // recomputes inside every pair (velocity, pressure, beta) are computed once per
-// node by the caller and passed in as NodeP, with identical arithmetic.
+// node by node_prims and passed to the pair fluxes, with identical arithmetic.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+
+#include "thx_lte.cuh"
 
 namespace thx {
 
@@ -23,7 +25,22 @@ struct GasT {
   R inv_gm1;      // 1/(gamma-1)
   R cv;           // cp/gamma
   int sutherland;
+  // FP32 working copies hold u - qref (a caller-chosen constant state);
+  // ke_ref and p_ref are its kinetic energy density and pressure.  Zero and
+  // unused in FP64.
+  R qref[5];
+  R ke_ref, p_ref;
+  // LTE Helmholtz gas (FP64 only): the device table and the per-node
+  // temperatures recovered once per right-hand side, [elem][node].
+  LteDev lte{};
+  const double *Tn = nullptr;
 };
+
+// The FP32-mixed path carries the state as an offset from qref and the
+// pressure as its fluctuation pp = p - p_ref; the FP64 path carries neither.
+template <typename R> struct IsF32 { static constexpr bool value = false; };
+template <> struct IsF32<float> { static constexpr bool value = true; };
+template <typename R, int DIM> constexpr int nprim() { return DIM + 3 + (IsF32<R>::value ? 1 : 0); }
 
 template <typename R> __device__ __forceinline__ R rsqrt_(R x);
 template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
@@ -46,15 +63,16 @@ __device__ __forceinline__ double log_mean(double x, double y) {
   }
   return (y - x) / log(xi);
 }
+// FP32 path: the near-equal series is summed and applied in FP64; its
+// argument u = ((xi-1)/(xi+1))^2 < 1e-4 only scales corrections of relative
+// size u/3, so it is formed in FP32.
 __device__ __forceinline__ float log_mean(float x, float y) {
   const float xi = y / x;
   const float u = (xi * (xi - 2.0f) + 1.0f) / (xi * (xi + 2.0f) + 1.0f);
   if (u < 1e-4f) {
-    const double xd = x, yd = y;
-    const double xid = yd / xd;
-    const double ud = (xid * (xid - 2.0) + 1.0) / (xid * (xid + 2.0) + 1.0);
+    const double ud = u;
     const double denom = 105.0 + ud * (35.0 + ud * (21.0 + 15.0 * ud));
-    return (float)((xd + yd) * 52.5 / denom);
+    return (float)(((double)x + (double)y) * 52.5 / denom);
   }
   return (y - x) / logf(xi);
 }
@@ -86,32 +104,57 @@ __device__ __forceinline__ R viscosity(const GasT<R> &g, const R *q) {
   return g.mu;
 }
 
-// Per-node data used by the volume kernel: density, velocity, pressure and one
-// flux-specific auxiliary (beta = rho/(2p) for Chandrashekar, specific
-// enthalpy e + p/rho for Pirozzoli, total enthalpy (rhoE+p)/rho for central).
-template <typename R, int DIM>
-struct NodeP {
-  R rho, v[DIM], p, aux;
-};
+// Per-node data used by the volume kernel (node_prims): density, velocity,
+// pressure and one flux-specific auxiliary (beta = rho/(2p) for Chandrashekar,
+// specific enthalpy e + p/rho for Pirozzoli, total enthalpy (rhoE+p)/rho for
+// central), plus in FP32 the pressure fluctuation p - p_ref.
 
-enum VolKind { VOL_CHANDRASHEKAR = 0, VOL_RANOCHA = 1, VOL_PIROZZOLI = 2, VOL_CENTRAL = 3 };
+enum VolKind { VOL_CHANDRASHEKAR = 0, VOL_RANOCHA = 1, VOL_PIROZZOLI = 2, VOL_CENTRAL = 3,
+               VOL_LTEEC = 4 };
 
 template <typename R, int DIM, int VOL>
-__device__ __forceinline__ void node_prims(const GasT<R> &g, const R *q, R *out /*[DIM+3]*/) {
-  const R rho = q[0];
-  R v[DIM];
+__device__ __forceinline__ void node_prims(const GasT<R> &g, const R *raw, R *out /*[nprim]*/) {
+  if constexpr (IsF32<R>::value) {
+    R q[DIM + 2];
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) v[d] = q[1 + d] / rho;
-  const R ke = ke_density<R, DIM>(q);
-  const R p = g.gm1 * (q[DIM + 1] - ke);
-  out[0] = rho;
+    for (int k = 0; k < DIM + 2; ++k) q[k] = g.qref[k] + raw[k];
+    const R rho = q[0];
+    const R ke = ke_density<R, DIM>(q);
+    const R pp = g.gm1 * (raw[DIM + 1] - (ke - g.ke_ref));
+    const R p = g.p_ref + pp;
+    out[0] = rho;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) out[1 + d] = v[d];
-  out[DIM + 1] = p;
-  if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = R(0.5) * rho / p;
-  else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = (q[DIM + 1] - ke) / rho + p / rho;
-  else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * (R(1) / rho);
-  else out[DIM + 2] = R(0);
+    for (int d = 0; d < DIM; ++d) out[1 + d] = q[1 + d] / rho;
+    out[DIM + 1] = p;
+    if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = R(0.5) * rho / p;
+    else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = (p * g.gm1_inv) / rho + p / rho;
+    else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * (R(1) / rho);
+    else out[DIM + 2] = R(0);
+    out[DIM + 3] = pp;
+  } else {
+    const R *q = raw;
+    const R rho = q[0];
+    R v[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = q[1 + d] / rho;
+    const R ke = ke_density<R, DIM>(q);
+    const R p = g.gm1 * (q[DIM + 1] - ke);
+    out[0] = rho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) out[1 + d] = v[d];
+    out[DIM + 1] = p;
+    if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = R(0.5) * rho / p;
+    else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = (q[DIM + 1] - ke) / rho + p / rho;
+    else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * (R(1) / rho);
+    else out[DIM + 2] = R(0);
+  }
+}
+
+// Pressure that enters the momentum fluxes: the fluctuation in FP32, p in FP64.
+template <typename R, int DIM>
+__device__ __forceinline__ R mom_p(const R *a) {
+  if constexpr (IsF32<R>::value) return a[DIM + 3];
+  else return a[DIM + 1];
 }
 
 // ---- two-point volume fluxes (metric rows already averaged) --------------
@@ -135,9 +178,12 @@ __device__ __forceinline__ void vol_chandrashekar(const GasT<R> &g, const R *a, 
   const R beta_ln = log_mean(beta1, beta2);
   const R p_hat = R(0.5) * (rho1 + rho2) / (beta1 + beta2);
   h_hat += R(0.5) / beta_ln * g.gm1_av_inv + p_hat / rho_ln;
+  // FP32: p_hat - p_ref = (beta1 pp1 + beta2 pp2)/(beta1 + beta2), exactly
+  R p_mom = p_hat;
+  if constexpr (IsF32<R>::value) p_mom = (beta1 * a[DIM + 3] + beta2 * b[DIM + 3]) / (beta1 + beta2);
   F[0] = rho_ln * vn;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom_hat[d] + p_hat * met[d];
+  for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom_hat[d] + p_mom * met[d];
   F[DIM + 1] = rho_ln * vn * h_hat;
 }
 
@@ -161,9 +207,10 @@ __device__ __forceinline__ void vol_ranocha(const GasT<R> &g, const R *a, const 
   }
   const R inv_beta_ln = (p1 * p2) / log_mean(rho1 * p2, rho2 * p1);
   const R ie = inv_beta_ln * g.inv_gm1;
+  const R p_mom = IsF32<R>::value ? R(0.5) * (mom_p<R, DIM>(a) + mom_p<R, DIM>(b)) : pbar;
   F[0] = rho_ln * vn;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_ln * vn * vbar[d] + pbar * met[d];
+  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_ln * vn * vbar[d] + p_mom * met[d];
   F[DIM + 1] = fe + rho_ln * (ie + ke) * vn;
 }
 
@@ -183,9 +230,10 @@ __device__ __forceinline__ void vol_pirozzoli(const GasT<R> &g, const R *a, cons
     ke_mean += R(0.25) * ((v1 * v1) + (v2 * v2));
   }
   const R h_mean = R(0.5) * (a[DIM + 2] + b[DIM + 2]);
+  const R p_mom = IsF32<R>::value ? R(0.5) * (mom_p<R, DIM>(a) + mom_p<R, DIM>(b)) : pbar;
   F[0] = rho_mean * vn;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_mean * vn * vbar[d] + pbar * met[d];
+  for (int d = 0; d < DIM; ++d) F[1 + d] = rho_mean * vn * vbar[d] + p_mom * met[d];
   F[DIM + 1] = rho_mean * (h_mean + ke_mean) * vn;
 }
 
@@ -206,7 +254,7 @@ __device__ __forceinline__ void vol_central(const R *qa, const R *qb, const R *a
 #pragma unroll
     for (int i = 0; i < DIM; ++i) {
       R fa = qa[1 + i] * qa[1 + d] * ia, fb = qb[1 + i] * qb[1 + d] * ib;
-      if (i == d) { fa += a[DIM + 1]; fb += b[DIM + 1]; }
+      if (i == d) { fa += mom_p<R, DIM>(a); fb += mom_p<R, DIM>(b); }
       accm[i] += R(0.5) * (fa + fb) * met[d];
     }
     accE += R(0.5) * (qa[1 + d] * a[DIM + 2] + qb[1 + d] * b[DIM + 2]) * met[d];
@@ -217,16 +265,51 @@ __device__ __forceinline__ void vol_central(const R *qa, const R *qb, const R *a
   F[DIM + 1] = accE;
 }
 
-// ---- surface fluxes on conserved states ----------------------------------
+// ---- surface fluxes ------------------------------------------------------
+// A face state: the conserved state q, its raw stored form d (FP32: the
+// offset u - qref, so that jumps d2 - d1 are exact; FP64: q itself), the
+// pressure p and the pressure entering momentum fluxes pp (FP32: p - p_ref).
 template <typename R, int DIM>
-struct NState { R inv_rho, p, H; };
+struct FState {
+  R q[DIM + 2], d[DIM + 2], p, pp;
+};
 
 template <typename R, int DIM>
-__device__ __forceinline__ NState<R, DIM> nstate(const GasT<R> &g, const R *q) {
+__device__ __forceinline__ void make_fstate(const GasT<R> &g, const R *raw, FState<R, DIM> &s) {
+  if constexpr (IsF32<R>::value) {
+#pragma unroll
+    for (int k = 0; k < DIM + 2; ++k) { s.d[k] = raw[k]; s.q[k] = g.qref[k] + raw[k]; }
+    const R ke = ke_density<R, DIM>(s.q);
+    s.pp = g.gm1 * (raw[DIM + 1] - (ke - g.ke_ref));
+    s.p = g.p_ref + s.pp;
+  } else {
+#pragma unroll
+    for (int k = 0; k < DIM + 2; ++k) { s.d[k] = raw[k]; s.q[k] = raw[k]; }
+    s.p = pressure<R, DIM>(g, s.q);
+    s.pp = s.p;
+  }
+}
+
+// Full conserved state from its stored form (adds qref in FP32).
+template <typename R, int DIM>
+__device__ __forceinline__ void reconstruct(const GasT<R> &g, const R *raw, R *q) {
+#pragma unroll
+  for (int k = 0; k < DIM + 2; ++k) {
+    if constexpr (IsF32<R>::value) q[k] = g.qref[k] + raw[k];
+    else q[k] = raw[k];
+  }
+}
+
+template <typename R, int DIM>
+struct NState { R inv_rho, p, pp, H; };
+
+template <typename R, int DIM>
+__device__ __forceinline__ NState<R, DIM> nstate(const FState<R, DIM> &f) {
   NState<R, DIM> s;
-  s.inv_rho = R(1) / q[0];
-  s.p = pressure<R, DIM>(g, q);
-  s.H = (q[DIM + 1] + s.p) * s.inv_rho;
+  s.inv_rho = R(1) / f.q[0];
+  s.p = f.p;
+  s.pp = f.pp;
+  s.H = (f.q[DIM + 1] + s.p) * s.inv_rho;
   return s;
 }
 // include/NavierStokesFlux.hpp:64-103
@@ -241,7 +324,7 @@ __device__ __forceinline__ R normal_flux(const R *q, const NState<R, DIM> &s, co
     else if (eq <= DIM) {
       const int c = eq - 1;
       pf = q[1 + c] * m * s.inv_rho;
-      if (c == dir) pf += s.p;
+      if (c == dir) pf += s.pp;
     } else pf = m * s.H;
     r += pf * n[dir];
   }
@@ -250,12 +333,13 @@ __device__ __forceinline__ R normal_flux(const R *q, const NState<R, DIM> &s, co
 
 // include/DissipationOperator.hpp:57-172
 template <typename R, int DIM>
-__device__ __forceinline__ void roe_dissipation(const GasT<R> &g, const R *q1, const R *q2,
-                                                const R *n, R *diss) {
+__device__ __forceinline__ void roe_dissipation(const GasT<R> &g, const FState<R, DIM> &A,
+                                                const FState<R, DIM> &B, const R *n, R *diss) {
   const int E = DIM + 1;
+  const R *q1 = A.q, *q2 = B.q;
   R vn1 = R(0), vn2 = R(0), vn_roe = R(0), nor_mag = R(0);
   const R rho1 = q1[0], rho2 = q2[0];
-  const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+  const R p1 = A.p, p2 = B.p;
   const R H1 = (q1[E] + p1) / rho1, H2 = (q2[E] + p2) / rho2;
   R roe[DIM + 2];
   const R ratio = rsqrt_(rho2 / rho1);
@@ -295,9 +379,9 @@ __device__ __forceinline__ void roe_dissipation(const GasT<R> &g, const R *q1, c
     e2 = (rabs(er) < eps) ? R(0.5) * (eps + (er * er) / eps) : rabs(er);
   }
   const R e1 = rabs(vn_roe);
-  const R del_rho = rho2 - rho1;
+  const R del_rho = B.d[0] - A.d[0];
   const R del_vn = vn2 - vn1;
-  const R del_p = p2 - p1;
+  const R del_p = B.pp - A.pp;
   const R ov_csq = R(1) / (c_roe * c_roe);
   const R pov_csq = del_p * ov_csq;
   const R rhoc_del_vn = roe[0] * del_vn * c_roe * ov_csq;
@@ -324,13 +408,14 @@ __device__ __forceinline__ void roe_dissipation(const GasT<R> &g, const R *q1, c
 
 // include/DissipationOperator.hpp:174-232
 template <typename R, int DIM>
-__device__ __forceinline__ void scalar_dissipation(const GasT<R> &g, const R *q1, const R *q2,
-                                                   const R *n, R *diss) {
+__device__ __forceinline__ void scalar_dissipation(const GasT<R> &g, const FState<R, DIM> &A,
+                                                   const FState<R, DIM> &B, const R *n, R *diss) {
   const int E = DIM + 1;
+  const R *q1 = A.q, *q2 = B.q;
   const R rho1 = q1[0], rho2 = q2[0];
   const R rho_mean = R(0.5) * (rho1 + rho2);
-  const R drho = rho2 - rho1;
-  const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+  const R drho = B.d[0] - A.d[0];
+  const R p1 = A.p, p2 = B.p;
   R vn1 = R(0), vn2 = R(0), nor_mag = R(0), de = R(0);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
@@ -350,17 +435,18 @@ __device__ __forceinline__ void scalar_dissipation(const GasT<R> &g, const R *q1
   de += R(0.5) * drho * g.inv_gm1 / beta_ln + R(0.5) * rho_mean * g.inv_gm1 * (R(1) / beta2 - R(1) / beta1);
   diss[0] = R(0.5) * lmax * drho;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) diss[1 + d] = R(0.5) * lmax * (q2[1 + d] - q1[1 + d]);
+  for (int d = 0; d < DIM; ++d) diss[1 + d] = R(0.5) * lmax * (B.d[1 + d] - A.d[1 + d]);
   diss[E] = de * (R(0.5) * lmax);
 }
 
 enum SurfKind { SURF_CHANDRASHEKAR = 0, SURF_RANOCHA = 1, SURF_PIROZZOLI = 2, SURF_HLL = 3,
-                SURF_LLF = 4, SURF_ROE = 5 };
+                SURF_LLF = 4, SURF_ROE = 5, SURF_LTEEC = 6 };
 
 template <typename R, int DIM, int SURF>
-__device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, const R *q2,
-                                             const R *n, R *F) {
+__device__ __forceinline__ void surface_flux(const GasT<R> &g, const FState<R, DIM> &A,
+                                             const FState<R, DIM> &B, const R *n, R *F) {
   constexpr int E = DIM + 1;
+  const R *q1 = A.q, *q2 = B.q;
   if (SURF == SURF_CHANDRASHEKAR) {
     // include/ChandrashekarFlux.hpp:91-155
     const R rho1 = q1[0], rho2 = q2[0];
@@ -375,23 +461,25 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
       mom[d] = rho_ln * vbar;
       hhat += -R(0.25) * (v1 * v1 + v2 * v2) + vbar * vbar;
     }
-    const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
+    const R p1 = A.p, p2 = B.p;
     const R beta1 = R(0.5) * rho1 / p1, beta2 = R(0.5) * rho2 / p2;
     const R beta_ln = log_mean(beta1, beta2);
     const R p_hat = R(0.5) * (rho1 + rho2) / (beta1 + beta2);
     hhat += R(0.5) / beta_ln * g.gm1_av_inv + p_hat / rho_ln;
+    R p_mom = p_hat;
+    if constexpr (IsF32<R>::value) p_mom = (beta1 * A.pp + beta2 * B.pp) / (beta1 + beta2);
     R diss[DIM + 2];
-    scalar_dissipation<R, DIM>(g, q1, q2, n, diss);
+    scalar_dissipation<R, DIM>(g, A, B, n, diss);
     F[0] = rho_ln * vn - diss[0];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom[d] + p_hat * n[d] - diss[1 + d];
+    for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom[d] + p_mom * n[d] - diss[1 + d];
     F[E] = rho_ln * vn * hhat - diss[E];
   } else if (SURF == SURF_RANOCHA) {
     // include/RanochaFlux.hpp:81-134
     const R rho1 = q1[0], rho2 = q2[0];
     const R rho_ln = log_mean(rho1, rho2);
-    const R p1 = pressure<R, DIM>(g, q1), p2 = pressure<R, DIM>(g, q2);
-    const R pbar = R(0.5) * (p1 + p2);
+    const R p1 = A.p, p2 = B.p;
+    const R pbar = IsF32<R>::value ? R(0.5) * (A.pp + B.pp) : R(0.5) * (p1 + p2);
     R vbar[DIM];
     R ke = R(0), vn = R(0), fe = R(0);
 #pragma unroll
@@ -405,7 +493,7 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
     const R inv_beta_ln = (p1 * p2) / log_mean(rho1 * p2, rho2 * p1);
     const R ie = inv_beta_ln * g.inv_gm1;
     R diss[DIM + 2];
-    roe_dissipation<R, DIM>(g, q1, q2, n, diss);
+    roe_dissipation<R, DIM>(g, A, B, n, diss);
     F[0] = rho_ln * vn - diss[0];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) F[1 + d] = rho_ln * vn * vbar[d] + pbar * n[d] - diss[1 + d];
@@ -415,8 +503,8 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
     const R rho1 = q1[0], rho2 = q2[0];
     const R rho_mean = R(0.5) * (rho1 + rho2);
     const R ke1 = ke_density<R, DIM>(q1), ke2 = ke_density<R, DIM>(q2);
-    const R p1 = g.gm1 * (q1[E] - ke1), p2 = g.gm1 * (q2[E] - ke2);
-    const R pbar = R(0.5) * (p1 + p2);
+    const R p1 = A.p, p2 = B.p;
+    const R pbar = IsF32<R>::value ? R(0.5) * (A.pp + B.pp) : R(0.5) * (p1 + p2);
     R vbar[DIM];
     R ke_mean = R(0), vn = R(0);
 #pragma unroll
@@ -426,16 +514,20 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
       vn += vbar[d] * n[d];
       ke_mean += R(0.25) * ((v1 * v1) + (v2 * v2));
     }
-    const R h_mean = R(0.5) * ((q1[E] - ke1) / rho1 + p1 / rho1 + (q2[E] - ke2) / rho2 + p2 / rho2);
+    R h_mean;
+    if constexpr (IsF32<R>::value)
+      h_mean = R(0.5) * ((p1 * g.gm1_inv) / rho1 + p1 / rho1 + (p2 * g.gm1_inv) / rho2 + p2 / rho2);
+    else
+      h_mean = R(0.5) * ((q1[E] - ke1) / rho1 + p1 / rho1 + (q2[E] - ke2) / rho2 + p2 / rho2);
     R diss[DIM + 2];
-    roe_dissipation<R, DIM>(g, q1, q2, n, diss);
+    roe_dissipation<R, DIM>(g, A, B, n, diss);
     F[0] = rho_mean * vn - diss[0];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) F[1 + d] = rho_mean * vn * vbar[d] + pbar * n[d] - diss[1 + d];
     F[E] = rho_mean * (h_mean + ke_mean) * vn - diss[E];
   } else if (SURF == SURF_HLL) {
     // include/HLLFlux.hpp:53-116
-    const NState<R, DIM> L = nstate<R, DIM>(g, q1), Rs = nstate<R, DIM>(g, q2);
+    const NState<R, DIM> L = nstate<R, DIM>(A), Rs = nstate<R, DIM>(B);
     R un1 = R(0), un2 = R(0), nn = R(0);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -453,11 +545,11 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
       const R fn1 = normal_flux<R, DIM>(q1, L, n, e), fn2 = normal_flux<R, DIM>(q2, Rs, n, e);
       if (sL >= R(0)) F[e] = fn1;
       else if (sR <= R(0)) F[e] = fn2;
-      else F[e] = (sR * fn1 - sL * fn2 + sL * sR * (q2[e] - q1[e])) / (sR - sL);
+      else F[e] = (sR * fn1 - sL * fn2 + sL * sR * (B.d[e] - A.d[e])) / (sR - sL);
     }
   } else if (SURF == SURF_LLF) {
     // include/LaxFriedrichsFlux.hpp:188-211, include/NavierStokesFlux.hpp:16-41
-    const NState<R, DIM> L = nstate<R, DIM>(g, q1), Rs = nstate<R, DIM>(g, q2);
+    const NState<R, DIM> L = nstate<R, DIM>(A), Rs = nstate<R, DIM>(B);
     R vn1 = R(0), vn2 = R(0), nn = R(0);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -471,11 +563,11 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
 #pragma unroll
     for (int e = 0; e < DIM + 2; ++e) {
       const R nl = normal_flux<R, DIM>(q1, L, n, e), nr = normal_flux<R, DIM>(q2, Rs, n, e);
-      F[e] = R(0.5) * (nl + nr) - R(0.5) * lmax * (q2[e] - q1[e]);
+      F[e] = R(0.5) * (nl + nr) - R(0.5) * lmax * (B.d[e] - A.d[e]);
     }
   } else {
     // include/RoeFlux.hpp:42-149
-    const NState<R, DIM> left = nstate<R, DIM>(g, q1), right = nstate<R, DIM>(g, q2);
+    const NState<R, DIM> left = nstate<R, DIM>(A), right = nstate<R, DIM>(B);
     R nm2 = R(0);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) nm2 += n[d] * n[d];
@@ -503,7 +595,7 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const R *q1, cons
     }
     const R a2 = (g.gamma - R(1)) * (H - R(0.5) * u2);
     const R a = rsqrt_(a2);
-    const R dp = pR - pL, drho = rhoR - rhoL;
+    const R dp = right.pp - left.pp, drho = B.d[0] - A.d[0];
     const R am = R(0.5) * (dp - rho_roe * a * dun) / a2;
     const R ap = R(0.5) * (dp + rho_roe * a * dun) / a2;
     const R az = drho - dp / a2;
@@ -606,6 +698,84 @@ __device__ __forceinline__ int trace_node(int N, int lf, int fp) {
   if (dir == 0) return pos + N * (a + N * b);
   if (dir == 1) return a + N * (pos + N * b);
   return a + N * (b + N * pos);
+}
+
+// ---- LTE Helmholtz gas at a node with its recovered temperature T ---------
+// Per-node staging of the LTEEC volume kernel: conserved state, T, the table
+// cell of (rho, T) and the pressure.
+enum : int { LTE_P_T = 0, LTE_P_XI = 1, LTE_P_ETA = 2, LTE_P_DR = 3, LTE_P_DT = 4, LTE_P_OFF = 5,
+             LTE_P_P = 6, LTE_P_COUNT = 7 };
+
+__device__ __forceinline__ LteEval lte_unpack(const double *x /* LTE_P_* block */, double rho, int nx) {
+  LteEval s;
+  s.cell.off = (int)x[LTE_P_OFF];
+  s.cell.nx = nx;
+  s.cell.dr = x[LTE_P_DR];
+  s.cell.dt = x[LTE_P_DT];
+  s.xi = x[LTE_P_XI];
+  s.eta = x[LTE_P_ETA];
+  s.rho = rho;
+  s.T = x[LTE_P_T];
+  s.valid = true;
+  return s;
+}
+
+// include/LTEHelmholtzGasEOS.hpp:144-157: (beta (g - |u|^2/2), beta u, -beta)
+template <int DIM>
+__device__ __forceinline__ void lte_entropy_vars(const LteDev &t, const double *q, double T, double *w) {
+  const LteEval s = lte_at(t, q[0], T);
+  const double beta = 1 / s.T;
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
+  const double kinetic = (0.5 * m2 / q[0]) / q[0];
+  w[0] = beta * (lte_gibbs(t, s) - kinetic);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) w[1 + d] = beta * (q[1 + d] / q[0]);
+  w[DIM + 1] = -beta;
+}
+
+// include/LTEHelmholtzGasEOS.hpp:159-172: the energy slot carries grad T
+template <int DIM>
+__device__ __forceinline__ void lte_grad_entropy_to_prim(const double *q, double T, const double *dE,
+                                                         double *dP) {
+  constexpr int E = DIM + 1;
+  dP[0] = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) dP[1 + d] = T * dE[1 + d] + T * (q[1 + d] / q[0]) * dE[E];
+  dP[E] = T * T * dE[E];
+}
+
+// include/NavierStokesFlux.hpp:160-290 with the LTE transport planes
+// (include/LTETransport.hpp:33-65) and grad T taken from the energy slot
+// (include/LTEHelmholtzGasEOS.hpp:133-142).
+template <int DIM>
+__device__ __forceinline__ void lte_viscous_flux(const GasT<double> &g, const double *q, double T,
+                                                 const double *dp, double *vf) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+  const LteEval s = lte_at(g.lte, q[0], T);
+  const double mu = lte_transport(g.lte, s, 4);
+  const double kappa = lte_transport(g.lte, s, 5);
+  const double rho = q[0];
+  double div = 0.0;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) div += dp[i * NEQ + 1 + i];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) vf[d] = 0.0;
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    double ef = kappa * dp[dir * NEQ + E];
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) {
+      double tau;
+      if (mom == dir) tau = mu * (2.0 * dp[dir * NEQ + 1 + mom] - g.mu_bulk * div);
+      else tau = mu * (dp[dir * NEQ + 1 + mom] + dp[mom * NEQ + 1 + dir]);
+      vf[(1 + mom) * DIM + dir] = tau;
+    }
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) ef += (q[1 + mom] / rho) * vf[(1 + mom) * DIM + dir];
+    vf[E * DIM + dir] = ef;
+  }
 }
 
 }  // namespace thx

@@ -16,7 +16,9 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
   THX_TYPE(THX_PREC) k;
 #define THX_SET(S)                                             \
   k.face[S][0] = &launch_face<R, THX_DIM, S, false>;           \
-  k.face[S][1] = &launch_face<R, THX_DIM, S, true>;
+  k.face[S][1] = &launch_face<R, THX_DIM, S, true>;            \
+  k.faceb[S][0] = &launch_face_batched<R, THX_DIM, S, false>;  \
+  k.faceb[S][1] = &launch_face_batched<R, THX_DIM, S, true>;
   THX_SET(SURF_CHANDRASHEKAR)
   THX_SET(SURF_RANOCHA)
   THX_SET(SURF_PIROZZOLI)

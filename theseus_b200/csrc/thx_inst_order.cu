@@ -37,6 +37,15 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   k.vol[VOL_CENTRAL][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, true>;
   k.grad = &launch_grad<R, THX_DIM, THX_N>;
   k.blend = &launch_blend<R, THX_DIM, THX_N>;
+#define THX_SETB(V)                                                              \
+  k.volb[V][0] = &launch_volume_batched<R, THX_DIM, THX_N, V, false>;             \
+  k.volb[V][1] = &launch_volume_batched<R, THX_DIM, THX_N, V, true>;
+  THX_SETB(VOL_CHANDRASHEKAR)
+  THX_SETB(VOL_RANOCHA)
+  THX_SETB(VOL_PIROZZOLI)
+  THX_SETB(VOL_CENTRAL)
+#undef THX_SETB
+  k.gradb = &launch_grad_batched<R, THX_DIM, THX_N>;
   return k;
 }
 

@@ -32,7 +32,6 @@ struct Shape {
   static constexpr int NP = N * (N - 1) / 2;  // pairs per line
   static constexpr int NLINE = ND / N;
   static constexpr int PAIRS = NLINE * NP;     // pairs per element and direction
-  static constexpr int NPRIM = DIM + 3;
   static constexpr int OPS = ((2 * N * N + N + 7) / 8) * 8;  // Dhat2 | Dhat | w, padded
   static constexpr int DPAD = ((N * N + 7) / 8) * 8;
 };
@@ -80,8 +79,35 @@ __device__ __forceinline__ void pair_decode(int k, int &a, int &b) {
   b = a + 1 + k;
 }
 
-// Status bits written by kernels (read by thx_read_status).
-enum : unsigned { STATUS_NONPOSITIVE = 1u, STATUS_NONFINITE = 2u };
+// Status bits written by kernels (read by thx_read_status).  STATUS_LAUNCH:
+// a kernel was given less dynamic shared memory than its layout needs and
+// returned without doing any work.
+// STATUS_EOS: an LTE temperature recovery failed or left the table.
+enum : unsigned { STATUS_NONPOSITIVE = 1u, STATUS_NONFINITE = 2u, STATUS_LAUNCH = 4u,
+                  STATUS_EOS = 8u };
+
+__device__ __forceinline__ unsigned dynamic_smem_bytes() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+  return v;
+}
+
+// Shared-memory layout of the volume kernel, in elements of R:
+// [ops | prim + pair fluxes, or the viscous flux | state (NEEDQ) | metric].
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+struct VolSmem {
+  using S = Shape<DIM, N>;
+  static constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
+  static constexpr int PRIM = VOL == VOL_LTEEC ? S::NEQ + LTE_P_COUNT : nprim<R, DIM>();
+  static constexpr int REGION = S::EPB * (PRIM * S::ND + S::PAIRS * S::NEQ);
+  static constexpr int VISC = NS ? S::EPB * DIM * (S::NEQ - 1) * S::ND : 0;
+  static constexpr int SHARED = REGION > VISC ? REGION : VISC;
+  static constexpr int STATE = NEEDQ ? S::EPB * S::NEQ * S::ND : 0;
+  __host__ __device__ static constexpr size_t bytes(bool metric_per_node) {
+    return sizeof(R) * ((size_t)S::OPS + SHARED + STATE +
+                        (size_t)S::EPB * (metric_per_node ? S::ND * DIM * DIM : DIM * DIM));
+  }
+};
 
 template <typename R>
 struct VolArgs {
@@ -109,46 +135,53 @@ struct VolArgs {
   double *um;             // FP64 master state (read every stage, written by stage 3)
   double *y;              // FP64 stage state (written by stages 1 and 2)
   float *yf;              // FP32 working copy of the next RHS input (mixed mode) or nullptr
+  double off[5];          // yf = (float)(y - off[eq])
   unsigned *status;
 };
 
 // Surface flux with a run-time selector (used on subcell faces).
 template <typename R, int DIM>
-__device__ __noinline__ void surface_flux_rt(int kind, const GasT<R> &g, const R *q1, const R *q2,
-                                             const R *n, R *F) {
+__device__ __noinline__ void surface_flux_rt(int kind, const GasT<R> &g, const FState<R, DIM> &A,
+                                             const FState<R, DIM> &B, const R *n, R *F) {
   switch (kind) {
-    case SURF_CHANDRASHEKAR: surface_flux<R, DIM, SURF_CHANDRASHEKAR>(g, q1, q2, n, F); break;
-    case SURF_RANOCHA: surface_flux<R, DIM, SURF_RANOCHA>(g, q1, q2, n, F); break;
-    case SURF_PIROZZOLI: surface_flux<R, DIM, SURF_PIROZZOLI>(g, q1, q2, n, F); break;
-    case SURF_HLL: surface_flux<R, DIM, SURF_HLL>(g, q1, q2, n, F); break;
-    case SURF_ROE: surface_flux<R, DIM, SURF_ROE>(g, q1, q2, n, F); break;
-    default: surface_flux<R, DIM, SURF_LLF>(g, q1, q2, n, F); break;
+    case SURF_CHANDRASHEKAR: surface_flux<R, DIM, SURF_CHANDRASHEKAR>(g, A, B, n, F); break;
+    case SURF_RANOCHA: surface_flux<R, DIM, SURF_RANOCHA>(g, A, B, n, F); break;
+    case SURF_PIROZZOLI: surface_flux<R, DIM, SURF_PIROZZOLI>(g, A, B, n, F); break;
+    case SURF_HLL: surface_flux<R, DIM, SURF_HLL>(g, A, B, n, F); break;
+    case SURF_ROE: surface_flux<R, DIM, SURF_ROE>(g, A, B, n, F); break;
+    default: surface_flux<R, DIM, SURF_LLF>(g, A, B, n, F); break;
   }
 }
 
+// One CTA's work of the volume kernel: elements [block*EPB, block*EPB + EPB).
+// Shared by the one-case kernel (block = blockIdx.x) and the batched
+// persistent kernel (block from its work list).
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
-volume_kernel(const VolArgs<R> a) {
+__device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block) {
   using S = Shape<DIM, N>;
-  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = S::NPRIM, PAIRS = S::PAIRS;
+  static_assert(VOL != VOL_LTEEC || (!BLEND && !IsF32<R>::value), "LTEEC: FP64, no blending");
+  using L_ = VolSmem<R, DIM, N, VOL, NS, BLEND>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = L_::PRIM, PAIRS = S::PAIRS;
   constexpr int MB = DIM * DIM;
-  constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
+  constexpr bool NEEDQ = L_::NEEDQ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (dynamic_smem_bytes() < L_::bytes(a.met_ns != 0)) {
+    if (threadIdx.x == 0) atomicOr(a.status, STATUS_LAUNCH);
+    return;
+  }
   // [ops | prim | pair fluxes | state (NEEDQ) | metric]; the viscous flux of the
   // NS phase reuses the prim + pair-flux region, the FV rate the pair fluxes.
   R *sOps = reinterpret_cast<R *>(smem_raw);              // 2*N*N + N (padded)
   R *sPrim = sOps + S::OPS;                               // [EPB][NPRIM][ND]
   R *sFB = sPrim + EPB * NPRIM * ND;                      // [EPB][PAIRS][NEQ]
-  constexpr int REGION = EPB * (NPRIM * ND + PAIRS * NEQ);
-  constexpr int VISC = NS ? EPB * DIM * (NEQ - 1) * ND : 0;
-  R *sQ = sPrim + (REGION > VISC ? REGION : VISC);        // [EPB][NEQ][ND] if NEEDQ
-  R *sMet = sQ + (NEEDQ ? EPB * NEQ * ND : 0);            // per node or once per element
+  R *sQ = sPrim + L_::SHARED;                             // [EPB][NEQ][ND] if NEEDQ
+  R *sMet = sQ + L_::STATE;                               // per node or once per element
   R *sFv = sPrim;                                         // [EPB][DIM][NEQ-1][ND] (NS)
   const int mns = a.met_ns != 0 ? MB : 0;                 // metric node stride in smem
   const int mbk = a.met_ns != 0 ? ND * MB : MB;           // metric element block in smem
 
   const int tid = threadIdx.x;
-  const int e0 = blockIdx.x * EPB;
+  const int e0 = block * EPB;
   const long long L = (long long)a.ne * ND;
   for (int i = tid; i < 2 * N * N + N; i += blockDim.x) sOps[i] = a.ops[i];
   const R *sD2 = sOps;
@@ -163,15 +196,34 @@ volume_kernel(const VolArgs<R> a) {
     R q[NEQ];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
-    R pr[NPRIM];
-    node_prims<R, DIM, VOL>(a.gas, q, pr);
+    if constexpr (VOL == VOL_LTEEC) {
+      // conserved state, recovered T, its table cell and the pressure
+      const double T = a.gas.Tn[(long long)e * ND + n];
+      const LteEval sv = lte_at(a.gas.lte, q[0], T);
+      R pr[NPRIM];
 #pragma unroll
-    for (int k = 0; k < NPRIM; ++k) sPrim[(el * NPRIM + k) * ND + n] = pr[k];
-    if (NEEDQ) {
+      for (int k = 0; k < NEQ; ++k) pr[k] = q[k];
+      pr[NEQ + LTE_P_T] = T;
+      pr[NEQ + LTE_P_XI] = sv.xi;
+      pr[NEQ + LTE_P_ETA] = sv.eta;
+      pr[NEQ + LTE_P_DR] = sv.cell.dr;
+      pr[NEQ + LTE_P_DT] = sv.cell.dt;
+      pr[NEQ + LTE_P_OFF] = (double)sv.cell.off;
+      pr[NEQ + LTE_P_P] = sv.valid ? lte_pressure(a.gas.lte, sv) : 0.0;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+      for (int k = 0; k < NPRIM; ++k) sPrim[(el * NPRIM + k) * ND + n] = pr[k];
+      if (!sv.valid || !(q[0] > 0.0)) atomicOr(a.status, STATUS_EOS);
+    } else {
+      R pr[NPRIM];
+      node_prims<R, DIM, VOL>(a.gas, q, pr);
+#pragma unroll
+      for (int k = 0; k < NPRIM; ++k) sPrim[(el * NPRIM + k) * ND + n] = pr[k];
+      if (NEEDQ) {
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+      }
+      if (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))) atomicOr(a.status, STATUS_NONPOSITIVE);
     }
-    if (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))) atomicOr(a.status, STATUS_NONPOSITIVE);
     if (mns != 0 || n == 0) {
       const R *mp = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
 #pragma unroll
@@ -205,16 +257,24 @@ volume_kernel(const VolArgs<R> a) {
 #pragma unroll
       for (int d = 0; d < DIM; ++d)
         met[d] = R(0.5) * (sMet[pel * mbk + na * mns + dir * DIM + d] + sMet[pel * mbk + nb * mns + dir * DIM + d]);
-      if (VOL == VOL_CHANDRASHEKAR) vol_chandrashekar<R, DIM>(a.gas, A, B, met, F);
+      if constexpr (VOL == VOL_LTEEC) {
+        // include/LTEECFlux.hpp:11-84: the averaged metric passed as both rows
+        // (0.5*(m+m) == m exactly)
+        const LteEval sa = lte_unpack(A + NEQ, A[0], a.gas.lte.nx);
+        const LteEval sb = lte_unpack(B + NEQ, B[0], a.gas.lte.nx);
+        lte_ec_flux<DIM, false>(a.gas.lte, A, B, sa, sb, A[NEQ + LTE_P_P], B[NEQ + LTE_P_P], met, met, F);
+      } else if (VOL == VOL_CHANDRASHEKAR) vol_chandrashekar<R, DIM>(a.gas, A, B, met, F);
       else if (VOL == VOL_RANOCHA) vol_ranocha<R, DIM>(a.gas, A, B, met, F);
       else if (VOL == VOL_PIROZZOLI) vol_pirozzoli<R, DIM>(a.gas, A, B, met, F);
       else {
-        R QA[NEQ], QB[NEQ];
+        R RA[NEQ], RB[NEQ], QA[NEQ], QB[NEQ];
 #pragma unroll
         for (int k = 0; k < NEQ; ++k) {
-          QA[k] = sQ[(pel * NEQ + k) * ND + na];
-          QB[k] = sQ[(pel * NEQ + k) * ND + nb];
+          RA[k] = sQ[(pel * NEQ + k) * ND + na];
+          RB[k] = sQ[(pel * NEQ + k) * ND + nb];
         }
+        reconstruct<R, DIM>(a.gas, RA, QA);
+        reconstruct<R, DIM>(a.gas, RB, QB);
         vol_central<R, DIM>(QA, QB, A, B, met, F);
       }
 #pragma unroll
@@ -262,16 +322,19 @@ volume_kernel(const VolArgs<R> a) {
           const int le = e0 + lel;
           if (le >= a.ne || !(a.alpha[le] > 1e-16)) continue;
           const R *sub = a.sub[dir] + (long long)le * a.sub_es[dir];
-          R s1[NEQ], s2[NEQ], fn[NEQ], dus[NEQ];
+          R raw[NEQ], fn[NEQ], dus[NEQ];
+          FState<R, DIM> s1, s2;
           int id1 = line_node<DIM, N>(dir, line, 0);
 #pragma unroll
-          for (int k = 0; k < NEQ; ++k) { dus[k] = R(0); s1[k] = sQ[(lel * NEQ + k) * ND + id1]; }
+          for (int k = 0; k < NEQ; ++k) { dus[k] = R(0); raw[k] = sQ[(lel * NEQ + k) * ND + id1]; }
+          make_fstate<R, DIM>(a.gas, raw, s1);
           for (int i = 0; i < N; ++i) {
             R Ji = a.jac[(long long)le * a.jac_es + (long long)id1 * a.jac_ns];
             if (i < N - 1) {
               const int id2 = line_node<DIM, N>(dir, line, i + 1);
 #pragma unroll
-              for (int k = 0; k < NEQ; ++k) s2[k] = sQ[(lel * NEQ + k) * ND + id2];
+              for (int k = 0; k < NEQ; ++k) raw[k] = sQ[(lel * NEQ + k) * ND + id2];
+              make_fstate<R, DIM>(a.gas, raw, s2);
               R nrm[DIM];
 #pragma unroll
               for (int d = 0; d < DIM; ++d) nrm[d] = sub[id2 * DIM + d];
@@ -286,7 +349,8 @@ volume_kernel(const VolArgs<R> a) {
                 dst = dir == 0 ? dus[k] : dst + dus[k];
               }
 #pragma unroll
-              for (int k = 0; k < NEQ; ++k) { dus[k] = fn[k]; s1[k] = s2[k]; }
+              for (int k = 0; k < NEQ; ++k) dus[k] = fn[k];
+              s1 = s2;
               id1 = id2;
             } else {
 #pragma unroll
@@ -411,9 +475,14 @@ volume_kernel(const VolArgs<R> a) {
         y = (1.0 / 3.0) * a.um[i] + (2.0 / 3.0) * y;
         a.um[i] = y;
       }
-      if (a.yf) a.yf[i] = (float)y;
+      if (a.yf) a.yf[i] = (float)(y - a.off[k]);
     }
   }
+}
+
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const VolArgs<R> a) {
+  volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -429,13 +498,13 @@ struct FaceArgs {
   GasT<R> gas;
 };
 
+// Face point t (face t / nfp, point t % nfp) of one case.
 template <typename R, int DIM, int SURF, bool NS>
-__global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
+__device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long t) {
   constexpr int NEQ = DIM + 2;
   const int N = a.N;
   const int nfp = DIM == 2 ? N : N * N;
   const int nd = DIM == 2 ? N * N : N * N * N;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)a.nf * nfp) return;
   const int f = (int)(t / nfp), fp = (int)(t % nfp);
   const long long L = (long long)a.ne * nd;
@@ -448,7 +517,21 @@ __global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
   const R *np = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) nrm[d] = np[d];
-  surface_flux<R, DIM, SURF>(a.gas, qm, qp, nrm, F);
+  if constexpr (SURF == SURF_LTEEC) {
+    // include/LTEECFlux.hpp:86-99 with the Lax dissipation
+    // (include/DissipationOperator.hpp:15-55); T recovered per node
+    static_assert(!IsF32<R>::value, "LTEEC: FP64 only");
+    const LteEval sm = lte_at(a.gas.lte, qm[0], a.gas.Tn[im]);
+    const LteEval sp = lte_at(a.gas.lte, qp[0], a.gas.Tn[ip]);
+    const double pm = sm.valid ? lte_pressure(a.gas.lte, sm) : 0.0;
+    const double pp = sp.valid ? lte_pressure(a.gas.lte, sp) : 0.0;
+    lte_ec_flux<DIM, true>(a.gas.lte, qm, qp, sm, sp, pm, pp, nrm, nrm, F);
+  } else {
+    FState<R, DIM> A, B;
+    make_fstate<R, DIM>(a.gas, qm, A);
+    make_fstate<R, DIM>(a.gas, qp, B);
+    surface_flux<R, DIM, SURF>(a.gas, A, B, nrm, F);
+  }
   if (NS) {
     // include/DGSEMIntegrator.hpp:261-316: F* -= n . avg(F_v), with the physical
     // viscous flux of both traces as stored by grad_kernel (mass row zero)
@@ -464,6 +547,11 @@ __global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
   }
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) a.fstar[((long long)f * NEQ + k) * nfp + fp] = F[k];
+}
+
+template <typename R, int DIM, int SURF, bool NS>
+__global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
+  face_body<R, DIM, SURF, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -483,31 +571,68 @@ struct GradArgs {
   long long w_fs, w_ps;
   const R *D;  // N*N
   GasT<R> gas;
+  unsigned *status;
 };
+
+template <typename R, int DIM, int N>
+__host__ __device__ constexpr size_t grad_smem_bytes() {
+  using S = Shape<DIM, N>;
+  return sizeof(R) * (S::DPAD + (size_t)S::EPB * S::NEQ * (S::ND + 2 * DIM * S::NFP));
+}
 
 // BR1 gradient (include/NSOperator_impl.hpp:11-159,194-517;
 // include/DGSEMIntegrator.hpp:764-850,1011-1044)
-template <typename R, int DIM, int N>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
+template <typename R, int DIM, int N, bool LTE>
+__device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block) {
+  static_assert(!LTE || !IsF32<R>::value, "LTE gas: FP64 only");
   using S = Shape<DIM, N>;
-  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NFP = S::NFP, NLF = 2 * DIM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded)
-  R *sS = sD + S::DPAD;                      // [EPB][NEQ][ND]
+  R *sS = sD + S::DPAD;                      // [EPB][NEQ][ND] own entropy variables
+  R *sN = sS + EPB * NEQ * ND;               // [EPB][2*DIM][NEQ][NFP] neighbour traces
+  if (dynamic_smem_bytes() < grad_smem_bytes<R, DIM, N>()) {
+    if (threadIdx.x == 0 && a.status) atomicOr(a.status, STATUS_LAUNCH);
+    return;
+  }
   const int tid = threadIdx.x;
   for (int i = tid; i < N * N; i += blockDim.x) sD[i] = a.D[i];
   const int el = tid / ND, n = tid % ND;
-  const int e = blockIdx.x * EPB + el;
+  const int e0 = block * EPB;
+  const int e = e0 + el;
   const bool active = (el < EPB) && (e < a.ne);
   const long long L = (long long)a.ne * ND;
   R q[NEQ];
   if (active) {
+    R raw[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
+    reconstruct<R, DIM>(a.gas, raw, q);
     R w[NEQ];
-    entropy_vars<R, DIM>(a.gas, q, w);
+    if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, q, a.gas.Tn[(long long)e * ND + n], w);
+    else entropy_vars<R, DIM>(a.gas, q, w);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) sS[(el * NEQ + k) * ND + n] = w[k];
+  }
+  // entropy variables of the neighbour's trace at every face point of the
+  // CTA's elements, one converged task per face point
+  for (int t = tid; t < EPB * NLF * NFP; t += blockDim.x) {
+    const int tel = t / (NLF * NFP), lf = (t / NFP) % NLF, fp = t % NFP;
+    const int te = e0 + tel;
+    if (te >= a.ne) continue;
+    const int fs = a.elem_face[te * NLF + lf];
+    if (fs < 0) continue;
+    const int f = fs >> 1, side = fs & 1;
+    const int eo = a.face_elem[2 * f + 1 - side];
+    const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
+    R ro[NEQ], qo[NEQ], so[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
+    reconstruct<R, DIM>(a.gas, ro, qo);
+    if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], so);
+    else entropy_vars<R, DIM>(a.gas, qo, so);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sN[((tel * NLF + lf) * NEQ + k) * NFP + fp] = so[k];
   }
   __syncthreads();
   if (!active) return;
@@ -560,12 +685,9 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const Grad
       if (fs < 0) continue;
       const int f = fs >> 1, side = fs & 1;
       const int fp = face_point<DIM, N>(dir, c);
-      const int eo = a.face_elem[2 * f + 1 - side];
-      const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
-      R qo[NEQ], so[NEQ];
+      R so[NEQ];
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) qo[k] = a.u[k * L + (long long)eo * ND + no];
-      entropy_vars<R, DIM>(a.gas, qo, so);
+      for (int k = 0; k < NEQ; ++k) so[k] = sN[((el * NLF + lf) * NEQ + k) * NFP + fp];
       const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
       const R w = side == 0 ? a.wm[wi] : a.wp[wi];
       const R *nr = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
@@ -588,16 +710,53 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const Grad
   // entropy gradient -> primitive gradient, then the physical viscous flux
   // (include/NavierStokesFlux.hpp:160-290) that the face and volume kernels use
   R dp[DIM * NEQ];
-#pragma unroll
-  for (int cc = 0; cc < DIM; ++cc) grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dp + cc * NEQ);
   R vf[NEQ * DIM];
-  viscous_flux<R, DIM>(a.gas, q, dp, vf);
+  if constexpr (LTE) {
+    const double T = a.gas.Tn[(long long)e * ND + n];
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc) lte_grad_entropy_to_prim<DIM>(q, T, g[cc], dp + cc * NEQ);
+    lte_viscous_flux<DIM>(a.gas, q, T, dp, vf);
+  } else {
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc) grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dp + cc * NEQ);
+    viscous_flux<R, DIM>(a.gas, q, dp, vf);
+  }
   constexpr int NV = NEQ - 1;
 #pragma unroll
   for (int d = 0; d < DIM; ++d)
 #pragma unroll
     for (int k = 0; k < NV; ++k)
       a.vflux[((long long)d * NV + k) * L + (long long)e * ND + n] = vf[(1 + k) * DIM + d];
+}
+
+template <typename R, int DIM, int N, bool LTE>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
+  grad_body<R, DIM, N, LTE>(a, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// LTE temperature recovery, once per node and right-hand side
+// (include/LTEHelmholtzGasEOS.hpp:59-76 evaluates it on every gas query; the
+// face, gradient and volume kernels read the stored T instead).
+template <int DIM>
+__global__ void __launch_bounds__(256) lte_temperature_kernel(const double *u, long long L, LteDev t,
+                                                              double *Tn, unsigned *status) {
+  constexpr int NEQ = DIM + 2;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride) {
+    double q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) q[k] = u[k * L + i];
+    double m2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
+    const double ke = 0.5 * m2 / q[0];
+    const double ei = (q[DIM + 1] - ke) / q[0];
+    int st;
+    const double T = lte_temperature(t, q[0], ei, &st);
+    Tn[i] = T;
+    if (st != LTE_CONVERGED) atomicOr(status, STATUS_EOS);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -627,9 +786,10 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const Ble
   const bool active = (el < EPB) && (e < a.ne);
   const long long L = (long long)a.ne * ND;
   if (active) {
-    R q[NEQ];
+    R raw[NEQ], q[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
+    reconstruct<R, DIM>(a.gas, raw, q);
     sA[el * ND + n] = (double)(pressure<R, DIM>(a.gas, q) * q[0]);
   }
   __syncthreads();
@@ -682,18 +842,17 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const Ble
 
 // ---------------------------------------------------------------------------
 // SSP-RK3 stage updates (mfem::RK3SSPSolver::Step order) for the unfused path.
-template <typename R>
-__global__ void rk_stage_kernel(int stage, long long n, double dt, const R *k, double *um,
-                                double *y, float *yf) {
+// Conversions between the FP64 L-vector and the FP32 working copy u - off.
+struct Offsets { double v[5]; };
+static __global__ void to_working(long long L, int neq, const double *src, float *dst, Offsets off) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const double kk = (double)k[i];
-    double v;
-    if (stage == 1) { v = um[i] + dt * kk; y[i] = v; }
-    else if (stage == 2) { v = y[i] + dt * kk; v = 0.75 * um[i] + 0.25 * v; y[i] = v; }
-    else { v = y[i] + dt * kk; v = (1.0 / 3.0) * um[i] + (2.0 / 3.0) * v; um[i] = v; }
-    if (yf) yf[i] = (float)v;
-  }
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L * neq; i += stride)
+    dst[i] = (float)(src[i] - off.v[i / L]);
+}
+static __global__ void widen(long long n, const float *src, double *dst) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    dst[i] = (double)src[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -791,6 +950,53 @@ __global__ void stability_kernel(const StabArgs a) {
     atomicMax(&a.out[0], (unsigned long long)__double_as_longlong(adv));
     atomicMax(&a.out[1], (unsigned long long)__double_as_longlong(sur));
     atomicMax(&a.out[2], (unsigned long long)__double_as_longlong(dif));
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched persistent forms: one launch serves every case of a batch group.
+// work[w] names a per-case argument record (item) and a CTA-sized block of
+// that case; a fixed grid walks the list, whose length *nwork is read on the
+// device, so a captured graph stays valid while cases come and go.
+struct BatchWork {
+  int item;
+  int block;
+};
+
+template <typename R, int DIM, int N, int VOL, bool NS>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+volume_batched(const VolArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
+               const int *__restrict__ nwork) {
+  const int n = *nwork;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    __syncthreads();  // the previous item's shared memory is free
+    const BatchWork it = work[w];
+    volume_body<R, DIM, N, VOL, NS, false>(args[it.item], it.block);
+  }
+}
+
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+grad_batched(const GradArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
+             const int *__restrict__ nwork) {
+  const int n = *nwork;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    __syncthreads();
+    const BatchWork it = work[w];
+    grad_body<R, DIM, N, false>(args[it.item], it.block);
+  }
+}
+
+// face work blocks are 128 face points
+template <typename R, int DIM, int SURF, bool NS>
+__global__ void __launch_bounds__(128)
+face_batched(const FaceArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
+             const int *__restrict__ nwork) {
+  const int n = *nwork;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const BatchWork it = work[w];
+    face_body<R, DIM, SURF, NS>(args[it.item], (long long)it.block * 128 + threadIdx.x);
   }
 }
 

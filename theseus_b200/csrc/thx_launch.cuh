@@ -3,6 +3,8 @@
 #pragma once
 #include "thx_kernels.cuh"
 
+#include <algorithm>
+
 namespace thx {
 
 using PREC_T_0 = double;
@@ -12,16 +14,21 @@ template <typename R> using VolLaunch = cudaError_t (*)(const VolArgs<R> &, cuda
 template <typename R> using FaceLaunch = cudaError_t (*)(const FaceArgs<R> &, cudaStream_t);
 template <typename R> using GradLaunch = cudaError_t (*)(const GradArgs<R> &, cudaStream_t, int prepare);
 template <typename R> using BlendLaunch = cudaError_t (*)(const BlendArgs<R> &, cudaStream_t);
+// batched persistent forms: (argument table, work list, device work count,
+// grid size, stream, prepare)
+template <typename R>
+using VolBatchLaunch = cudaError_t (*)(const VolArgs<R> *, const BatchWork *, const int *, int,
+                                       cudaStream_t, int);
+template <typename R>
+using GradBatchLaunch = cudaError_t (*)(const GradArgs<R> *, const BatchWork *, const int *, int,
+                                        cudaStream_t, int);
+template <typename R>
+using FaceBatchLaunch = cudaError_t (*)(const FaceArgs<R> *, const BatchWork *, const int *, int,
+                                        cudaStream_t, int);
 
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 constexpr size_t volume_smem_bytes(bool metric_per_node) {
-  using S = Shape<DIM, N>;
-  constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
-  constexpr size_t region = (size_t)S::EPB * (S::NPRIM * S::ND + S::PAIRS * S::NEQ);
-  constexpr size_t visc = NS ? (size_t)S::EPB * DIM * (S::NEQ - 1) * S::ND : 0;
-  const size_t met = (size_t)S::EPB * (metric_per_node ? S::ND * DIM * DIM : DIM * DIM);
-  return sizeof(R) * (S::OPS + (region > visc ? region : visc) +
-                      (NEEDQ ? (size_t)S::EPB * S::NEQ * S::ND : 0) + met);
+  return VolSmem<R, DIM, N, VOL, NS, BLEND>::bytes(metric_per_node);
 }
 
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
@@ -49,16 +56,59 @@ cudaError_t launch_face(const FaceArgs<R> &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <typename R, int DIM, int N>
+template <typename R, int DIM, int N, bool LTE = false>
 cudaError_t launch_grad(const GradArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
-  constexpr size_t smem = sizeof(R) * (S::DPAD + (size_t)S::EPB * S::NEQ * S::ND);
+  constexpr size_t smem = grad_smem_bytes<R, DIM, N>();
   if (prepare)
-    return cudaFuncSetAttribute(grad_kernel<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(grad_kernel<R, DIM, N, LTE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem);
   if (a.ne <= 0) return cudaSuccess;
   const int grid = (a.ne + S::EPB - 1) / S::EPB;
-  grad_kernel<R, DIM, N><<<grid, S::THREADS, smem, s>>>(a);
+  grad_kernel<R, DIM, N, LTE><<<grid, S::THREADS, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int DIM>
+cudaError_t launch_lte_temperature(const double *u, long long L, const LteDev &t, double *Tn,
+                                   unsigned *status, cudaStream_t s) {
+  if (L <= 0) return cudaSuccess;
+  const int grid = (int)std::min<long long>((L + 255) / 256, 148LL * 8);
+  lte_temperature_kernel<DIM><<<grid, 256, 0, s>>>(u, L, t, Tn, status);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int N, int VOL, bool NS>
+cudaError_t launch_volume_batched(const VolArgs<R> *args, const BatchWork *work, const int *nwork,
+                                  int grid, cudaStream_t s, int prepare) {
+  using S = Shape<DIM, N>;
+  constexpr size_t smem = volume_smem_bytes<R, DIM, N, VOL, NS, false>(true);
+  if (prepare)
+    return cudaFuncSetAttribute(volume_batched<R, DIM, N, VOL, NS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (grid <= 0) return cudaSuccess;
+  volume_batched<R, DIM, N, VOL, NS><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int N>
+cudaError_t launch_grad_batched(const GradArgs<R> *args, const BatchWork *work, const int *nwork,
+                                int grid, cudaStream_t s, int prepare) {
+  using S = Shape<DIM, N>;
+  constexpr size_t smem = grad_smem_bytes<R, DIM, N>();
+  if (prepare)
+    return cudaFuncSetAttribute(grad_batched<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+  if (grid <= 0) return cudaSuccess;
+  grad_batched<R, DIM, N><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int SURF, bool NS>
+cudaError_t launch_face_batched(const FaceArgs<R> *args, const BatchWork *work, const int *nwork,
+                                int grid, cudaStream_t s, int prepare) {
+  if (prepare || grid <= 0) return cudaSuccess;
+  face_batched<R, DIM, SURF, NS><<<grid, 128, 0, s>>>(args, work, nwork);
   return cudaGetLastError();
 }
 
@@ -71,10 +121,27 @@ cudaError_t launch_blend(const BlendArgs<R> &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-struct OrderKernels0 { VolLaunch<double> vol[4][2][2]; GradLaunch<double> grad; BlendLaunch<double> blend; };
-struct OrderKernels1 { VolLaunch<float> vol[4][2][2]; GradLaunch<float> grad; BlendLaunch<float> blend; };
-struct FaceKernels0 { FaceLaunch<double> face[6][2]; };
-struct FaceKernels1 { FaceLaunch<float> face[6][2]; };
+template <typename R>
+struct OrderKernelsT {
+  VolLaunch<R> vol[4][2][2];     // [volume flux][ns][blend]
+  GradLaunch<R> grad;
+  BlendLaunch<R> blend;
+  VolBatchLaunch<R> volb[4][2];  // [volume flux][ns]
+  GradBatchLaunch<R> gradb;
+};
+template <typename R>
+struct FaceKernelsT {
+  FaceLaunch<R> face[6][2];      // [surface flux][ns]
+  FaceBatchLaunch<R> faceb[6][2];
+};
+using OrderKernels0 = OrderKernelsT<double>;
+using OrderKernels1 = OrderKernelsT<float>;
+using FaceKernels0 = FaceKernelsT<double>;
+using FaceKernels1 = FaceKernelsT<float>;
+// LTE Helmholtz gas, FP64: LTEEC volume kernel [euler|ns], gradient, face
+// flux [euler|ns].
+struct LteKernels { VolLaunch<double> vol[2]; GradLaunch<double> grad; };
+struct LteFaceKernels { FaceLaunch<double> face[2]; };
 
 #define THX_DECLARE_ORDER(P, D, N) OrderKernels##P order_kernels_##P##_##D##_##N();
 #define THX_DECLARE_FACE(P, D) FaceKernels##P face_kernels_##P##_##D();
@@ -83,6 +150,11 @@ THX_FOR_ORDERS(THX_DECLARE_ORDER, 0, 2)
 THX_FOR_ORDERS(THX_DECLARE_ORDER, 0, 3)
 THX_FOR_ORDERS(THX_DECLARE_ORDER, 1, 2)
 THX_FOR_ORDERS(THX_DECLARE_ORDER, 1, 3)
+#define THX_DECLARE_LTE(P, D, N) LteKernels lte_kernels_##D##_##N();
+THX_FOR_ORDERS(THX_DECLARE_LTE, 0, 2)
+THX_FOR_ORDERS(THX_DECLARE_LTE, 0, 3)
+LteFaceKernels lte_face_kernels_2();
+LteFaceKernels lte_face_kernels_3();
 THX_DECLARE_FACE(0, 2)
 THX_DECLARE_FACE(0, 3)
 THX_DECLARE_FACE(1, 2)

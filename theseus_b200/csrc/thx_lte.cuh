@@ -1,0 +1,341 @@
+// thx_lte.cuh -- LTE Helmholtz equation of state and the LTEEC flux, for host
+// and device (FP64).
+//
+// Restates, in the reference's operation order:
+//   table layout, cell search        include/LTEHelmholtzTable.hpp:13-35,83-105
+//   bicubic Hermite evaluation       include/LTEHelmholtzInterpolation.hpp:15-212
+//   state evaluation, Newton T(rho,e) include/LTEHelmholtzEOS.hpp:14-223
+//   Itoh-Abe discrete gradients      include/LTEHelmholtzEOS.hpp:225-397
+//   gas adapter (entropy variables,  include/LTEHelmholtzGasEOS.hpp:10-172,
+//     gradient conversion, transport) include/LTETransport.hpp:19-66
+//   LTEEC flux                       include/LTEECFlux.hpp:11-99
+// Failed recoveries are reported through a status flag instead of the
+// reference's device trap.
+#pragma once
+#include <cuda_runtime.h>
+#include <cmath>
+
+namespace thx {
+
+#define THX_HD __host__ __device__ __forceinline__
+// The discrete gradients and the Newton recovery are called, not inlined:
+// inlined into a flux they multiply its register footprint.
+#define THX_HDC static __host__ __device__ __noinline__
+
+struct LteDev {
+  int nx = 0, ny = 0;
+  const double *rho = nullptr, *T = nullptr, *e = nullptr;
+  const double *planes = nullptr;  // [6][ny][nx]
+  const double *inv = nullptr;     // [ny][nx]
+};
+
+THX_HD int lte_find_cell(const double *grid, int count, double v) {
+  if (count < 2 || !isfinite(v) || v < grid[0] || v > grid[count - 1]) return -1;
+  int lo = 0, hi = count - 1;
+  while (hi - lo > 1) {
+    const int mid = lo + (hi - lo) / 2;
+    if (v < grid[mid]) hi = mid;
+    else lo = mid;
+  }
+  return lo;
+}
+
+template <int D> THX_HD double hpos(int side, double x) {
+  const double x2 = x * x;
+  if (D == 0) { const double x3 = x2 * x; return side == 0 ? 2 * x3 - 3 * x2 + 1 : -2 * x3 + 3 * x2; }
+  if (D == 1) return side == 0 ? 6 * x2 - 6 * x : -6 * x2 + 6 * x;
+  return side == 0 ? 12 * x - 6 : -12 * x + 6;
+}
+template <int D> THX_HD double hslope(int side, double x) {
+  const double x2 = x * x;
+  if (D == 0) { const double x3 = x2 * x; return side == 0 ? x3 - 2 * x2 + x : x3 - x2; }
+  if (D == 1) return side == 0 ? 3 * x2 - 4 * x + 1 : 3 * x2 - 2 * x;
+  return side == 0 ? 6 * x - 4 : 6 * x - 2;
+}
+template <int D> THX_HD double hdivpos(int side, double x, double y) {
+  double v;
+  if (D == 0) v = 2 * (x * x + x * y + y * y) - 3 * (x + y);
+  else if (D == 1) v = 6 * (x + y) - 6;
+  else v = 12;
+  return side == 0 ? v : -v;
+}
+template <int D> THX_HD double hdivslope(int side, double x, double y) {
+  if (D == 0) return x * x + x * y + y * y - (side == 0 ? 2 : 1) * (x + y) + (side == 0 ? 1 : 0);
+  if (D == 1) return 3 * (x + y) - (side == 0 ? 4 : 2);
+  return 6;
+}
+template <int D> THX_HD double hscale(double w) { return D == 0 ? 1.0 : (D == 1 ? w : w * w); }
+
+// One table cell: lower-corner index into a plane, widths, density count.
+struct LteCell {
+  int off;       // j*nx + i
+  int nx;
+  double dr, dt;
+};
+
+template <int DR, int DT>
+THX_HD double lte_eval(const LteDev &t, const LteCell &c, double xi, double eta) {
+  const long ps = (long)t.nx * t.ny;
+  const double *H = t.planes + c.off, *Hr = H + ps, *HT = H + 2 * ps, *HrT = H + 3 * ps;
+  double r = 0.0;
+#pragma unroll
+  for (int ds = 0; ds < 2; ++ds) {
+    const double dv = hpos<DR>(ds, xi), dsl = hslope<DR>(ds, xi);
+#pragma unroll
+    for (int ts = 0; ts < 2; ++ts) {
+      const int o = ds + ts * c.nx;
+      const double tv = hpos<DT>(ts, eta), tsl = hslope<DT>(ts, eta);
+      r += H[o] * dv * tv;
+      r += (Hr[o] * c.dr) * dsl * tv;
+      r += (HT[o] * c.dt) * dv * tsl;
+      r += (HrT[o] * c.dr * c.dt) * dsl * tsl;
+    }
+  }
+  return r / (hscale<DR>(c.dr) * hscale<DT>(c.dt));
+}
+
+// Divided difference along AXIS (0: density, 1: temperature) within one cell.
+template <int AXIS, int DR, int DT>
+THX_HD double lte_divided(const LteDev &t, const LteCell &c, double xi1, double eta1, double xi2,
+                          double eta2) {
+  const long ps = (long)t.nx * t.ny;
+  const double *H = t.planes + c.off, *Hr = H + ps, *HT = H + 2 * ps, *HrT = H + 3 * ps;
+  double r = 0.0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double rv = AXIS == 0 ? hdivpos<DR>(i, xi1, xi2) : hpos<DR>(i, xi1);
+    const double rs = AXIS == 0 ? hdivslope<DR>(i, xi1, xi2) : hslope<DR>(i, xi1);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const double tv = AXIS == 1 ? hdivpos<DT>(j, eta1, eta2) : hpos<DT>(j, eta1);
+      const double ts = AXIS == 1 ? hdivslope<DT>(j, eta1, eta2) : hslope<DT>(j, eta1);
+      const int o = i + j * c.nx;
+      r += H[o] * rv * tv;
+      r += (Hr[o] * c.dr) * rs * tv;
+      r += (HT[o] * c.dt) * rv * ts;
+      r += (HrT[o] * c.dr * c.dt) * rs * ts;
+    }
+  }
+  const double sc = hscale<DR>(c.dr) * hscale<DT>(c.dt) * (AXIS == 0 ? c.dr : c.dt);
+  return r / sc;
+}
+
+struct LteEval {
+  LteCell cell;
+  double xi, eta, rho, T;
+  bool valid;
+};
+
+THX_HD LteEval lte_at(const LteDev &t, double rho, double T) {
+  LteEval r;
+  r.valid = false;
+  r.cell = {0, t.nx, 0.0, 0.0};
+  r.xi = r.eta = r.rho = r.T = 0.0;
+  const int i = lte_find_cell(t.rho, t.nx, rho), j = lte_find_cell(t.T, t.ny, T);
+  if (i < 0 || j < 0) return r;
+  const double dr = t.rho[i + 1] - t.rho[i], dt = t.T[j + 1] - t.T[j];
+  r.cell = {j * t.nx + i, t.nx, dr, dt};
+  r.xi = (rho - t.rho[i]) / dr;
+  r.eta = (T - t.T[j]) / dt;
+  r.rho = rho;
+  r.T = T;
+  r.valid = true;
+  return r;
+}
+
+THX_HD double lte_pressure(const LteDev &t, const LteEval &s) {
+  return s.rho * s.rho * lte_eval<1, 0>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_energy(const LteDev &t, const LteEval &s) {
+  return lte_eval<0, 0>(t, s.cell, s.xi, s.eta) - s.T * lte_eval<0, 1>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_gibbs(const LteDev &t, const LteEval &s) {
+  return lte_eval<0, 0>(t, s.cell, s.xi, s.eta) + s.rho * lte_eval<1, 0>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_dp_drho(const LteDev &t, const LteEval &s) {
+  return 2 * s.rho * lte_eval<1, 0>(t, s.cell, s.xi, s.eta) +
+         s.rho * s.rho * lte_eval<2, 0>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_dp_dT(const LteDev &t, const LteEval &s) {
+  return s.rho * s.rho * lte_eval<1, 1>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_dg_drho(const LteDev &t, const LteEval &s) {
+  return 2 * lte_eval<1, 0>(t, s.cell, s.xi, s.eta) + s.rho * lte_eval<2, 0>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_dg_dT(const LteDev &t, const LteEval &s) {
+  return lte_eval<0, 1>(t, s.cell, s.xi, s.eta) + s.rho * lte_eval<1, 1>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_cv(const LteDev &t, const LteEval &s) {
+  return -s.T * lte_eval<0, 2>(t, s.cell, s.xi, s.eta);
+}
+THX_HD double lte_c2(const LteDev &t, const LteEval &s) {
+  const double m = lte_eval<1, 1>(t, s.cell, s.xi, s.eta);
+  return lte_dp_drho(t, s) - s.rho * s.rho * m * m / lte_eval<0, 2>(t, s.cell, s.xi, s.eta);
+}
+// bilinear transport plane (4: mu, 5: lambda)
+THX_HD double lte_transport(const LteDev &t, const LteEval &s, int prop) {
+  const double *p = t.planes + (long)prop * t.nx * t.ny + s.cell.off;
+  return p[0] * (1 - s.xi) * (1 - s.eta) + p[1] * s.xi * (1 - s.eta) + p[t.nx] * (1 - s.xi) * s.eta +
+         p[t.nx + 1] * s.xi * s.eta;
+}
+
+enum LteStatus { LTE_CONVERGED = 0, LTE_OUTSIDE = 1, LTE_INVALID = 2, LTE_ITERATIONS = 3 };
+
+// Inverse-table guess, then Newton on e(rho, T) with the analytic cv.
+THX_HDC double lte_temperature(const LteDev &t, double rho, double e, int *status) {
+  *status = LTE_OUTSIDE;
+  const int i = lte_find_cell(t.rho, t.nx, rho), j = lte_find_cell(t.e, t.ny, e);
+  if (i < 0 || j < 0) return 0.0;
+  const double x = (rho - t.rho[i]) / (t.rho[i + 1] - t.rho[i]);
+  const double y = (e - t.e[j]) / (t.e[j + 1] - t.e[j]);
+  const double *p = t.inv + j * t.nx + i;
+  const double lower = p[0] + x * (p[1] - p[0]);
+  const double upper = p[t.nx] + x * (p[t.nx + 1] - p[t.nx]);
+  double T = lower + y * (upper - lower);
+  for (int it = 0; it < 100; ++it) {
+    const LteEval s = lte_at(t, rho, T);
+    if (!s.valid) return T;
+    const double cv = lte_cv(t, s), guess = lte_energy(t, s);
+    if (!isfinite(cv) || cv <= 0 || !isfinite(guess)) { *status = LTE_INVALID; return T; }
+    const double step = (e - guess) / cv;
+    const double next = T + step;
+    const bool inside = isfinite(next) && next >= t.T[0] && next <= t.T[t.ny - 1];
+    if (fabs(step) <= 1e-9 + 1e-12 * T) {
+      if (next < t.T[0]) T = t.T[0];
+      else if (next > t.T[t.ny - 1]) T = t.T[t.ny - 1];
+      else T = next;
+      *status = LTE_CONVERGED;
+      return T;
+    }
+    T = next;
+    if (!inside) return T;
+  }
+  *status = LTE_ITERATIONS;
+  return T;
+}
+
+// Recover T from a conserved state and evaluate there (adapter evaluate()).
+template <int DIM>
+THX_HD LteEval lte_state(const LteDev &t, const double *q, bool *bad) {
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
+  const double e = (q[DIM + 1] - 0.5 * m2 / q[0]) / q[0];
+  int st;
+  const double T = lte_temperature(t, q[0], e, &st);
+  LteEval s = lte_at(t, q[0], T);
+  if (st != LTE_CONVERGED || !s.valid) *bad = true;
+  return s;
+}
+
+// ---- discrete gradients of f/T in (rho, beta=1/T); f = p (P=0) or g (P=1) ---
+template <int P> THX_HD double lte_value(const LteDev &t, const LteEval &s) {
+  return P == 0 ? lte_pressure(t, s) : lte_gibbs(t, s);
+}
+
+template <int P>
+THX_HD double lte_density_secant(const LteDev &t, const LteEval &a, const LteEval &b, double eta) {
+  const LteCell &c = a.cell;
+  const double r1 = a.rho, r2 = b.rho;
+  const double mean_hr = 0.5 * (lte_eval<1, 0>(t, c, a.xi, eta) + lte_eval<1, 0>(t, c, b.xi, eta));
+  const double div_hr = lte_divided<0, 1, 0>(t, c, a.xi, eta, b.xi, eta);
+  if (P == 0) return 0.5 * (r1 * r1 + r2 * r2) * div_hr + (r1 + r2) * mean_hr;
+  const double div_h = lte_divided<0, 0, 0>(t, c, a.xi, eta, b.xi, eta);
+  return div_h + 0.5 * (r1 + r2) * div_hr + mean_hr;
+}
+
+template <int P>
+THX_HD double lte_beta_secant(const LteDev &t, const LteEval &a, const LteEval &b, double xi,
+                              double rho) {
+  const LteCell &c = a.cell;
+  const double mean_t = 0.5 * (a.T + b.T);
+  const double mean_hr = 0.5 * (lte_eval<1, 0>(t, c, xi, a.eta) + lte_eval<1, 0>(t, c, xi, b.eta));
+  const double div_hr = lte_divided<1, 1, 0>(t, c, xi, a.eta, xi, b.eta);
+  const double hr_beta = mean_hr - mean_t * div_hr;
+  if (P == 0) return rho * rho * hr_beta;
+  const double mean_h = 0.5 * (lte_eval<0, 0>(t, c, xi, a.eta) + lte_eval<0, 0>(t, c, xi, b.eta));
+  const double div_h = lte_divided<1, 0, 0>(t, c, xi, a.eta, xi, b.eta);
+  return mean_h - mean_t * div_h + rho * hr_beta;
+}
+
+template <int P>
+THX_HDC void lte_discrete_gradient(const LteDev &t, const LteEval &left, const LteEval &right,
+                                  double *grho, double *gbeta) {
+  const bool rev = left.rho > right.rho || (left.rho == right.rho && left.T > right.T);
+  const LteEval &A = rev ? right : left;
+  const LteEval &B = rev ? left : right;
+  const double b1 = 1 / A.T, b2 = 1 / B.T;
+  const double dr = B.rho - A.rho, db = b2 - b1;
+  const double rmx = A.rho > B.rho ? A.rho : B.rho;
+  const double bmx = b1 > b2 ? b1 : b2;
+  const bool ddiff = fabs(dr) >= 2.22e-15 + 1.49e-8 * rmx;
+  const bool bdiff = fabs(db) >= 2.22e-15 + 1.49e-8 * bmx;
+  const double f11 = lte_value<P>(t, A), f22 = lte_value<P>(t, B);
+  double gr = 0.0, gb = 0.0;
+  if (A.cell.off == B.cell.off) {
+    if (ddiff) gr = 0.5 * (lte_density_secant<P>(t, A, B, A.eta) * b1 + lte_density_secant<P>(t, A, B, B.eta) * b2);
+    if (bdiff) gb = 0.5 * (lte_beta_secant<P>(t, A, B, A.xi, A.rho) + lte_beta_secant<P>(t, A, B, B.xi, B.rho));
+  } else if (ddiff || bdiff) {
+    const double f12 = lte_value<P>(t, lte_at(t, A.rho, B.T));
+    const double f21 = lte_value<P>(t, lte_at(t, B.rho, A.T));
+    if (ddiff) gr = 0.5 * ((f21 * b1 - f11 * b1) + (f22 * b2 - f12 * b2)) / dr;
+    if (bdiff) gb = 0.5 * ((f12 * b2 - f11 * b1) + (f22 * b2 - f21 * b1)) / db;
+  }
+  if (!ddiff)
+    gr = P == 0 ? 0.5 * (lte_dp_drho(t, A) * b1 + lte_dp_drho(t, B) * b2)
+                : 0.5 * (lte_dg_drho(t, A) * b1 + lte_dg_drho(t, B) * b2);
+  if (!bdiff) {
+    const double d1 = P == 0 ? lte_dp_dT(t, A) : lte_dg_dT(t, A);
+    const double d2 = P == 0 ? lte_dp_dT(t, B) : lte_dg_dT(t, B);
+    gb = 0.5 * ((f11 - A.T * d1) + (f22 - B.T * d2));
+  }
+  *grho = gr;
+  *gbeta = gb;
+}
+
+// LTEEC flux from two evaluated endpoints with their pressures p1, p2: FACE
+// uses the normal d1 and the Lax dissipation; the volume form averages the
+// two metric rows.
+template <int DIM, bool FACE>
+THX_HD void lte_ec_flux(const LteDev &t, const double *q1, const double *q2, const LteEval &s1,
+                        const LteEval &s2, double p1, double p2, const double *d1, const double *d2,
+                        double *F) {
+  double pr, pb, gr, gb;
+  lte_discrete_gradient<0>(t, s1, s2, &pr, &pb);
+  lte_discrete_gradient<1>(t, s1, s2, &gr, &gb);
+  const double rho_mean = pr / gr;
+  const double e_mean = gb - pb / rho_mean;
+  double c1 = 0, c2 = 0;
+  if (FACE) { c1 = sqrt(lte_c2(t, s1)); c2 = sqrt(lte_c2(t, s2)); }
+  const double pm = 0.5 * (p1 + p2);
+  double vn = 0, ck = 0, pw = 0, v1n = 0, v2n = 0, nn = 0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double dir = FACE ? d1[d] : 0.5 * (d1[d] + d2[d]);
+    const double u1 = q1[1 + d] / q1[0], u2 = q2[1 + d] / q2[0];
+    vn += 0.5 * (u1 + u2) * dir;
+    ck += 0.5 * u1 * u2;
+    pw += 0.5 * (p1 * u2 + p2 * u1) * dir;
+    if (FACE) { v1n += u1 * dir; v2n += u2 * dir; nn += dir * dir; }
+  }
+  double dis = 0.0;
+  if (FACE) {
+    const double nm = sqrt(nn);
+    const double sp1 = fabs(v1n) + c1 * nm, sp2 = fabs(v2n) + c2 * nm;
+    dis = 0.5 * (sp1 > sp2 ? sp1 : sp2);
+  }
+  const double mf = rho_mean * vn;
+  F[0] = mf - dis * (q2[0] - q1[0]);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double dir = FACE ? d1[d] : 0.5 * (d1[d] + d2[d]);
+    const double v = 0.5 * (q1[1 + d] / q1[0] + q2[1 + d] / q2[0]);
+    F[1 + d] = mf * v + pm * dir - dis * (q2[1 + d] - q1[1 + d]);
+  }
+  F[DIM + 1] = mf * (e_mean + ck) + pw - dis * (q2[DIM + 1] - q1[DIM + 1]);
+}
+
+#undef THX_HD
+#undef THX_HDC
+
+}  // namespace thx
