@@ -228,6 +228,21 @@ int thx_destroy(thx_handle h);
  * (include/RHSOperator_impl.hpp:719-793). */
 int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream);
 
+/* Allocation-free Euler right-hand side (no counterpart in the reference).
+ * For hosts that cannot let a library call cudaMalloc -- a solver whose
+ * device memory belongs to its own pool or caching allocator, or a time loop
+ * that must not absorb cudaMalloc's device-wide synchronisation.  Needs no
+ * handle: geom holds DEVICE pointers in the thx_geometry layout (full per-node
+ * arrays), u and dudt are device FP64 L-vectors.  Euler flow, FP64, no
+ * blending (else THX_ERR_UNSUPPORTED).  Its scratch (face fluxes, element-to-face
+ * table, operators) is one static 8 MiB device array per GPU, kept until the
+ * process exits: meshes needing more return THX_ERR_INVALID_ARGUMENT.  The
+ * first call on a device looks the array up (make it before any stream
+ * capture); every call rewrites what it reads, and calls that overlap on the
+ * GPU race on the shared array. */
+int thx_rhs_euler_noalloc(const thx_geometry *geom_dev, const thx_config *cfg,
+                          const double *u, double *dudt, void *stream);
+
 /* nsteps SSP-RK3 steps (Shu-Osher form, as mfem::RK3SSPSolver::Step driven at
  * src/Simulation.cpp:1255) on a device FP64 state u, in place, with fixed dt.
  * In FP32-mixed mode the FP64 master state is accumulated in double and each
