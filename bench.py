@@ -364,6 +364,78 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """Batched serving of the mixed 2-D stream: N cases (Poisson arrivals at
+    2000/s) through the batch engine in FP32-mixed, against the same cases
+    run one at a time on the plain FP64 path (a seeded sample of them), whose
+    results also give each served case's final-solution error."""
+    import torch
+    import theseus_b200 as T
+    from theseus_b200.serving import BatchEngine, SyntheticStream, serve
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = SyntheticStream(args.cases, rate=2000.0, seed=0)
+    reqs = [stream.case(i, lazy=True) for i in range(args.cases)]
+    sample = set(range(0, args.cases, max(1, args.cases // args.sample)))
+    flux = dict(numerical_flux="chandrashekar", surface_flux="roe")
+
+    # one case at a time, plain FP64 (create, upload, steps, download, free)
+    def one(c):
+        op = (T.NSOperator if c.viscous else T.EulerOperator)(c.mesh, mu=c.mu, Pr=c.Pr, **flux)
+        u = torch.as_tensor(c.state(), device="cuda").contiguous()
+        op.rk3_steps(u, c.dt, c.nsteps)
+        out = u.cpu().numpy()
+        del op
+        return out
+    one(reqs[0])  # warm-up (library load, first kernels)
+    ref = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in sorted(sample):
+        ref[i] = one(reqs[i])
+    torch.cuda.synchronize()
+    base_s = time.perf_counter() - t0
+    base_rate = len(sample) / base_s
+    for i in sample:
+        reqs[i].u0 = None
+
+    errs = []
+
+    def keep(i, out):
+        if i in ref:
+            r = ref[i]
+            groups = [[0], [1, 2], [3]]
+            errs.append(max(float(np.sqrt(((out[g] - r[g]) ** 2).sum() / (r[g] ** 2).sum()))
+                            for g in groups))
+
+    eng = BatchEngine(precision="fp32", steps_per_launch=args.chunk, **flux)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        _, lat, makespan = serve(eng, reqs, on_result=keep)
+    st = eng.stats()
+    eng.close()
+    nodes = [r.mesh.num_nodes for r in reqs]
+    line = {"metric": "solves/s (batched serving, FP32-mixed, 200 SSP-RK3 steps per case)",
+            "value": args.cases / makespan, "unit": "solves/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32-mixed", "data": "synthetic",
+            "config": {"workload": "serving_2d_mixed_stream", "cases": args.cases,
+                       "arrival_rate_per_s": 2000.0, "sides": [8, 64], "orders": [2, 5],
+                       "mach": [0.1, 2.0], "reynolds": [100, 1e4], "inviscid_fraction": 0.5,
+                       "steps_per_case": 200, "steps_per_launch": args.chunk,
+                       "mean_nodes_per_case": float(np.mean(nodes)), "fluxes": flux},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "makespan_s": makespan,
+            "dof_rhs_per_s": 3 * 200 * float(np.sum(nodes)) / makespan,
+            "one_at_a_time_fp64": {"solves_per_s": base_rate, "sample_cases": len(sample),
+                                   "seconds": base_s},
+            "speedup_vs_one_at_a_time": (args.cases / makespan) / base_rate,
+            "final_solution_rel_l2_vs_fp64": {"max": max(errs) if errs else None,
+                                              "median": float(np.median(errs)) if errs else None,
+                                              "cases": len(errs),
+                                              "norm": "per conserved field (rho, momentum, E)"},
+            "engine": st, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,9 +447,16 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
+    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving"],
+                    help="rhs: the headline RHS throughput; serving: the batched case stream")
+    ap.add_argument("--cases", type=int, default=4096, help="serving: cases in the stream")
+    ap.add_argument("--sample", type=int, default=256, help="serving: cases also run one at a time")
+    ap.add_argument("--chunk", type=int, default=10, help="serving: SSP-RK3 steps per graph launch")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

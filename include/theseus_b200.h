@@ -42,7 +42,8 @@ typedef enum {
   THX_ERR_CUDA = 3,               /* a CUDA runtime call failed */
   THX_ERR_NO_DEVICE = 4,          /* no CUDA device visible: there is no CPU fallback */
   THX_ERR_OUT_OF_MEMORY = 5,
-  THX_ERR_NUMERICS = 6            /* device-side status flag set (non-positive state, Newton failure) */
+  THX_ERR_NUMERICS = 6,           /* device-side status flag set (non-positive state, Newton failure) */
+  THX_ERR_BUSY = 7                /* batch engine: the case does not fit the memory budget now */
 } thx_status;
 
 /* Two-point volume fluxes and surface (Riemann) fluxes.  The numbering is the
@@ -270,6 +271,61 @@ int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out,
 #define THX_STATUS_LAUNCH 4u       /* a kernel got too little shared memory and did nothing */
 #define THX_STATUS_EOS 8u          /* LTE temperature recovery failed or left the table */
 int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
+
+/* ---- batch engine (no counterpart in the reference) -----------------------
+ * Many independent cases -- each its own periodic mesh, polynomial order and
+ * flow model -- advanced together: cases with the same (dimension, order,
+ * flow model) form a group whose SSP-RK3 stages run as persistent kernels
+ * over one device work list, launched from a CUDA graph of `steps_per_launch`
+ * steps that stays valid while cases join and leave.  The reference's
+ * Simulation (src/Simulation.cpp:43-47) runs one case per process; the engine
+ * replaces a loop of RHSOperator::Mult-driven solves.
+ *
+ * cfg fixes the flux selection, precision and gas constants of every case;
+ * each case brings its geometry (host pointers), flow model, step count, dt,
+ * viscosity and FP32 working-copy offset.  States stay on the device from
+ * admission to fetch.  Results are bit-identical to the same case run alone
+ * through thx_rk3_steps with the same configuration. */
+typedef struct thx_engine_s *thx_engine;
+
+typedef struct {
+  int32_t flow_model;        /* THX_FLOW_EULER or THX_FLOW_NAVIER_STOKES */
+  int32_t nsteps;            /* SSP-RK3 steps */
+  double dt;                 /* fixed step */
+  double mu, Pr;             /* transport (Navier-Stokes) */
+  double state_offset[5];    /* FP32 working-copy offset (FP32-mixed engines) */
+} thx_case;
+
+typedef struct {
+  int32_t active_cases;      /* admitted and not yet fetched */
+  int32_t groups;            /* (dimension, order, flow) groups seen */
+  int64_t bytes_in_use;      /* footprint of the active cases */
+  int64_t launches;          /* graph launches so far */
+  int64_t cases_done;        /* cases fetched */
+} thx_engine_stats;
+
+/* Device bytes one case needs (state, stage copies, scratch, geometry). */
+int thx_case_footprint(const thx_geometry *geom, const thx_config *cfg, int flow_model,
+                       size_t *bytes);
+/* hbm_budget: bytes the engine may hold for cases; steps_per_launch: SSP-RK3
+ * steps per graph launch (cases whose step count is not a multiple finish
+ * their last steps one launch at a time). */
+int thx_engine_create(const thx_config *cfg, size_t hbm_budget, int steps_per_launch,
+                      thx_engine *out);
+int thx_engine_destroy(thx_engine e);
+/* Admit a case with initial state u0 (host FP64 L-vector); THX_ERR_BUSY if its
+ * footprint does not fit the budget now.  Set-up runs on the engine's own
+ * stream and overlaps with the running groups. */
+int thx_engine_admit(thx_engine e, const thx_geometry *geom, const thx_case *c,
+                     const double *u0, int64_t *id);
+/* Launch the next `steps_per_launch` steps of every group with active cases
+ * (asynchronous; returns immediately). */
+int thx_engine_advance(thx_engine e);
+/* Ids of cases whose steps are complete on the device (up to cap). */
+int thx_engine_poll(thx_engine e, int64_t *ids, int cap, int *count);
+/* Copy a finished case's state to the host and release it. */
+int thx_engine_fetch(thx_engine e, int64_t id, double *u_host);
+int thx_engine_get_stats(thx_engine e, thx_engine_stats *out);
 
 /* Diagnostics of the configured kernels (for roofline bookkeeping). */
 int thx_describe(thx_handle h, char *buf, size_t len);

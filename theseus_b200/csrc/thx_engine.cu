@@ -1,0 +1,722 @@
+// thx_engine.cu -- batch engine: many independent cases advanced together by
+// persistent kernels launched from CUDA graphs (C ABI in
+// include/theseus_b200.h, "batch engine").
+//
+// Cases with the same (dimension, order, flow model) form a group.  A group
+// owns, on the device, one argument record per case and SSP-RK3 stage (the
+// same VolArgs / FaceArgs / GradArgs a one-case right-hand side uses) and the
+// work lists of its persistent kernels (CTA-sized blocks of every case).  Its
+// CUDA graph holds `steps_per_launch` SSP-RK3 steps of [gradient] face volume
+// launches whose grids are fixed and whose work counts are read on the
+// device, so admitting or retiring a case rewrites the tables between graph
+// launches and never re-captures the graph.  Each case keeps its own buffers
+// (allocated stream-ordered from a memory pool on the engine's set-up stream,
+// so admission overlaps the running groups), which makes every result
+// bit-identical to the same case run alone.
+//
+// The volume kernel's grid (CTAs per SM) is tuned online per group: the first
+// launches try each candidate, cost = device time / work items, and the
+// cheapest is kept.
+#include "thx_operator.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <tuple>
+#include <vector>
+
+using namespace thx;
+
+namespace {
+
+constexpr int kFaceBlock = 128;  // face points per face work item
+
+size_t round_up(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Upper bound of the device bytes of one case (geometry counted uncompressed).
+size_t case_bytes(const thx_geometry *g, const thx_config *cfg, int flow) {
+  const int dim = g->dim, N = g->order + 1;
+  const size_t nd = dim == 2 ? N * N : N * N * N, nfp = dim == 2 ? N : N * N;
+  const size_t neq = dim + 2, ne = g->num_elements, nf = g->num_faces, L = ne * nd;
+  const bool mixed = cfg->precision == THX_PRECISION_FP32_MIXED;
+  const bool ns = flow == THX_FLOW_NAVIER_STOKES;
+  const size_t s = mixed ? 4 : 8, gs = mixed ? 12 : 8;  // working / geometry element bytes
+  size_t b = 0;
+  b += round_up(L * neq * 8) * 2;                             // master state, stage copy
+  if (mixed) b += round_up(L * neq * 4);                      // FP32 working copy
+  b += round_up(nf * nfp * neq * s);                          // face fluxes
+  if (ns) b += round_up((size_t)dim * (neq - 1) * L * s);     // viscous flux
+  b += round_up(L * gs) + round_up(L * dim * dim * gs);       // J, metric
+  b += round_up(nf * nfp * dim * gs) + 2 * round_up(nf * nfp * gs);  // normals, lift weights
+  b += round_up(nf * 2 * 4) * 2 + round_up(ne * 2 * dim * 4); // connectivity
+  b += round_up(ne * 8) * 2 + 4096;                           // alpha, eta, operators, status
+  return b;
+}
+
+struct EngineCase {
+  int64_t id = 0;
+  thx_operator_s *h = nullptr;
+  double *u = nullptr;     // FP64 master state
+  double dt = 0.0;
+  int steps_left = 0;
+  size_t bytes = 0;
+  cudaEvent_t done = nullptr;
+  bool finished = false;   // all steps enqueued; done recorded
+};
+
+struct EngineBase {
+  virtual ~EngineBase() {}
+  virtual int admit(const thx_geometry *g, const thx_case *c, const double *u0, int64_t *id) = 0;
+  virtual int advance() = 0;
+  virtual int poll(int64_t *ids, int cap, int *count) = 0;
+  virtual int fetch(int64_t id, double *u_host) = 0;
+  virtual void stats(thx_engine_stats *st) = 0;
+};
+
+template <typename R>
+struct Group {
+  int dim = 0, N = 0;
+  bool ns = false;
+  int epb = 1, nfp = 1;
+  std::vector<EngineCase *> cases;
+  bool dirty = true;
+  cudaStream_t stream = nullptr;
+  // device tables: [stage 1..3][cap] argument records, work lists, counts
+  VolArgs<R> *dvol = nullptr;
+  FaceArgs<R> *dface = nullptr;
+  GradArgs<R> *dgrad = nullptr;
+  BatchWork *dwv = nullptr, *dwf = nullptr;
+  int *dcount = nullptr;  // [0] volume/gradient work, [1] face work
+  int cap_cases = 0, cap_wv = 0, cap_wf = 0;
+  // pinned staging of the tables
+  unsigned char *staging = nullptr;
+  size_t staging_bytes = 0;
+  cudaEvent_t staged = nullptr;
+  int nwv = 0, nwf = 0;
+  // kernels and graph
+  VolBatchLaunch<R> volb = nullptr;
+  FaceBatchLaunch<R> faceb = nullptr;
+  GradBatchLaunch<R> gradb = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int exec_grid = -1;
+  // launches in flight: at most two per group, so that newly admitted cases
+  // join after a short queue
+  cudaEvent_t ring[2] = {nullptr, nullptr};
+  int ring_pos = 0;
+  // online tuning of the volume grid
+  std::vector<int> candidates;
+  std::vector<double> cost;
+  int next_candidate = 0, chosen = -1;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int timing_candidate = -1;
+  long long timing_work = 0;
+};
+
+template <typename R>
+class Engine final : public EngineBase {
+ public:
+  Engine(const thx_config &cfg, size_t budget, int k) : cfg_(cfg), budget_(budget), k_(k) {}
+
+  int init() {
+    if (cudaGetDevice(&device_) != cudaSuccess) return THX_ERR_NO_DEVICE;
+    if (cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_) != cudaSuccess)
+      return THX_ERR_CUDA;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_;
+    if (cudaMemPoolCreate(&pool_, &props) != cudaSuccess) return THX_ERR_CUDA;
+    uint64_t keep = ~uint64_t(0);  // keep freed memory in the pool
+    cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (cudaStreamCreateWithFlags(&setup_, cudaStreamNonBlocking) != cudaSuccess) return THX_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&setup_done_, cudaEventDisableTiming) != cudaSuccess) return THX_ERR_CUDA;
+    return THX_OK;
+  }
+
+  ~Engine() override {
+    for (auto &kv : groups_) {
+      Group<R> &G = *kv.second;
+      if (G.stream) cudaStreamSynchronize(G.stream);
+    }
+    if (setup_) cudaStreamSynchronize(setup_);
+    for (auto &kv : cases_) release(kv.second.get(), false);
+    cases_.clear();
+    for (auto &kv : groups_) destroy_group(*kv.second);
+    if (setup_) {
+      cudaStreamSynchronize(setup_);
+      cudaStreamDestroy(setup_);
+    }
+    if (setup_done_) cudaEventDestroy(setup_done_);
+    if (pool_) cudaMemPoolDestroy(pool_);
+  }
+
+  int admit(const thx_geometry *g, const thx_case *c, const double *u0, int64_t *id) override {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!g || !c || !u0 || !id) return THX_ERR_INVALID_ARGUMENT;
+    if (c->nsteps < 0 || !(c->dt > 0.0) || !(c->mu >= 0.0) ||
+        (c->flow_model != THX_FLOW_EULER && c->flow_model != THX_FLOW_NAVIER_STOKES) ||
+        (c->flow_model == THX_FLOW_NAVIER_STOKES && !(c->Pr > 0.0)))
+      return THX_ERR_INVALID_ARGUMENT;
+    if (g->dim < 2 || g->dim > 3 || g->num_elements <= 0 || g->num_faces < 0 || !g->jac ||
+        !g->metric || (g->num_faces > 0 && (!g->face_elem || !g->face_lface || !g->face_normal ||
+                                            !g->face_wminus || !g->face_wplus)))
+      return THX_ERR_INVALID_ARGUMENT;
+    if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
+    const size_t bytes = case_bytes(g, &cfg_, c->flow_model);
+    if (bytes_ + bytes > budget_) return THX_ERR_BUSY;
+    thx_config cc = cfg_;
+    cc.flow_model = c->flow_model;
+    cc.mu = c->mu;
+    cc.Pr = c->Pr;
+    for (int k = 0; k < 5; ++k) cc.state_offset[k] = c->state_offset[k];
+    auto ec = std::make_unique<EngineCase>();
+    thx_operator_s *h = new (std::nothrow) thx_operator_s();
+    if (!h) return THX_ERR_OUT_OF_MEMORY;
+    h->device = device_;
+    h->pool = pool_;
+    h->setup_stream = setup_;
+    ec->h = h;
+    int st = op_create(g, &cc, h, nullptr);
+    if (st) {
+      op_free(h);
+      delete h;
+      return st;
+    }
+    const size_t n = (size_t)h->L * h->neq;
+    if ((st = alloc(h, &ec->u, n)) || (st = alloc(h, &h->y, n)) ||
+        (h->mixed && (st = alloc(h, &h->yf, n)))) {
+      op_free(h);
+      delete h;
+      return st;
+    }
+    if (cudaMemcpyAsync(ec->u, u0, n * sizeof(double), cudaMemcpyHostToDevice, setup_) != cudaSuccess ||
+        (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
+        cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(setup_done_, setup_) != cudaSuccess) {
+      cudaGetLastError();
+      op_free(h);
+      delete h;
+      return THX_ERR_CUDA;
+    }
+    Group<R> *G = nullptr;
+    if ((st = group_for(h, &G))) {
+      op_free(h);
+      delete h;
+      return st;
+    }
+    ec->id = next_id_++;
+    ec->dt = c->dt;
+    ec->steps_left = c->nsteps;
+    ec->bytes = bytes;
+    bytes_ += bytes;
+    G->cases.push_back(ec.get());
+    G->dirty = true;
+    *id = ec->id;
+    cases_[ec->id] = std::move(ec);
+    return THX_OK;
+  }
+
+  int advance() override {
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto &kv : groups_) {
+      int st = advance_group(*kv.second);
+      if (st) return st;
+    }
+    return THX_OK;
+  }
+
+  int poll(int64_t *ids, int cap, int *count) override {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!count || (cap > 0 && !ids)) return THX_ERR_INVALID_ARGUMENT;
+    int n = 0;
+    for (auto &kv : cases_) {
+      EngineCase *c = kv.second.get();
+      if (!c->finished || n >= cap) continue;
+      const cudaError_t q = cudaEventQuery(c->done);
+      if (q == cudaSuccess) ids[n++] = c->id;
+      else if (q != cudaErrorNotReady) { cudaGetLastError(); return THX_ERR_CUDA; }
+    }
+    *count = n;
+    return THX_OK;
+  }
+
+  int fetch(int64_t id, double *u_host) override {
+    std::lock_guard<std::mutex> lock(mu_);
+    auto it = cases_.find(id);
+    if (it == cases_.end() || !u_host) return THX_ERR_INVALID_ARGUMENT;
+    EngineCase *c = it->second.get();
+    if (!c->finished) return THX_ERR_BUSY;
+    const size_t n = (size_t)c->h->L * c->h->neq;
+    if (cudaStreamWaitEvent(setup_, c->done, 0) != cudaSuccess ||
+        cudaMemcpyAsync(u_host, c->u, n * sizeof(double), cudaMemcpyDeviceToHost, setup_) != cudaSuccess ||
+        cudaStreamSynchronize(setup_) != cudaSuccess) {
+      cudaGetLastError();
+      return THX_ERR_CUDA;
+    }
+    release(c, true);
+    cases_.erase(it);
+    ++done_;
+    return THX_OK;
+  }
+
+  void stats(thx_engine_stats *st) override {
+    std::lock_guard<std::mutex> lock(mu_);
+    st->active_cases = (int32_t)cases_.size();
+    st->groups = (int32_t)groups_.size();
+    st->bytes_in_use = (int64_t)bytes_;
+    st->launches = launches_;
+    st->cases_done = done_;
+  }
+
+ private:
+  using Key = std::tuple<int, int, bool>;
+
+  template <typename T>
+  int alloc(thx_operator_s *h, T **p, size_t n) {
+    if (cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool_, setup_) != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      return THX_ERR_OUT_OF_MEMORY;
+    }
+    h->allocs.push_back(*p);
+    return THX_OK;
+  }
+
+  // free a case's buffers after its last work (stream-ordered on set-up)
+  void release(EngineCase *c, bool account) {
+    if (c->done) cudaStreamWaitEvent(setup_, c->done, 0);
+    if (c->h) {
+      op_free(c->h);
+      delete c->h;
+      c->h = nullptr;
+    }
+    if (c->done) cudaEventDestroy(c->done);
+    c->done = nullptr;
+    if (account) bytes_ -= c->bytes;
+  }
+
+  int group_for(thx_operator_s *h, Group<R> **out) {
+    const Key key(h->dim, h->N, h->ns);
+    auto it = groups_.find(key);
+    if (it != groups_.end()) {
+      *out = it->second.get();
+      return THX_OK;
+    }
+    auto G = std::make_unique<Group<R>>();
+    G->dim = h->dim;
+    G->N = h->N;
+    G->ns = h->ns;
+    G->epb = std::max(1, 256 / h->nd);
+    G->nfp = h->nfp;
+    const int vk = (cfg_.volume_flux == THX_FLUX_CHANDRASHEKAR) ? VOL_CHANDRASHEKAR
+                 : (cfg_.volume_flux == THX_FLUX_RANOCHA)     ? VOL_RANOCHA
+                 : (cfg_.volume_flux == THX_FLUX_PIROZZOLI)   ? VOL_PIROZZOLI
+                                                              : VOL_CENTRAL;
+    const int ns = h->ns ? 1 : 0;
+    pick_kernels(*G, vk, ns);
+    if (!G->volb || !G->faceb || !G->gradb) return THX_ERR_UNSUPPORTED;
+    if (G->volb(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess ||
+        G->gradb(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return THX_ERR_CUDA;
+    }
+    if (cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->staged, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&G->t0) != cudaSuccess || cudaEventCreate(&G->t1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->ring[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->ring[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return THX_ERR_CUDA;
+    }
+    for (int m : {1, 2, 4}) G->candidates.push_back(m * sms_);
+    G->cost.assign(G->candidates.size(), -1.0);
+    *out = G.get();
+    groups_[key] = std::move(G);
+    return THX_OK;
+  }
+
+  void pick_kernels(Group<R> &G, int vk, int ns);
+
+  void destroy_group(Group<R> &G) {
+    if (G.stream) cudaStreamSynchronize(G.stream);
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    cudaFree(G.dvol);
+    cudaFree(G.dface);
+    cudaFree(G.dgrad);
+    cudaFree(G.dwv);
+    cudaFree(G.dwf);
+    cudaFree(G.dcount);
+    if (G.staging) cudaFreeHost(G.staging);
+    if (G.staged) cudaEventDestroy(G.staged);
+    if (G.t0) cudaEventDestroy(G.t0);
+    if (G.t1) cudaEventDestroy(G.t1);
+    for (cudaEvent_t ev : G.ring)
+      if (ev) cudaEventDestroy(ev);
+    if (G.stream) cudaStreamDestroy(G.stream);
+  }
+
+  // Rewrite the group's argument tables and work lists (between launches).
+  int upload_tables(Group<R> &G) {
+    const int nc = (int)G.cases.size();
+    int nwv = 0, nwf = 0;
+    for (EngineCase *c : G.cases) {
+      nwv += (c->h->ne + G.epb - 1) / G.epb;
+      nwf += (int)(((long long)c->h->nf * G.nfp + kFaceBlock - 1) / kFaceBlock);
+    }
+    bool grow = nc > G.cap_cases || nwv > G.cap_wv || nwf > G.cap_wf;
+    if (grow) {
+      // buffers may be read by a launch in flight: wait, then reallocate
+      if (cudaStreamSynchronize(G.stream) != cudaSuccess) return THX_ERR_CUDA;
+      auto grow_to = [](int need, int have) { return std::max(need, std::max(16, 2 * have)); };
+      const int cc = nc > G.cap_cases ? grow_to(nc, G.cap_cases) : G.cap_cases;
+      const int cv = nwv > G.cap_wv ? grow_to(nwv, G.cap_wv) : G.cap_wv;
+      const int cf = nwf > G.cap_wf ? grow_to(nwf, G.cap_wf) : G.cap_wf;
+      cudaFree(G.dvol); cudaFree(G.dface); cudaFree(G.dgrad); cudaFree(G.dwv); cudaFree(G.dwf);
+      G.dvol = nullptr; G.dface = nullptr; G.dgrad = nullptr; G.dwv = nullptr; G.dwf = nullptr;
+      if (cudaMalloc(&G.dvol, sizeof(VolArgs<R>) * 3 * cc) != cudaSuccess ||
+          cudaMalloc(&G.dface, sizeof(FaceArgs<R>) * 3 * cc) != cudaSuccess ||
+          cudaMalloc(&G.dgrad, sizeof(GradArgs<R>) * 3 * cc) != cudaSuccess ||
+          cudaMalloc(&G.dwv, sizeof(BatchWork) * cv) != cudaSuccess ||
+          cudaMalloc(&G.dwf, sizeof(BatchWork) * cf) != cudaSuccess ||
+          (!G.dcount && cudaMalloc(&G.dcount, sizeof(int) * 2) != cudaSuccess)) {
+        cudaGetLastError();
+        return THX_ERR_OUT_OF_MEMORY;
+      }
+      G.cap_cases = cc;
+      G.cap_wv = cv;
+      G.cap_wf = cf;
+      if (G.exec) {
+        cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+      }
+    }
+    const size_t bv = sizeof(VolArgs<R>) * 3 * nc, bf = sizeof(FaceArgs<R>) * 3 * nc;
+    const size_t bg = sizeof(GradArgs<R>) * 3 * nc;
+    const size_t bw = sizeof(BatchWork) * (size_t)(nwv + nwf);
+    const size_t need = bv + bf + bg + bw + 2 * sizeof(int) + 64;
+    if (cudaEventSynchronize(G.staged) != cudaSuccess) return THX_ERR_CUDA;  // staging free again
+    if (need > G.staging_bytes) {
+      if (G.staging) cudaFreeHost(G.staging);
+      G.staging = nullptr;
+      G.staging_bytes = std::max(need, 2 * G.staging_bytes);
+      if (cudaHostAlloc((void **)&G.staging, G.staging_bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        G.staging_bytes = 0;
+        return THX_ERR_OUT_OF_MEMORY;
+      }
+    }
+    VolArgs<R> *hv = reinterpret_cast<VolArgs<R> *>(G.staging);
+    FaceArgs<R> *hf = reinterpret_cast<FaceArgs<R> *>(G.staging + bv);
+    GradArgs<R> *hg = reinterpret_cast<GradArgs<R> *>(G.staging + bv + bf);
+    BatchWork *hw = reinterpret_cast<BatchWork *>(G.staging + bv + bf + bg);
+    int *hc = reinterpret_cast<int *>(G.staging + bv + bf + bg + bw);
+    int wv = 0, wf = 0;
+    for (int i = 0; i < nc; ++i) {
+      EngineCase *c = G.cases[i];
+      thx_operator_s *h = c->h;
+      for (int stage = 1; stage <= 3; ++stage) {
+        const int j = (stage - 1) * nc + i;
+        const R *in;
+        if constexpr (IsF32<R>::value) in = h->yf;
+        else in = stage == 1 ? c->u : h->y;
+        op_args<R>(h, in, nullptr, stage, c->dt, c->u, h->y, h->yf, hg[j], hf[j], hv[j]);
+      }
+      const int nb = (h->ne + G.epb - 1) / G.epb;
+      for (int b = 0; b < nb; ++b) hw[wv++] = BatchWork{i, b};
+    }
+    for (int i = 0; i < nc; ++i) {
+      thx_operator_s *h = G.cases[i]->h;
+      const int nb = (int)(((long long)h->nf * G.nfp + kFaceBlock - 1) / kFaceBlock);
+      for (int b = 0; b < nb; ++b) hw[nwv + wf++] = BatchWork{i, b};
+    }
+    hc[0] = nwv;
+    hc[1] = nwf;
+    // the argument records of stage s start at s*nc; the graph indexes
+    // tables by capacity, so place each stage block at s*cap
+    for (int stage = 0; stage < 3; ++stage) {
+      if (cudaMemcpyAsync(G.dvol + (size_t)stage * G.cap_cases, hv + (size_t)stage * nc,
+                          sizeof(VolArgs<R>) * nc, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
+          cudaMemcpyAsync(G.dface + (size_t)stage * G.cap_cases, hf + (size_t)stage * nc,
+                          sizeof(FaceArgs<R>) * nc, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
+          cudaMemcpyAsync(G.dgrad + (size_t)stage * G.cap_cases, hg + (size_t)stage * nc,
+                          sizeof(GradArgs<R>) * nc, cudaMemcpyHostToDevice, G.stream) != cudaSuccess)
+        return THX_ERR_CUDA;
+    }
+    if ((nwv && cudaMemcpyAsync(G.dwv, hw, sizeof(BatchWork) * nwv, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
+        (nwf && cudaMemcpyAsync(G.dwf, hw + nwv, sizeof(BatchWork) * nwf, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
+        cudaMemcpyAsync(G.dcount, hc, sizeof(int) * 2, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
+        cudaEventRecord(G.staged, G.stream) != cudaSuccess)
+      return THX_ERR_CUDA;
+    G.nwv = nwv;
+    G.nwf = nwf;
+    G.dirty = false;
+    return THX_OK;
+  }
+
+  int capture(Group<R> &G, int grid) {
+    if (G.exec) {
+      cudaGraphExecDestroy(G.exec);
+      G.exec = nullptr;
+    }
+    const int gf = 8 * sms_, gg = 2 * sms_;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return THX_ERR_CUDA;
+    cudaError_t e = cudaSuccess;
+    for (int step = 0; step < k_ && e == cudaSuccess; ++step)
+      for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
+        const size_t o = (size_t)stage * G.cap_cases;
+        if (G.ns) e = G.gradb(G.dgrad + o, G.dwv, G.dcount, gg, G.stream, 0);
+        if (e == cudaSuccess) e = G.faceb(G.dface + o, G.dwf, G.dcount + 1, gf, G.stream, 0);
+        if (e == cudaSuccess) e = G.volb(G.dvol + o, G.dwv, G.dcount, grid, G.stream, 0);
+      }
+    const cudaError_t ee = cudaStreamEndCapture(G.stream, &graph);
+    if (e != cudaSuccess || ee != cudaSuccess || !graph) {
+      cudaGetLastError();
+      if (graph) cudaGraphDestroy(graph);
+      return THX_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      G.exec = nullptr;
+      return THX_ERR_CUDA;
+    }
+    G.exec_grid = grid;
+    return THX_OK;
+  }
+
+  // collect the timing of the previous tuning launch, if it has finished
+  void collect_timing(Group<R> &G) {
+    if (G.timing_candidate < 0) return;
+    if (cudaEventQuery(G.t1) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, G.t0, G.t1) == cudaSuccess && G.timing_work > 0)
+      G.cost[G.timing_candidate] = ms / (double)G.timing_work;
+    G.timing_candidate = -1;
+    bool all = true;
+    for (double c : G.cost) all = all && c >= 0.0;
+    if (all && G.chosen < 0)
+      G.chosen = (int)(std::min_element(G.cost.begin(), G.cost.end()) - G.cost.begin());
+  }
+
+  int advance_group(Group<R> &G) {
+    collect_timing(G);
+    // cases with fewer steps left than a launch holds finish one at a time
+    for (size_t i = 0; i < G.cases.size();) {
+      EngineCase *c = G.cases[i];
+      if (c->steps_left < k_) {
+        if (cudaStreamWaitEvent(G.stream, setup_done_, 0) != cudaSuccess) return THX_ERR_CUDA;
+        if (c->steps_left > 0) {
+          int st = thx_rk3_steps(c->h, c->u, c->dt, c->steps_left, G.stream);
+          if (st) return st;
+        }
+        c->steps_left = 0;
+        c->finished = true;
+        if (cudaEventRecord(c->done, G.stream) != cudaSuccess) return THX_ERR_CUDA;
+        G.cases.erase(G.cases.begin() + i);
+        G.dirty = true;
+      } else {
+        ++i;
+      }
+    }
+    if (G.cases.empty()) return THX_OK;
+    {
+      const cudaError_t q = cudaEventQuery(G.ring[G.ring_pos]);
+      if (q == cudaErrorNotReady) return THX_OK;  // two launches still queued
+      if (q != cudaSuccess) { cudaGetLastError(); return THX_ERR_CUDA; }
+    }
+    if (cudaStreamWaitEvent(G.stream, setup_done_, 0) != cudaSuccess) return THX_ERR_CUDA;
+    int st;
+    if (G.dirty && (st = upload_tables(G))) return st;
+    int cand = -1, grid;
+    if (G.chosen >= 0) {
+      grid = G.candidates[G.chosen];
+    } else if (G.timing_candidate < 0 && G.next_candidate < (int)G.candidates.size()) {
+      cand = G.next_candidate++;
+      grid = G.candidates[cand];
+    } else {
+      grid = G.exec_grid > 0 ? G.exec_grid : G.candidates[0];
+    }
+    if (!G.exec || G.exec_grid != grid) {
+      if ((st = capture(G, grid))) return st;
+    }
+    if (cand >= 0) cudaEventRecord(G.t0, G.stream);
+    if (cudaGraphLaunch(G.exec, G.stream) != cudaSuccess) {
+      cudaGetLastError();
+      return THX_ERR_CUDA;
+    }
+    if (cand >= 0) {
+      cudaEventRecord(G.t1, G.stream);
+      G.timing_candidate = cand;
+      G.timing_work = (long long)G.nwv * k_;
+    }
+    ++launches_;
+    if (cudaEventRecord(G.ring[G.ring_pos], G.stream) != cudaSuccess) return THX_ERR_CUDA;
+    G.ring_pos ^= 1;
+    for (size_t i = 0; i < G.cases.size();) {
+      EngineCase *c = G.cases[i];
+      c->steps_left -= k_;
+      if (c->steps_left == 0) {
+        c->finished = true;
+        if (cudaEventRecord(c->done, G.stream) != cudaSuccess) return THX_ERR_CUDA;
+        G.cases.erase(G.cases.begin() + i);
+        G.dirty = true;
+      } else {
+        ++i;
+      }
+    }
+    return THX_OK;
+  }
+
+  thx_config cfg_;
+  size_t budget_;
+  int k_;
+  int device_ = 0, sms_ = 148;
+  cudaMemPool_t pool_ = nullptr;
+  cudaStream_t setup_ = nullptr;
+  cudaEvent_t setup_done_ = nullptr;
+  std::map<Key, std::unique_ptr<Group<R>>> groups_;
+  std::map<int64_t, std::unique_ptr<EngineCase>> cases_;
+  size_t bytes_ = 0;
+  int64_t next_id_ = 1, launches_ = 0, done_ = 0;
+  std::mutex mu_;
+};
+
+template <>
+void Engine<double>::pick_kernels(Group<double> &G, int vk, int ns) {
+#define THX_PICKB(P, D, NN)                                 \
+  if (G.dim == D && G.N == NN) {                            \
+    const OrderKernels0 k = order_kernels_##P##_##D##_##NN(); \
+    G.volb = k.volb[vk][ns];                                \
+    G.gradb = k.gradb;                                      \
+  }
+  THX_FOR_ORDERS(THX_PICKB, 0, 2)
+  THX_FOR_ORDERS(THX_PICKB, 0, 3)
+#undef THX_PICKB
+  const FaceKernels0 f = G.dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
+  G.faceb = f.faceb[cfg_.surface_flux][ns];
+}
+
+template <>
+void Engine<float>::pick_kernels(Group<float> &G, int vk, int ns) {
+#define THX_PICKB(P, D, NN)                                 \
+  if (G.dim == D && G.N == NN) {                            \
+    const OrderKernels1 k = order_kernels_##P##_##D##_##NN(); \
+    G.volb = k.volb[vk][ns];                                \
+    G.gradb = k.gradb;                                      \
+  }
+  THX_FOR_ORDERS(THX_PICKB, 1, 2)
+  THX_FOR_ORDERS(THX_PICKB, 1, 3)
+#undef THX_PICKB
+  const FaceKernels1 f = G.dim == 2 ? face_kernels_1_2() : face_kernels_1_3();
+  G.faceb = f.faceb[cfg_.surface_flux][ns];
+}
+
+}  // namespace
+
+struct thx_engine_s {
+  EngineBase *impl = nullptr;
+  int device = 0;
+};
+
+extern "C" {
+
+int thx_case_footprint(const thx_geometry *g, const thx_config *cfg, int flow_model, size_t *bytes) {
+  if (!g || !cfg || !bytes || g->dim < 2 || g->dim > 3 || g->order < 1 || g->num_elements <= 0 ||
+      g->num_faces < 0)
+    return THX_ERR_INVALID_ARGUMENT;
+  *bytes = case_bytes(g, cfg, flow_model);
+  return THX_OK;
+}
+
+int thx_engine_create(const thx_config *cfg, size_t hbm_budget, int steps_per_launch, thx_engine *out) {
+  if (!cfg || !out || steps_per_launch < 1 || steps_per_launch > 1000) return THX_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (cfg->blending || cfg->volume_flux < 0 || cfg->volume_flux >= THX_FLUX_LTEEC ||
+      cfg->surface_flux < 0 || cfg->surface_flux >= THX_FLUX_LTEEC)
+    return THX_ERR_UNSUPPORTED;  // ideal gas, no subcell blending
+  if (cfg->precision != THX_PRECISION_FP64 && cfg->precision != THX_PRECISION_FP32_MIXED)
+    return THX_ERR_INVALID_ARGUMENT;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return THX_ERR_NO_DEVICE;
+  }
+  thx_engine_s *e = new (std::nothrow) thx_engine_s();
+  if (!e) return THX_ERR_OUT_OF_MEMORY;
+  cudaGetDevice(&e->device);
+  int st;
+  if (cfg->precision == THX_PRECISION_FP32_MIXED) {
+    auto *impl = new (std::nothrow) Engine<float>(*cfg, hbm_budget, steps_per_launch);
+    st = impl ? impl->init() : THX_ERR_OUT_OF_MEMORY;
+    e->impl = impl;
+  } else {
+    auto *impl = new (std::nothrow) Engine<double>(*cfg, hbm_budget, steps_per_launch);
+    st = impl ? impl->init() : THX_ERR_OUT_OF_MEMORY;
+    e->impl = impl;
+  }
+  if (st) {
+    delete e->impl;
+    delete e;
+    return st;
+  }
+  *out = e;
+  return THX_OK;
+}
+
+int thx_engine_destroy(thx_engine e) {
+  if (!e) return THX_ERR_INVALID_ARGUMENT;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(e->device);
+  delete e->impl;
+  cudaSetDevice(prev);
+  delete e;
+  return THX_OK;
+}
+
+#define THX_ENGINE_CALL(expr)          \
+  int prev = 0;                        \
+  cudaGetDevice(&prev);                \
+  if (prev != e->device) cudaSetDevice(e->device); \
+  const int st = (expr);               \
+  if (prev != e->device) cudaSetDevice(prev);      \
+  return st;
+
+int thx_engine_admit(thx_engine e, const thx_geometry *g, const thx_case *c, const double *u0,
+                     int64_t *id) {
+  if (!e) return THX_ERR_INVALID_ARGUMENT;
+  THX_ENGINE_CALL(e->impl->admit(g, c, u0, id))
+}
+
+int thx_engine_advance(thx_engine e) {
+  if (!e) return THX_ERR_INVALID_ARGUMENT;
+  THX_ENGINE_CALL(e->impl->advance())
+}
+
+int thx_engine_poll(thx_engine e, int64_t *ids, int cap, int *count) {
+  if (!e) return THX_ERR_INVALID_ARGUMENT;
+  THX_ENGINE_CALL(e->impl->poll(ids, cap, count))
+}
+
+int thx_engine_fetch(thx_engine e, int64_t id, double *u_host) {
+  if (!e) return THX_ERR_INVALID_ARGUMENT;
+  THX_ENGINE_CALL(e->impl->fetch(id, u_host))
+}
+
+int thx_engine_get_stats(thx_engine e, thx_engine_stats *out) {
+  if (!e || !out) return THX_ERR_INVALID_ARGUMENT;
+  e->impl->stats(out);
+  return THX_OK;
+}
+
+#undef THX_ENGINE_CALL
+
+}  // extern "C"

@@ -1,0 +1,256 @@
+"""Batched serving of many independent DGSEM cases on one GPU.
+
+`BatchEngine` wraps the library's batch engine (C ABI `thx_engine_*`): cases of
+any periodic mesh size, polynomial order and flow model are admitted while
+others run, their states stay on the device, and every (dimension, order,
+flow) group advances by persistent kernels launched from one CUDA graph of
+`steps_per_launch` SSP-RK3 steps.
+
+`serve()` is the continuous-batching loop: requests arrive on a schedule
+(seconds from the start), are admitted as soon as the engine's memory budget
+has room (first come, first served), advance together, and are fetched when
+their steps are done.  It returns each case's final state and its
+time-to-solution (arrival -> result on the host).
+
+`SyntheticStream` draws the mixed 2-D workload used by the serving benchmark:
+periodic square meshes of 8..64 elements per side, p = 2..5, freestream Mach
+0.1..2, Reynolds 100..10^4 or inviscid with probability 0.5, an isentropic
+vortex of strength 1..5, Poisson arrivals.
+"""
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (library, _check, make_config, Geometry, periodic_box, THXError, FLOW_EULER,
+               FLOW_NAVIER_STOKES, PRECISION_FP32_MIXED)
+from . import cases as _cases
+
+THX_ERR_BUSY = 7
+
+
+class CaseDesc(C.Structure):
+    _fields_ = [("flow_model", C.c_int32), ("nsteps", C.c_int32), ("dt", C.c_double),
+                ("mu", C.c_double), ("Pr", C.c_double), ("state_offset", C.c_double * 5)]
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("active_cases", C.c_int32), ("groups", C.c_int32), ("bytes_in_use", C.c_int64),
+                ("launches", C.c_int64), ("cases_done", C.c_int64)]
+
+
+def _bind(lib):
+    if getattr(lib, "_engine_bound", False):
+        return lib
+    P = C.c_void_p
+    lib.thx_engine_create.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(P)]
+    lib.thx_engine_destroy.argtypes = [P]
+    lib.thx_engine_admit.argtypes = [P, C.POINTER(Geometry), C.POINTER(CaseDesc), C.c_void_p,
+                                     C.POINTER(C.c_int64)]
+    lib.thx_engine_advance.argtypes = [P]
+    lib.thx_engine_poll.argtypes = [P, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]
+    lib.thx_engine_fetch.argtypes = [P, C.c_int64, C.c_void_p]
+    lib.thx_engine_get_stats.argtypes = [P, C.POINTER(EngineStats)]
+    lib.thx_case_footprint.argtypes = [C.POINTER(Geometry), C.c_void_p, C.c_int,
+                                       C.POINTER(C.c_size_t)]
+    lib._engine_bound = True
+    return lib
+
+
+@dataclass
+class Case:
+    """One request: mesh, initial state (host FP64 L-vector), physics, steps."""
+    mesh: object
+    u0: np.ndarray
+    nsteps: int
+    dt: float
+    viscous: bool = False
+    mu: float = 0.0
+    Pr: float = 0.72
+    state_offset: tuple = (0.0, 0.0, 0.0, 0.0, 0.0)
+    arrival: float = 0.0
+    tag: dict = field(default_factory=dict)
+    factory: object = None   # builds u0 on first use when u0 is None
+
+    def state(self):
+        if self.u0 is None:
+            self.u0 = self.factory()
+        return self.u0
+
+    def desc(self):
+        off = (C.c_double * 5)(*[float(x) for x in self.state_offset])
+        return CaseDesc(FLOW_NAVIER_STOKES if self.viscous else FLOW_EULER, int(self.nsteps),
+                        float(self.dt), float(self.mu), float(self.Pr), off)
+
+
+class BatchEngine:
+    """Mirror of the C ABI batch engine.  `numerical_flux`, `surface_flux`,
+    `precision` and the gas constants are shared by all cases."""
+
+    def __init__(self, numerical_flux="chandrashekar", surface_flux="roe", precision="fp32",
+                 hbm_budget=None, steps_per_launch=10, device=None, **physics):
+        import torch
+        if not torch.cuda.is_available():
+            raise THXError("no CUDA device: the batch engine has no CPU fallback")
+        self.lib = _bind(library())
+        self.cfg = make_config(flow="euler", volume_flux=numerical_flux, surface_flux=surface_flux,
+                               precision=precision, **physics)
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = int(0.8 * free)
+        self.steps_per_launch = int(steps_per_launch)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            _check(self.lib.thx_engine_create(C.byref(self.cfg), C.c_size_t(int(hbm_budget)),
+                                              self.steps_per_launch, C.byref(h)), "thx_engine_create")
+        self._h = h
+        self.hbm_budget = int(hbm_budget)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.thx_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def footprint(self, case):
+        b = C.c_size_t()
+        _check(self.lib.thx_case_footprint(C.byref(case.mesh.struct()), C.byref(self.cfg),
+                                           FLOW_NAVIER_STOKES if case.viscous else FLOW_EULER,
+                                           C.byref(b)), "thx_case_footprint")
+        return b.value
+
+    def admit(self, case):
+        """Case id, or None when the memory budget has no room now."""
+        u0 = np.ascontiguousarray(case.state(), np.float64)
+        cid = C.c_int64()
+        st = self.lib.thx_engine_admit(self._h, C.byref(case.mesh.struct()), C.byref(case.desc()),
+                                       u0.ctypes.data, C.byref(cid))
+        if st == THX_ERR_BUSY:
+            return None
+        _check(st, "thx_engine_admit")
+        return cid.value
+
+    def advance(self):
+        _check(self.lib.thx_engine_advance(self._h), "thx_engine_advance")
+
+    def poll(self, cap=4096):
+        ids = (C.c_int64 * cap)()
+        n = C.c_int()
+        _check(self.lib.thx_engine_poll(self._h, ids, cap, C.byref(n)), "thx_engine_poll")
+        return [ids[i] for i in range(n.value)]
+
+    def fetch(self, cid, shape):
+        out = np.empty(shape, np.float64)
+        _check(self.lib.thx_engine_fetch(self._h, int(cid), out.ctypes.data), "thx_engine_fetch")
+        return out
+
+    def stats(self):
+        s = EngineStats()
+        _check(self.lib.thx_engine_get_stats(self._h, C.byref(s)), "thx_engine_get_stats")
+        return {k: getattr(s, k) for k, _ in EngineStats._fields_}
+
+
+def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None):
+    """Continuous batching: requests (sorted by .arrival, seconds from start)
+    are admitted as they arrive and the budget allows, advanced together, and
+    fetched when done.  Returns (results, latencies, makespan): results[i] is
+    the final state of requests[i] (None when on_result(i, state) consumed it),
+    latencies[i] its arrival-to-result time."""
+    n = len(requests)
+    results = [None] * n
+    latency = np.zeros(n)
+    pending = 0                # next request not yet admitted
+    running = {}               # engine id -> request index
+    t0 = clock()
+    while pending < n or running:
+        now = clock() - t0
+        # admit everything that has arrived, in order, while it fits
+        while pending < n and requests[pending].arrival <= now:
+            cid = engine.admit(requests[pending])
+            if cid is None:
+                break
+            running[cid] = pending
+            pending += 1
+        if running:
+            engine.advance()
+            for cid in engine.poll():
+                i = running.pop(cid)
+                r = requests[i]
+                out = engine.fetch(cid, r.u0.shape)
+                latency[i] = (clock() - t0) - r.arrival
+                if on_result is None:
+                    results[i] = out
+                else:
+                    on_result(i, out)
+                    r.u0 = None if r.factory is not None else r.u0
+        elif pending < n:
+            wait = requests[pending].arrival - (clock() - t0)
+            if wait > 0:
+                time.sleep(min(wait, 0.01))
+        else:
+            time.sleep(idle_sleep)
+    return results, latency, clock() - t0
+
+
+class SyntheticStream:
+    """Seeded mixed 2-D workload (isentropic vortices on periodic squares)."""
+
+    def __init__(self, count, rate=2000.0, seed=0, sides=(8, 64), orders=(2, 5), mach=(0.1, 2.0),
+                 reynolds=(100.0, 1e4), p_inviscid=0.5, strength=(1.0, 5.0), nsteps=200, cfl=0.4,
+                 gamma=1.4):
+        rng = np.random.default_rng(seed)
+        self.params = []
+        t = 0.0
+        for i in range(count):
+            t += rng.exponential(1.0 / rate)
+            side = int(rng.integers(sides[0], sides[1] + 1))
+            order = int(rng.integers(orders[0], orders[1] + 1))
+            ma = float(rng.uniform(*mach))
+            inviscid = bool(rng.random() < p_inviscid)
+            re = float(rng.uniform(*reynolds))
+            b = float(rng.uniform(*strength))
+            self.params.append(dict(arrival=t, side=side, order=order, mach=ma, inviscid=inviscid,
+                                    reynolds=re, strength=b))
+        self.nsteps, self.cfl, self.gamma = nsteps, cfl, gamma
+        self._meshes = {}
+
+    def mesh(self, side, order):
+        """Periodic [-5, 5]^2 mesh, shared by the cases that draw the same size."""
+        key = (side, order)
+        if key not in self._meshes:
+            self._meshes[key] = periodic_box(2, order, (side, side), (-5.0, -5.0), (5.0, 5.0))
+        return self._meshes[key]
+
+    def case(self, i, lazy=False):
+        """Case i: domain [-5, 5]^2, freestream (rho=1, p=1, speed Ma*c along the
+        diagonal), vortex of the drawn strength; mu from Re on the unit length.
+        lazy: the initial state is built at admission."""
+        p = self.params[i]
+        m = self.mesh(p["side"], p["order"])
+        c = np.sqrt(self.gamma)
+        v = p["mach"] * c / np.sqrt(2.0)
+
+        def build():
+            return _cases.isentropic_vortex(m.coords, gamma=self.gamma, strength=p["strength"],
+                                            u_inf=(v, v))
+        u0 = None if lazy else build()
+        # fixed step: cfl * h / ((2p+1) lambda) with lambda = |u| + c bounded over
+        # the vortex, and the diffusive limit h^2 / ((p+1)^4 nu)
+        h = 10.0 / p["side"]
+        lam = np.sqrt(2.0) * v + 0.5 * p["strength"] / np.pi + c
+        dt = self.cfl * h / ((2 * p["order"] + 1) * lam)
+        mu = 0.0 if p["inviscid"] else p["mach"] * c * 1.0 / p["reynolds"]
+        if mu > 0:
+            nu = mu * self.gamma / 0.72
+            dt = min(dt, self.cfl * h * h / ((p["order"] + 1) ** 4 * nu))
+        off = (1.0, v, v, 1.0 / (self.gamma - 1.0) + v * v, 0.0)
+        return Case(mesh=m, u0=u0, nsteps=self.nsteps, dt=dt, viscous=not p["inviscid"], mu=mu,
+                    Pr=0.72, state_offset=off, arrival=p["arrival"], tag=p, factory=build)
