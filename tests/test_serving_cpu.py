@@ -1,6 +1,8 @@
 """Host logic of the continuous-batching loop, on the CPU: a fake engine with
 a memory budget and a fixed number of advance calls per case stands in for
-the GPU engine."""
+the GPU engine (admission runs on a second thread, as with the real one)."""
+import threading
+
 import numpy as np
 
 from theseus_b200.serving import Case, SyntheticStream, serve
@@ -14,29 +16,34 @@ class FakeEngine:
         self.next = 1
         self.admitted = []
         self.max_concurrent = 0
+        self.lock = threading.Lock()
 
     def admit(self, case):
         need = case.tag["bytes"]
-        if self.used + need > self.budget:
-            return None
-        cid = self.next
-        self.next += 1
-        self.used += need
-        self.running[cid] = [self.calls, case]
-        self.admitted.append(case.tag["i"])
-        self.max_concurrent = max(self.max_concurrent, len(self.running))
-        return cid
+        with self.lock:
+            if self.used + need > self.budget:
+                return None
+            cid = self.next
+            self.next += 1
+            self.used += need
+            self.running[cid] = [self.calls, case]
+            self.admitted.append(case.tag["i"])
+            self.max_concurrent = max(self.max_concurrent, len(self.running))
+            return cid
 
     def advance(self):
-        for v in self.running.values():
-            v[0] -= 1
+        with self.lock:
+            for v in self.running.values():
+                v[0] -= 1
 
     def poll(self):
-        return [cid for cid, v in self.running.items() if v[0] <= 0]
+        with self.lock:
+            return [cid for cid, v in self.running.items() if v[0] <= 0]
 
     def fetch(self, cid, shape):
-        _, case = self.running.pop(cid)
-        self.used -= case.tag["bytes"]
+        with self.lock:
+            _, case = self.running.pop(cid)
+            self.used -= case.tag["bytes"]
         return np.full(shape, float(case.tag["i"]))
 
 

@@ -63,16 +63,18 @@ __device__ __forceinline__ double log_mean(double x, double y) {
   }
   return (y - x) / log(xi);
 }
-// FP32 path: the near-equal series is summed and applied in FP64; its
-// argument u = ((xi-1)/(xi+1))^2 < 1e-4 only scales corrections of relative
-// size u/3, so it is formed in FP32.
+// FP32 path: the near-equal series is evaluated in FP64.  Its argument
+// u = ((xi-1)/(xi+1))^2 < 1e-4 only scales corrections of relative size u/3,
+// so it is formed in FP32; and with eps = u (35 + u (21 + 15 u)) / 105 <= 3.4e-5,
+// (x+y) 52.5 / (105 (1 + eps)) = (x+y)/2 (1 - eps + eps^2) to a relative
+// 4e-14, far below the FP32 result's rounding, without an FP64 division.
 __device__ __forceinline__ float log_mean(float x, float y) {
   const float xi = y / x;
   const float u = (xi * (xi - 2.0f) + 1.0f) / (xi * (xi + 2.0f) + 1.0f);
   if (u < 1e-4f) {
     const double ud = u;
-    const double denom = 105.0 + ud * (35.0 + ud * (21.0 + 15.0 * ud));
-    return (float)(((double)x + (double)y) * 52.5 / denom);
+    const double eps = ud * (35.0 + ud * (21.0 + 15.0 * ud)) * (1.0 / 105.0);
+    return (float)(((double)x + (double)y) * 0.5 * (1.0 - eps + eps * eps));
   }
   return (y - x) / logf(xi);
 }
@@ -702,9 +704,20 @@ __device__ __forceinline__ int trace_node(int N, int lf, int fp) {
 
 // ---- LTE Helmholtz gas at a node with its recovered temperature T ---------
 // Per-node staging of the LTEEC volume kernel: conserved state, T, the table
-// cell of (rho, T) and the pressure.
+// cell of (rho, T) and the free-energy jet there (lte_jet).
 enum : int { LTE_P_T = 0, LTE_P_XI = 1, LTE_P_ETA = 2, LTE_P_DR = 3, LTE_P_DT = 4, LTE_P_OFF = 5,
-             LTE_P_P = 6, LTE_P_COUNT = 7 };
+             LTE_P_H = 6, LTE_P_HR = 7, LTE_P_HT = 8, LTE_P_HRR = 9, LTE_P_HRT = 10,
+             LTE_P_COUNT = 11 };
+
+__device__ __forceinline__ LteJet lte_unpack_jet(const double *x /* LTE_P_* block */) {
+  LteJet j;
+  j.H = x[LTE_P_H];
+  j.Hr = x[LTE_P_HR];
+  j.HT = x[LTE_P_HT];
+  j.Hrr = x[LTE_P_HRR];
+  j.HrT = x[LTE_P_HRT];
+  return j;
+}
 
 __device__ __forceinline__ LteEval lte_unpack(const double *x /* LTE_P_* block */, double rho, int nx) {
   LteEval s;

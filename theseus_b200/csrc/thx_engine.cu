@@ -132,6 +132,7 @@ class Engine final : public EngineBase {
     uint64_t keep = ~uint64_t(0);  // keep freed memory in the pool
     cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
     if (cudaStreamCreateWithFlags(&setup_, cudaStreamNonBlocking) != cudaSuccess) return THX_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&fetch_, cudaStreamNonBlocking) != cudaSuccess) return THX_ERR_CUDA;
     if (cudaEventCreateWithFlags(&setup_done_, cudaEventDisableTiming) != cudaSuccess) return THX_ERR_CUDA;
     return THX_OK;
   }
@@ -149,12 +150,19 @@ class Engine final : public EngineBase {
       cudaStreamSynchronize(setup_);
       cudaStreamDestroy(setup_);
     }
+    if (fetch_) {
+      cudaStreamSynchronize(fetch_);
+      cudaStreamDestroy(fetch_);
+    }
     if (setup_done_) cudaEventDestroy(setup_done_);
     if (pool_) cudaMemPoolDestroy(pool_);
   }
 
+  // Validation and the budget reservation happen under the engine lock; the
+  // operator set-up (host packing, stream-ordered allocations and uploads on
+  // the set-up stream) runs outside it, so one thread can admit while another
+  // advances the running groups.
   int admit(const thx_geometry *g, const thx_case *c, const double *u0, int64_t *id) override {
-    std::lock_guard<std::mutex> lock(mu_);
     if (!g || !c || !u0 || !id) return THX_ERR_INVALID_ARGUMENT;
     if (c->nsteps < 0 || !(c->dt > 0.0) || !(c->mu >= 0.0) ||
         (c->flow_model != THX_FLOW_EULER && c->flow_model != THX_FLOW_NAVIER_STOKES) ||
@@ -166,7 +174,16 @@ class Engine final : public EngineBase {
       return THX_ERR_INVALID_ARGUMENT;
     if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
     const size_t bytes = case_bytes(g, &cfg_, c->flow_model);
-    if (bytes_ + bytes > budget_) return THX_ERR_BUSY;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      if (bytes_ + bytes > budget_) return THX_ERR_BUSY;
+      bytes_ += bytes;  // reserved
+    }
+    auto unreserve = [&](int st) {
+      std::lock_guard<std::mutex> lock(mu_);
+      bytes_ -= bytes;
+      return st;
+    };
     thx_config cc = cfg_;
     cc.flow_model = c->flow_model;
     cc.mu = c->mu;
@@ -174,44 +191,49 @@ class Engine final : public EngineBase {
     for (int k = 0; k < 5; ++k) cc.state_offset[k] = c->state_offset[k];
     auto ec = std::make_unique<EngineCase>();
     thx_operator_s *h = new (std::nothrow) thx_operator_s();
-    if (!h) return THX_ERR_OUT_OF_MEMORY;
+    if (!h) return unreserve(THX_ERR_OUT_OF_MEMORY);
     h->device = device_;
     h->pool = pool_;
     h->setup_stream = setup_;
     ec->h = h;
-    int st = op_create(g, &cc, h, nullptr);
-    if (st) {
+    auto fail = [&](int st) {
       op_free(h);
       delete h;
-      return st;
-    }
+      ec->h = nullptr;
+      return unreserve(st);
+    };
+    int st = op_create(g, &cc, h, nullptr);
+    if (st) return fail(st);
     const size_t n = (size_t)h->L * h->neq;
     if ((st = alloc(h, &ec->u, n)) || (st = alloc(h, &h->y, n)) ||
-        (h->mixed && (st = alloc(h, &h->yf, n)))) {
-      op_free(h);
-      delete h;
-      return st;
-    }
+        (h->mixed && (st = alloc(h, &h->yf, n))))
+      return fail(st);
     if (cudaMemcpyAsync(ec->u, u0, n * sizeof(double), cudaMemcpyHostToDevice, setup_) != cudaSuccess ||
         (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
-        cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventRecord(setup_done_, setup_) != cudaSuccess) {
+        cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(THX_ERR_CUDA);
+    }
+    std::lock_guard<std::mutex> lock(mu_);
+    // the groups wait on the latest record before their next launch
+    if (cudaEventRecord(setup_done_, setup_) != cudaSuccess) {
       cudaGetLastError();
       op_free(h);
       delete h;
+      bytes_ -= bytes;
       return THX_ERR_CUDA;
     }
     Group<R> *G = nullptr;
     if ((st = group_for(h, &G))) {
       op_free(h);
       delete h;
+      bytes_ -= bytes;
       return st;
     }
     ec->id = next_id_++;
     ec->dt = c->dt;
     ec->steps_left = c->nsteps;
     ec->bytes = bytes;
-    bytes_ += bytes;
     G->cases.push_back(ec.get());
     G->dirty = true;
     *id = ec->id;
@@ -250,9 +272,9 @@ class Engine final : public EngineBase {
     EngineCase *c = it->second.get();
     if (!c->finished) return THX_ERR_BUSY;
     const size_t n = (size_t)c->h->L * c->h->neq;
-    if (cudaStreamWaitEvent(setup_, c->done, 0) != cudaSuccess ||
-        cudaMemcpyAsync(u_host, c->u, n * sizeof(double), cudaMemcpyDeviceToHost, setup_) != cudaSuccess ||
-        cudaStreamSynchronize(setup_) != cudaSuccess) {
+    if (cudaStreamWaitEvent(fetch_, c->done, 0) != cudaSuccess ||
+        cudaMemcpyAsync(u_host, c->u, n * sizeof(double), cudaMemcpyDeviceToHost, fetch_) != cudaSuccess ||
+        cudaStreamSynchronize(fetch_) != cudaSuccess) {
       cudaGetLastError();
       return THX_ERR_CUDA;
     }
@@ -581,6 +603,7 @@ class Engine final : public EngineBase {
   int device_ = 0, sms_ = 148;
   cudaMemPool_t pool_ = nullptr;
   cudaStream_t setup_ = nullptr;
+  cudaStream_t fetch_ = nullptr;  // result copies to the host
   cudaEvent_t setup_done_ = nullptr;
   std::map<Key, std::unique_ptr<Group<R>>> groups_;
   std::map<int64_t, std::unique_ptr<EngineCase>> cases_;

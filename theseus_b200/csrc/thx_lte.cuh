@@ -293,16 +293,193 @@ THX_HDC void lte_discrete_gradient(const LteDev &t, const LteEval &left, const L
   *gbeta = gb;
 }
 
-// LTEEC flux from two evaluated endpoints with their pressures p1, p2: FACE
+// ---- both discrete gradients at once ------------------------------------
+// The pressure (P=0) and Gibbs (P=1) gradients of the LTEEC means evaluate
+// the same bicubic jets at the same points; lte_discrete_gradients forms each
+// jet once and, when both endpoints share a table cell, reads that cell's
+// sixteen corner values once.  Every output is computed with the operations,
+// in the order, of lte_discrete_gradient<P>.
+struct LteCorners {
+  double H[4], Hr[4], HT[4], HrT[4];  // corner j = rho side + 2 * T side
+  double dr, dt;
+};
+
+THX_HD LteCorners lte_corners(const LteDev &t, const LteCell &c) {
+  const long ps = (long)t.nx * t.ny;
+  const double *H = t.planes + c.off;
+  LteCorners k;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = (j & 1) + (j >> 1) * c.nx;
+    k.H[j] = H[o];
+    k.Hr[j] = H[ps + o];
+    k.HT[j] = H[2 * ps + o];
+    k.HrT[j] = H[3 * ps + o];
+  }
+  k.dr = c.dr;
+  k.dt = c.dt;
+  return k;
+}
+
+template <int DR, int DT>
+THX_HD double lte_eval_k(const LteCorners &k, double xi, double eta) {
+  double r = 0.0;
+#pragma unroll
+  for (int ds = 0; ds < 2; ++ds) {
+    const double dv = hpos<DR>(ds, xi), dsl = hslope<DR>(ds, xi);
+#pragma unroll
+    for (int ts = 0; ts < 2; ++ts) {
+      const int o = ds + 2 * ts;
+      const double tv = hpos<DT>(ts, eta), tsl = hslope<DT>(ts, eta);
+      r += k.H[o] * dv * tv;
+      r += (k.Hr[o] * k.dr) * dsl * tv;
+      r += (k.HT[o] * k.dt) * dv * tsl;
+      r += (k.HrT[o] * k.dr * k.dt) * dsl * tsl;
+    }
+  }
+  return r / (hscale<DR>(k.dr) * hscale<DT>(k.dt));
+}
+
+template <int AXIS, int DR, int DT>
+THX_HD double lte_divided_k(const LteCorners &k, double xi1, double eta1, double xi2, double eta2) {
+  double r = 0.0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double rv = AXIS == 0 ? hdivpos<DR>(i, xi1, xi2) : hpos<DR>(i, xi1);
+    const double rs = AXIS == 0 ? hdivslope<DR>(i, xi1, xi2) : hslope<DR>(i, xi1);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const double tv = AXIS == 1 ? hdivpos<DT>(j, eta1, eta2) : hpos<DT>(j, eta1);
+      const double ts = AXIS == 1 ? hdivslope<DT>(j, eta1, eta2) : hslope<DT>(j, eta1);
+      const int o = i + 2 * j;
+      r += k.H[o] * rv * tv;
+      r += (k.Hr[o] * k.dr) * rs * tv;
+      r += (k.HT[o] * k.dt) * rv * ts;
+      r += (k.HrT[o] * k.dr * k.dt) * rs * ts;
+    }
+  }
+  const double sc = hscale<DR>(k.dr) * hscale<DT>(k.dt) * (AXIS == 0 ? k.dr : k.dt);
+  return r / sc;
+}
+
+// Jets of one endpoint at its own point: H, H_rho, H_T, H_rhorho, H_rhoT.
+struct LteJet {
+  double H, Hr, HT, Hrr, HrT;
+};
+
+THX_HD LteJet lte_jet(const LteDev &t, const LteEval &s) {
+  const LteCorners k = lte_corners(t, s.cell);
+  LteJet j;
+  j.H = lte_eval_k<0, 0>(k, s.xi, s.eta);
+  j.Hr = lte_eval_k<1, 0>(k, s.xi, s.eta);
+  j.HT = lte_eval_k<0, 1>(k, s.xi, s.eta);
+  j.Hrr = lte_eval_k<2, 0>(k, s.xi, s.eta);
+  j.HrT = lte_eval_k<1, 1>(k, s.xi, s.eta);
+  return j;
+}
+
+// g[0..3] = (p: d/drho, d/dbeta; g: d/drho, d/dbeta); jl, jr: lte_jet of
+// left and right
+THX_HDC void lte_discrete_gradients(const LteDev &t, const LteEval &left, const LteEval &right,
+                                    const LteJet &jl, const LteJet &jr, double *g) {
+  const bool rev = left.rho > right.rho || (left.rho == right.rho && left.T > right.T);
+  const LteEval &A = rev ? right : left;
+  const LteEval &B = rev ? left : right;
+  const LteJet &JA = rev ? jr : jl;
+  const LteJet &JB = rev ? jl : jr;
+  const double b1 = 1 / A.T, b2 = 1 / B.T;
+  const double dr = B.rho - A.rho, db = b2 - b1;
+  const double rmx = A.rho > B.rho ? A.rho : B.rho;
+  const double bmx = b1 > b2 ? b1 : b2;
+  const bool ddiff = fabs(dr) >= 2.22e-15 + 1.49e-8 * rmx;
+  const bool bdiff = fabs(db) >= 2.22e-15 + 1.49e-8 * bmx;
+  // f11, f22: pressure and Gibbs energy at the endpoints
+  const double p11 = A.rho * A.rho * JA.Hr, p22 = B.rho * B.rho * JB.Hr;
+  const double g11 = JA.H + A.rho * JA.Hr, g22 = JB.H + B.rho * JB.Hr;
+  double pr = 0.0, pb = 0.0, gr = 0.0, gb = 0.0;
+  if (A.cell.off == B.cell.off) {
+    const LteCorners k = lte_corners(t, A.cell);
+    const double r1 = A.rho, r2 = B.rho;
+    if (ddiff) {
+      double ps[2], gs[2];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const double eta = side == 0 ? A.eta : B.eta;
+        const double mean_hr = 0.5 * (lte_eval_k<1, 0>(k, A.xi, eta) + lte_eval_k<1, 0>(k, B.xi, eta));
+        const double div_hr = lte_divided_k<0, 1, 0>(k, A.xi, eta, B.xi, eta);
+        const double div_h = lte_divided_k<0, 0, 0>(k, A.xi, eta, B.xi, eta);
+        ps[side] = 0.5 * (r1 * r1 + r2 * r2) * div_hr + (r1 + r2) * mean_hr;
+        gs[side] = div_h + 0.5 * (r1 + r2) * div_hr + mean_hr;
+      }
+      pr = 0.5 * (ps[0] * b1 + ps[1] * b2);
+      gr = 0.5 * (gs[0] * b1 + gs[1] * b2);
+    }
+    if (bdiff) {
+      const double mean_t = 0.5 * (A.T + B.T);
+      double ps[2], gs[2];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const double xi = side == 0 ? A.xi : B.xi;
+        const double rho = side == 0 ? A.rho : B.rho;
+        const double mean_hr = 0.5 * (lte_eval_k<1, 0>(k, xi, A.eta) + lte_eval_k<1, 0>(k, xi, B.eta));
+        const double div_hr = lte_divided_k<1, 1, 0>(k, xi, A.eta, xi, B.eta);
+        const double hr_beta = mean_hr - mean_t * div_hr;
+        const double mean_h = 0.5 * (lte_eval_k<0, 0>(k, xi, A.eta) + lte_eval_k<0, 0>(k, xi, B.eta));
+        const double div_h = lte_divided_k<1, 0, 0>(k, xi, A.eta, xi, B.eta);
+        ps[side] = rho * rho * hr_beta;
+        gs[side] = mean_h - mean_t * div_h + rho * hr_beta;
+      }
+      pb = 0.5 * (ps[0] + ps[1]);
+      gb = 0.5 * (gs[0] + gs[1]);
+    }
+  } else if (ddiff || bdiff) {
+    const LteEval s12 = lte_at(t, A.rho, B.T), s21 = lte_at(t, B.rho, A.T);
+    const LteCorners k12 = lte_corners(t, s12.cell), k21 = lte_corners(t, s21.cell);
+    const double hr12 = lte_eval_k<1, 0>(k12, s12.xi, s12.eta);
+    const double hr21 = lte_eval_k<1, 0>(k21, s21.xi, s21.eta);
+    const double p12 = s12.rho * s12.rho * hr12, p21 = s21.rho * s21.rho * hr21;
+    const double g12 = lte_eval_k<0, 0>(k12, s12.xi, s12.eta) + s12.rho * hr12;
+    const double g21 = lte_eval_k<0, 0>(k21, s21.xi, s21.eta) + s21.rho * hr21;
+    if (ddiff) {
+      pr = 0.5 * ((p21 * b1 - p11 * b1) + (p22 * b2 - p12 * b2)) / dr;
+      gr = 0.5 * ((g21 * b1 - g11 * b1) + (g22 * b2 - g12 * b2)) / dr;
+    }
+    if (bdiff) {
+      pb = 0.5 * ((p12 * b2 - p11 * b1) + (p22 * b2 - p21 * b1)) / db;
+      gb = 0.5 * ((g12 * b2 - g11 * b1) + (g22 * b2 - g21 * b1)) / db;
+    }
+  }
+  if (!ddiff) {
+    const double dpA = 2 * A.rho * JA.Hr + A.rho * A.rho * JA.Hrr;
+    const double dpB = 2 * B.rho * JB.Hr + B.rho * B.rho * JB.Hrr;
+    const double dgA = 2 * JA.Hr + A.rho * JA.Hrr, dgB = 2 * JB.Hr + B.rho * JB.Hrr;
+    pr = 0.5 * (dpA * b1 + dpB * b2);
+    gr = 0.5 * (dgA * b1 + dgB * b2);
+  }
+  if (!bdiff) {
+    const double dpA = A.rho * A.rho * JA.HrT, dpB = B.rho * B.rho * JB.HrT;
+    const double dgA = JA.HT + A.rho * JA.HrT, dgB = JB.HT + B.rho * JB.HrT;
+    pb = 0.5 * ((p11 - A.T * dpA) + (p22 - B.T * dpB));
+    gb = 0.5 * ((g11 - A.T * dgA) + (g22 - B.T * dgB));
+  }
+  g[0] = pr;
+  g[1] = pb;
+  g[2] = gr;
+  g[3] = gb;
+}
+
+// LTEEC flux from two evaluated endpoints with their jets (lte_jet): FACE
 // uses the normal d1 and the Lax dissipation; the volume form averages the
 // two metric rows.
 template <int DIM, bool FACE>
 THX_HD void lte_ec_flux(const LteDev &t, const double *q1, const double *q2, const LteEval &s1,
-                        const LteEval &s2, double p1, double p2, const double *d1, const double *d2,
-                        double *F) {
-  double pr, pb, gr, gb;
-  lte_discrete_gradient<0>(t, s1, s2, &pr, &pb);
-  lte_discrete_gradient<1>(t, s1, s2, &gr, &gb);
+                        const LteEval &s2, const LteJet &j1, const LteJet &j2, const double *d1,
+                        const double *d2, double *F) {
+  double dg[4];
+  lte_discrete_gradients(t, s1, s2, j1, j2, dg);
+  const double pr = dg[0], pb = dg[1], gr = dg[2], gb = dg[3];
+  // p = rho^2 H_rho
+  const double p1 = s1.rho * s1.rho * j1.Hr, p2 = s2.rho * s2.rho * j2.Hr;
   const double rho_mean = pr / gr;
   const double e_mean = gb - pb / rho_mean;
   double c1 = 0, c2 = 0;

@@ -142,10 +142,11 @@ class BatchEngine:
         _check(self.lib.thx_engine_advance(self._h), "thx_engine_advance")
 
     def poll(self, cap=4096):
-        ids = (C.c_int64 * cap)()
+        if getattr(self, "_ids", None) is None or len(self._ids) < cap:
+            self._ids = (C.c_int64 * cap)()
         n = C.c_int()
-        _check(self.lib.thx_engine_poll(self._h, ids, cap, C.byref(n)), "thx_engine_poll")
-        return [ids[i] for i in range(n.value)]
+        _check(self.lib.thx_engine_poll(self._h, self._ids, cap, C.byref(n)), "thx_engine_poll")
+        return [self._ids[i] for i in range(n.value)]
 
     def fetch(self, cid, shape):
         out = np.empty(shape, np.float64)
@@ -158,45 +159,87 @@ class BatchEngine:
         return {k: getattr(s, k) for k, _ in EngineStats._fields_}
 
 
-def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None):
+def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None, host=None):
     """Continuous batching: requests (sorted by .arrival, seconds from start)
     are admitted as they arrive and the budget allows, advanced together, and
     fetched when done.  Returns (results, latencies, makespan): results[i] is
     the final state of requests[i] (None when on_result(i, state) consumed it),
-    latencies[i] its arrival-to-result time."""
+    latencies[i] its arrival-to-result time.  host, if a dict, receives the
+    host seconds spent admitting, advancing/polling and fetching.
+
+    Admission (building the initial state, the library's set-up of the case)
+    runs on a second host thread, in arrival order; a request that does not
+    fit waits until a result is fetched.  The calling thread keeps the GPU
+    fed: it advances the running groups and fetches finished cases."""
+    import threading
     n = len(requests)
     results = [None] * n
     latency = np.zeros(n)
-    pending = 0                # next request not yet admitted
     running = {}               # engine id -> request index
+    cv = threading.Condition()
+    box = {"admitted": 0, "error": None, "admit_s": 0.0}
     t0 = clock()
-    while pending < n or running:
-        now = clock() - t0
-        # admit everything that has arrived, in order, while it fits
-        while pending < n and requests[pending].arrival <= now:
-            cid = engine.admit(requests[pending])
-            if cid is None:
-                break
-            running[cid] = pending
-            pending += 1
-        if running:
-            engine.advance()
-            for cid in engine.poll():
-                i = running.pop(cid)
-                r = requests[i]
-                out = engine.fetch(cid, r.u0.shape)
-                latency[i] = (clock() - t0) - r.arrival
-                if on_result is None:
-                    results[i] = out
-                else:
-                    on_result(i, out)
-                    r.u0 = None if r.factory is not None else r.u0
-        elif pending < n:
-            wait = requests[pending].arrival - (clock() - t0)
-            if wait > 0:
-                time.sleep(min(wait, 0.01))
-        else:
+
+    def admitter():
+        try:
+            for i, r in enumerate(requests):
+                wait = r.arrival - (clock() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                ta = clock()
+                r.state()
+                while True:
+                    cid = engine.admit(r)
+                    if cid is not None:
+                        break
+                    with cv:               # no room: wait for a fetch
+                        cv.wait(timeout=0.005)
+                with cv:
+                    running[cid] = i
+                    box["admitted"] += 1
+                box["admit_s"] += clock() - ta
+        except Exception as exc:           # surfaced by the serving thread
+            box["error"] = exc
+
+    th = threading.Thread(target=admitter, daemon=True)
+    th.start()
+    t_adv = t_fetch = 0.0
+    finished = 0
+    while finished < n:
+        if box["error"] is not None:
+            th.join()
+            raise box["error"]
+        with cv:
+            busy = bool(running)
+        if not busy:
             time.sleep(idle_sleep)
+            continue
+        ta = clock()
+        engine.advance()
+        done = engine.poll()
+        t_adv += clock() - ta
+        if not done:
+            time.sleep(idle_sleep)
+            continue
+        ta = clock()
+        for cid in done:
+            with cv:
+                i = running.pop(cid)
+            r = requests[i]
+            out = engine.fetch(cid, r.u0.shape)
+            latency[i] = (clock() - t0) - r.arrival
+            finished += 1
+            if on_result is None:
+                results[i] = out
+            else:
+                on_result(i, out)
+                r.u0 = None if r.factory is not None else r.u0
+            with cv:
+                cv.notify_all()
+        t_fetch += clock() - ta
+    th.join()
+    if isinstance(host, dict):
+        host.update(admit_s=box["admit_s"], advance_poll_s=t_adv, fetch_s=t_fetch)
     return results, latency, clock() - t0
 
 
