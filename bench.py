@@ -128,8 +128,24 @@ def bytes_per_phase(m, elem_size=8):
     return {"blend": nodes * neq * s, "grad": grad, "face": face, "volume": vol}
 
 
-def cpu_reference(args, sample_n=(16, 16, 16), budget_s=20.0):
-    """FP64 oracle on a bounded sample of the workload, all host threads."""
+def cpu_rhs_fn():
+    """The CPU right-hand side that stands for the reference: the reference's
+    own point kernels compiled from its headers (oracle/_ref, OpenMP over
+    elements and faces) when that library was built, else the oracle's
+    restatement.  Returns (rhs(mesh, cfg, u), kind, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = O.max_threads()
+    if os.path.exists(O.REF_PATH):
+        try:
+            O.ref()
+            return (lambda om, cfg, u: O.ref_rhs(om, cfg, u)), "reference", threads
+        except OSError:
+            pass
+    return (lambda om, cfg, u: O.rhs(om, cfg, u, nthreads=threads)), "port", threads
+
+
+def cpu_case(sample_n):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     import theseus_b200 as T
@@ -138,17 +154,23 @@ def cpu_reference(args, sample_n=(16, 16, 16), budget_s=20.0):
                 m.face_wminus, m.face_wplus)
     cfg = T.make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
                         surface_flux=WORKLOAD["surface_flux"], **physics())
-    threads = O.max_threads()
-    O.rhs(om, cfg, u, nthreads=threads)  # warm-up
+    return m, om, cfg, u
+
+
+def cpu_reference(args, sample_n=(16, 16, 16), budget_s=20.0):
+    """The CPU reference on a bounded sample of the workload, all host threads."""
+    fn, kind, threads = cpu_rhs_fn()
+    m, om, cfg, u = cpu_case(sample_n)
+    fn(om, cfg, u)  # warm-up
     t0 = time.perf_counter()
     evals = 0
     while True:
-        O.rhs(om, cfg, u, nthreads=threads)
+        fn(om, cfg, u)
         evals += 1
         if time.perf_counter() - t0 > budget_s or evals >= 200:
             break
     dt = time.perf_counter() - t0
-    return {"value": m.num_nodes * evals / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": m.num_nodes * evals / dt, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"TGV {sample_n[0]}x{sample_n[1]}x{sample_n[2]} p=4 ({m.num_nodes} nodes), "
                       f"{evals} RHS evaluations in {dt:.1f} s"}
 
@@ -157,21 +179,14 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    import theseus_b200 as T
+    fn, kind, threads = cpu_rhs_fn()
     sample = (16, 16, 16)
-    m, u = build_case(sample)
-    om = O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
-                m.face_wminus, m.face_wplus)
-    cfg = T.make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
-                        surface_flux=WORKLOAD["surface_flux"], **physics())
-    threads = O.max_threads()
+    m, om, cfg, u = cpu_case(sample)
     for _ in range(args.warmup):
-        O.rhs(om, cfg, u, nthreads=threads)
+        fn(om, cfg, u)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.rhs(om, cfg, u, nthreads=threads)
+        fn(om, cfg, u)
     dt = time.perf_counter() - t0
     value = m.num_nodes * args.steps / dt
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -180,7 +195,7 @@ def run_reference(args):
             "data": "synthetic", "impl": "reference",
             "config": dict(WORKLOAD, sample=f"{sample[0]}^3 p=4 sub-mesh of the workload",
                            parallelism="cpu threads"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": f"TGV {sample[0]}^3 p=4 ({m.num_nodes} nodes) per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -264,6 +264,14 @@ int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev,
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out,
                     double *rates_out /* [3]: advective, surface, diffusive */);
 
+/* Integral measures of a device FP64 state u (IntegralMeasures,
+ * include/RHSOperator_impl.hpp:530-717): out[9] = integrals of rho, of the
+ * kinetic energy density |m|^2/(2 rho) and of rho E (node quadrature, J times
+ * the LGL weights), then min/max pressure, min/max temperature, min/max density.
+ * Per-element sums in node order, combined on the host in element order.
+ * Blocks until done (it returns host values). */
+int thx_integral_measures(thx_handle h, const double *u, double *out);
+
 /* Device status word of the evaluations since the last read, a bitwise OR of
  * THX_STATUS_* flags.  Reading it synchronises the stream and clears it. */
 #define THX_STATUS_NONPOSITIVE 1u  /* non-positive density or pressure seen */

@@ -140,6 +140,20 @@ def rhs(mesh, cfg, u, nthreads=1, want_alpha=False):
     return du
 
 
+MEASURES = ("mass", "ke", "energy", "min_pressure", "max_pressure", "min_temperature",
+            "max_temperature", "min_density", "max_density")
+
+
+def integral_measures(mesh, cfg, u, table=None):
+    """IntegralMeasures (include/RHSOperator_impl.hpp:530-717) of state u."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.zeros(9)
+    tab = C.byref(table.struct()) if table is not None else None
+    _check(lib().orc_integral_measures(C.byref(mesh.struct()), C.byref(cfg), tab, _dp(u), _dp(out)),
+           "orc_integral_measures")
+    return dict(zip(MEASURES, out.tolist()))
+
+
 def gradient(mesh, cfg, u, nthreads=1):
     u = np.ascontiguousarray(u, dtype=np.float64)
     g = np.zeros((mesh.dim,) + u.shape)

@@ -137,7 +137,13 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
   const bool ns = cfg->flow_model == THX_FLOW_NAVIER_STOKES;
 
   // E-vector [e][eq][node] (restr_v->Mult)
-  std::vector<double> Ue((size_t)neq * L), dUe((size_t)neq * L, 0.0), dUfv((size_t)neq * nd);
+  std::vector<double> Ue((size_t)neq * L), dUe((size_t)neq * L, 0.0);
+  // faces of each element in ascending (face, side) order: the order in
+  // which the serial restriction transpose adds face contributions
+  std::vector<std::vector<std::pair<int, int>>> elem_faces(ne);
+  for (int f = 0; f < nf; ++f)
+    for (int s = 0; s < 2; ++s) elem_faces[geo->face_elem[2 * f + s]].push_back({f, s});
+#pragma omp parallel for schedule(static)
   for (int e = 0; e < ne; ++e)
     for (int q = 0; q < neq; ++q)
       for (int a = 0; a < nd; ++a) Ue[((size_t)e * neq + q) * nd + a] = u[q * L + (size_t)e * nd + a];
@@ -147,6 +153,7 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
   std::vector<double> gradE;
   if (ns) {
     std::vector<double> Se((size_t)neq * L);
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < ne; ++e)
       for (int a = 0; a < nd; ++a) {
         double q[5], s[5];
@@ -157,6 +164,7 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
         for (int k = 0; k < neq; ++k) Se[((size_t)e * neq + k) * nd + a] = s[k];
       }
     gradE.assign((size_t)dim * neq * L, 0.0);
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < ne; ++e) {
       double *gp[3] = {nullptr, nullptr, nullptr};
       for (int c = 0; c < dim; ++c) gp[c] = gradE.data() + (size_t)c * neq * L + (size_t)e * neq * nd;
@@ -165,33 +173,42 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
             ctx, Se.data() + (size_t)e * neq * nd, geo->jac + (size_t)e * nd,
             geo->metric + (size_t)e * nd * dd, a, gp);
     }
-    // interior-face lift: per face restriction [side][eq][fp], kernel, transpose, add
-    std::vector<double> uf(2 * neq * nfp), rf((size_t)dim * 2 * neq * nfp);
+    // interior-face lift: per face restriction [side][eq][fp], kernel; the
+    // transpose adds the stored face results element by element, in face order
+    const size_t fstride = (size_t)dim * 2 * neq * nfp;
+    std::vector<double> rfall((size_t)nf * fstride);
     std::vector<double> acc((size_t)dim * neq * L, 0.0);
+#pragma omp parallel for schedule(static)
     for (int f = 0; f < nf; ++f) {
+      std::vector<double> uf(2 * neq * nfp);
+      double *rf = rfall.data() + (size_t)f * fstride;
       for (int s = 0; s < 2; ++s) {
         const int e = geo->face_elem[2 * f + s], lf = geo->face_lface[2 * f + s];
         for (int fp = 0; fp < nfp; ++fp)
           for (int q = 0; q < neq; ++q)
             uf[(s * neq + q) * nfp + fp] = Se[((size_t)e * neq + q) * nd + trace_node(dim, N, lf, fp)];
       }
-      double *rp[3] = {rf.data(), rf.data() + 2 * neq * nfp, rf.data() + 4 * neq * nfp};
+      double *rp[3] = {rf, rf + 2 * neq * nfp, rf + 4 * neq * nfp};
       for (int fp = 0; fp < nfp; ++fp)
         Theseus::DGSEMIntegrator::AssembleGradInteriorFacePointKernel(
             ctx, uf.data(), geo->face_normal + ((size_t)f * nfp + fp) * dim,
             geo->face_wminus[(size_t)f * nfp + fp], geo->face_wplus[(size_t)f * nfp + fp], fp, rp);
-      for (int c = 0; c < dim; ++c)
-        for (int s = 0; s < 2; ++s) {
-          const int e = geo->face_elem[2 * f + s], lf = geo->face_lface[2 * f + s];
+    }
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < ne; ++e)
+      for (const auto &fs : elem_faces[e]) {
+        const int f = fs.first, s = fs.second, lf = geo->face_lface[2 * f + s];
+        const double *rf = rfall.data() + (size_t)f * fstride;
+        for (int c = 0; c < dim; ++c)
           for (int fp = 0; fp < nfp; ++fp)
             for (int q = 0; q < neq; ++q)
               acc[(size_t)c * neq * L + ((size_t)e * neq + q) * nd + trace_node(dim, N, lf, fp)] +=
-                  rp[c][(s * neq + q) * nfp + fp];
-        }
-    }
+                  rf[(size_t)c * 2 * neq * nfp + (s * neq + q) * nfp + fp];
+      }
     for (size_t i = 0; i < gradE.size(); ++i) gradE[i] += acc[i];
     // entropy gradient -> primitive gradient
     for (int c = 0; c < dim; ++c)
+#pragma omp parallel for schedule(static)
       for (int e = 0; e < ne; ++e)
         for (int a = 0; a < nd; ++a) {
           double q[5], dS[5], dP[5];
@@ -209,8 +226,9 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
 
   const int nxi = (N + 1) * N * (dim > 2 ? N : 1), neta = N * (N + 1) * (dim > 2 ? N : 1),
             nzeta = N * N * (N + 1);
-  std::vector<double> vflux((size_t)dim * neq * nd);
+#pragma omp parallel for schedule(dynamic, 16)
   for (int e = 0; e < ne; ++e) {
+    std::vector<double> vflux((size_t)dim * neq * nd), dUfv((size_t)neq * nd);
     const double *ue = Ue.data() + (size_t)e * neq * nd;
     double *du = dUe.data() + (size_t)e * neq * nd;
     const double *J = geo->jac + (size_t)e * nd;
@@ -236,13 +254,16 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
     }
   }
   // restr_v->AddMultTranspose into zeroed dudt
+#pragma omp parallel for schedule(static)
   for (int e = 0; e < ne; ++e)
     for (int q = 0; q < neq; ++q)
       for (int a = 0; a < nd; ++a) dudt[q * L + (size_t)e * nd + a] = dUe[((size_t)e * neq + q) * nd + a];
-  // interior faces
-  std::vector<double> uf(2 * neq * nfp), rf(2 * neq * nfp), acc((size_t)neq * L, 0.0);
-  std::vector<double> gf((size_t)3 * 2 * neq * nfp, 0.0);
+  // interior faces: face results stored, then added element by element in face order
+  std::vector<double> rfall((size_t)nf * 2 * neq * nfp), acc((size_t)neq * L, 0.0);
+#pragma omp parallel for schedule(static)
   for (int f = 0; f < nf; ++f) {
+    std::vector<double> uf(2 * neq * nfp), gf((size_t)3 * 2 * neq * nfp, 0.0);
+    double *rf = rfall.data() + (size_t)f * 2 * neq * nfp;
     for (int s = 0; s < 2; ++s) {
       const int e = geo->face_elem[2 * f + s], lf = geo->face_lface[2 * f + s];
       for (int fp = 0; fp < nfp; ++fp)
@@ -261,17 +282,20 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
       if (ns)
         Theseus::DGSEMIntegrator::AssembleViscousFacePointKernel(
             ctx, uf.data(), nr, wm, wp, gf.data(), gf.data() + 2 * neq * nfp,
-            gf.data() + 4 * neq * nfp, 0.0, fp, rf.data());
+            gf.data() + 4 * neq * nfp, 0.0, fp, rf);
       else
-        Theseus::DGSEMIntegrator::AssembleFacePointKernel(ctx, uf.data(), nr, wm, wp, fp, rf.data());
+        Theseus::DGSEMIntegrator::AssembleFacePointKernel(ctx, uf.data(), nr, wm, wp, fp, rf);
     }
-    for (int s = 0; s < 2; ++s) {
-      const int e = geo->face_elem[2 * f + s], lf = geo->face_lface[2 * f + s];
+  }
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < ne; ++e)
+    for (const auto &fs : elem_faces[e]) {
+      const int f = fs.first, s = fs.second, lf = geo->face_lface[2 * f + s];
+      const double *rf = rfall.data() + (size_t)f * 2 * neq * nfp;
       for (int fp = 0; fp < nfp; ++fp)
         for (int q = 0; q < neq; ++q)
           acc[q * L + (size_t)e * nd + trace_node(dim, N, lf, fp)] += rf[(s * neq + q) * nfp + fp];
     }
-  }
   for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += acc[i];
   return 0;
 }

@@ -1671,6 +1671,70 @@ int orc_rhs_lte(const thx_geometry *g, const thx_config *cfg, const thx_lte_tabl
   return bad.load() ? THX_ERR_NUMERICS : THX_OK;
 }
 
+// Integral measures (include/RHSOperator_impl.hpp:530-717): per element, in
+// node order, the sums of rho, |m|^2/(2 rho) and rho E weighted by
+// J * (w_a w_b w_c), and the extrema of pressure, temperature and density;
+// then the element sums and extrema in element order.  out[9] = mass, ke,
+// energy, min p, max p, min T, max T, min rho, max rho.  LTE gas when t.
+static int integral_measures(Disc &c, const double *u, double *out) {
+  const Gas &g = c.gas;
+  const long long L = (long long)c.ne * c.nd;
+  double mass = 0, ke = 0, en = 0, pmin = 1e32, pmax = 0, tmin = 1e32, tmax = 0, rmin = 1e32, rmax = 0;
+  for (int e = 0; e < c.ne; ++e) {
+    double m_i = 0, k_i = 0, e_i = 0, pn = 1e32, px = 0, tn = 1e32, tx = 0, dn = 1e32, dx = 0;
+    for (int n = 0; n < c.nd; ++n) {
+      double q[MAXEQ];
+      for (int k = 0; k < c.neq; ++k) q[k] = u[k * L + (long long)e * c.nd + n];
+      const int a = n % c.Np, b = (n / c.Np) % c.Np, cz = n / (c.Np * c.Np);
+      double W = c.w[a] * c.w[b];
+      if (c.dim == 3) W = W * c.w[cz];
+      const double measure = c.geom->jac[(long long)e * c.nd + n] * W;
+      const double rho = q[0];
+      const double kin = ke_density(g, q);
+      const double rhoE = q[c.dim + 1];
+      double press, temper;
+      if (g.lte) {
+        const lte::Eval s = lte_state(g, q);
+        press = s.pressure();
+        temper = s.T;
+      } else {
+        press = pressure(g, q);
+        temper = temperature(g, q);
+      }
+      m_i += rho * measure;
+      k_i += kin * measure;
+      e_i += rhoE * measure;
+      tn = std::min(tn, temper); tx = std::max(tx, temper);
+      dn = std::min(dn, rho); dx = std::max(dx, rho);
+      pn = std::min(pn, press); px = std::max(px, press);
+    }
+    mass += m_i; ke += k_i; en += e_i;
+    pmin = std::min(pmin, pn); pmax = std::max(pmax, px);
+    tmin = std::min(tmin, tn); tmax = std::max(tmax, tx);
+    rmin = std::min(rmin, dn); rmax = std::max(rmax, dx);
+  }
+  const double r[9] = {mass, ke, en, pmin, pmax, tmin, tmax, rmin, rmax};
+  for (int k = 0; k < 9; ++k) out[k] = r[k];
+  return THX_OK;
+}
+
+int orc_integral_measures(const thx_geometry *g, const thx_config *cfg, const thx_lte_table *t,
+                          const double *u, double *out) {
+  Disc c;
+  int st = setup(c, g, cfg);
+  if (st) return st;
+  lte::Table v;
+  std::atomic<int> bad{0};
+  if (t) {
+    v = lte_view(t);
+    c.gas.lte = &v;
+    c.gas.bad = &bad;
+  }
+  st = integral_measures(c, u, out);
+  if (st) return st;
+  return bad.load() ? THX_ERR_NUMERICS : THX_OK;
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -120,3 +120,16 @@ def test_lte_recovery_failure_sets_status(cuda):
     # the handle stays usable
     op.Mult(to_dev(cases.lte_taylor_green(m.coords), torch.float64), du)
     assert op.read_status() == 0
+
+
+def test_lte_integral_measures_match_oracle(cuda):
+    import torch
+    tab_p, tab_o = product_table(64, 128), oracle_table(64, 128)
+    m = T.periodic_box(3, 3, (2, 3, 2), (0.0,) * 3, (2 * np.pi,) * 3)
+    u = cases.lte_taylor_green(m.coords, dT=0.2)
+    op = T.EulerOperator(m, numerical_flux="lteec", surface_flux="lteec", gas=tab_p)
+    got = op.IntegralMeasures(to_dev(u, torch.float64))
+    cfg = T.make_config(volume_flux="lteec", surface_flux="lteec")
+    ref = O.integral_measures(oracle_mesh(m), cfg, u, table=tab_o)
+    for k in ref:
+        assert abs(got[k] - ref[k]) <= 1e-14 * abs(ref[k]), (k, got[k], ref[k])

@@ -229,3 +229,19 @@ def test_status_flag(cuda):
     du, op = gpu_rhs(m, u, numerical_flux="ranocha", surface_flux="hll")
     assert op.read_status() & 1
     assert op.read_status() == 0
+
+
+@pytest.mark.parametrize("dim,order,n,ns", [(2, 3, (6, 5), False), (3, 4, (3, 2, 3), True),
+                                            (3, 2, (4, 3, 2), False)])
+def test_integral_measures_match_oracle(cuda, dim, order, n, ns):
+    """IntegralMeasures (include/RHSOperator_impl.hpp:530-717) on random geometry."""
+    m = random_geometry(box(dim, order, n), seed=order)
+    u = smooth_state(m, seed=2)
+    kw = dict(numerical_flux="ranocha", surface_flux="hll", mu=0.01, Pr=0.71)
+    op = (T.NSOperator if ns else T.EulerOperator)(m, **kw)
+    got = op.IntegralMeasures(to_dev(u))
+    cfg = T.make_config(flow="ns" if ns else "euler", volume_flux="ranocha", surface_flux="hll",
+                        mu=0.01, Pr=0.71)
+    ref = O.integral_measures(oracle_mesh(m), cfg, u)
+    for k in ref:
+        assert abs(got[k] - ref[k]) <= 1e-14 * abs(ref[k]), (k, got[k], ref[k])

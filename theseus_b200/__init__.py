@@ -60,6 +60,7 @@ def library():
         lib.thx_read_status.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
         lib.thx_describe.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
         lib.thx_rhs_profile.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _D]
+        lib.thx_integral_measures.argtypes = [C.c_void_p, C.c_void_p, _D]
         _lib = lib
     return _lib
 
@@ -272,6 +273,21 @@ class RHSOperator:
         _check(library().thx_estimate_dt(self._h, C.c_void_p(u.data_ptr()), 1.0, C.byref(dt),
                                          rates.ctypes.data_as(_D)), "thx_estimate_dt")
         return rates
+
+    MEASURES = ("mass", "ke", "energy", "min_pressure", "max_pressure", "min_temperature",
+                "max_temperature", "min_density", "max_density")
+
+    def IntegralMeasures(self, u):
+        """Integrals of rho, kinetic energy and rho E and the pressure,
+        temperature and density extrema of a device FP64 state
+        (RHSOperator::ComputeIntegralMeasures, include/RHSOperator_impl.hpp:530-717)."""
+        import torch
+        self._check_state(u, torch.float64)
+        out = np.zeros(9)
+        torch.cuda.current_stream().synchronize()
+        _check(library().thx_integral_measures(self._h, C.c_void_p(u.data_ptr()),
+                                               out.ctypes.data_as(_D)), "thx_integral_measures")
+        return dict(zip(self.MEASURES, out.tolist()))
 
     def estimate_dt(self, u, cfl):
         r = self.EstimateStability(u)

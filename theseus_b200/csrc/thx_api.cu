@@ -822,6 +822,40 @@ int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev, 
   return THX_OK;
 }
 
+int thx_integral_measures(thx_handle h, const double *u, double *out) {
+  if (!h || !u || !out) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  double *el = nullptr;
+  if (cudaMalloc(&el, sizeof(double) * 9 * (size_t)h->ne) != cudaSuccess) {
+    cudaGetLastError();
+    return THX_ERR_OUT_OF_MEMORY;
+  }
+  MeasureArgs a;
+  a.u = u; a.ne = h->ne; a.N = h->N;
+  a.jac = h->jac64; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
+  a.w = h->ops64 + 2 * h->N * h->N;
+  a.gas = h->g64; a.lte = h->lte ? 1 : 0; a.out = el; a.status = h->status;
+  const int grid = (h->ne + 127) / 128;
+  if (h->dim == 2) measures_kernel<2><<<grid, 128>>>(a);
+  else measures_kernel<3><<<grid, 128>>>(a);
+  std::vector<double> hv((size_t)9 * h->ne);
+  const bool ok = cudaGetLastError() == cudaSuccess &&
+                  cudaMemcpy(hv.data(), el, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost) == cudaSuccess;
+  cudaFree(el);
+  if (!ok) return THX_ERR_CUDA;
+  double r[9] = {0, 0, 0, 1e32, 0, 1e32, 0, 1e32, 0};
+  for (int e = 0; e < h->ne; ++e) {
+    const double *v = hv.data() + (size_t)9 * e;
+    r[0] += v[0]; r[1] += v[1]; r[2] += v[2];
+    r[3] = std::min(r[3], v[3]); r[4] = std::max(r[4], v[4]);
+    r[5] = std::min(r[5], v[5]); r[6] = std::max(r[6], v[6]);
+    r[7] = std::min(r[7], v[7]); r[8] = std::max(r[8], v[8]);
+  }
+  for (int k = 0; k < 9; ++k) out[k] = r[k];
+  return THX_OK;
+}
+
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, double *rates_out) {
   if (!h || !u || !dt_out) return THX_ERR_INVALID_ARGUMENT;
   if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only

@@ -486,14 +486,22 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   }
 }
 
-// Without blending: four CTAs per SM (FP64 measured 8 % faster than the
-// compiler's three; FP32 fits in 64 registers); blending and LTEEC keep the
-// compiler's choice.
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, VOL == VOL_LTEEC || BLEND ? 1 : 4)
-volume_kernel(const VolArgs<R> a) {
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
 }
+
+// The same with four CTAs per SM required: used for FP64 without blending,
+// where it measured 8 % faster than the compiler's three.
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 4) volume_kernel_occ4(const VolArgs<R> a) {
+  volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
+}
+
+template <typename R, int VOL, bool BLEND>
+struct VolOcc4 {
+  static constexpr bool value = !IsF32<R>::value && VOL != VOL_LTEEC && !BLEND;
+};
 
 // ---------------------------------------------------------------------------
 template <typename R>
@@ -862,6 +870,65 @@ static __global__ void widen(long long n, const float *src, double *dst) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     dst[i] = (double)src[i];
+}
+
+// ---------------------------------------------------------------------------
+// Integral measures (include/RHSOperator_impl.hpp:530-717): one thread per
+// element sums rho, |m|^2/(2 rho) and rho E over its nodes in node order,
+// weighted by J * (w_a w_b w_c), and finds the extrema of pressure,
+// temperature and density; the host combines the elements in order.
+struct MeasureArgs {
+  const double *u;
+  int ne, N;
+  const double *jac;
+  long long jac_es, jac_ns;
+  const double *w;  // LGL weights on [0,1]
+  GasT<double> gas;
+  int lte;
+  double *out;      // [e][9]
+  unsigned *status;
+};
+
+template <int DIM>
+__global__ void __launch_bounds__(128) measures_kernel(const MeasureArgs a) {
+  constexpr int NEQ = DIM + 2;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.ne) return;
+  const int N = a.N, nd = DIM == 2 ? N * N : N * N * N;
+  const long long L = (long long)a.ne * nd;
+  double m_i = 0, k_i = 0, e_i = 0, pn = 1e32, px = 0, tn = 1e32, tx = 0, dn = 1e32, dx = 0;
+  bool bad = false;
+  for (int n = 0; n < nd; ++n) {
+    double q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * nd + n];
+    const int ia = n % N, ib = (n / N) % N, ic = n / (N * N);
+    double W = a.w[ia] * a.w[ib];
+    if (DIM == 3) W = W * a.w[ic];
+    const double measure = a.jac[(long long)e * a.jac_es + (long long)n * a.jac_ns] * W;
+    const double rho = q[0];
+    const double kin = ke_density<double, DIM>(q);
+    const double rhoE = q[DIM + 1];
+    double press, temper;
+    if (a.lte) {
+      const LteEval sv = lte_state<DIM>(a.gas.lte, q, &bad);
+      press = sv.valid ? lte_pressure(a.gas.lte, sv) : 0.0;
+      temper = sv.T;
+    } else {
+      press = pressure<double, DIM>(a.gas, q);
+      temper = press / (q[0] * a.gas.R_gas);
+    }
+    m_i += rho * measure;
+    k_i += kin * measure;
+    e_i += rhoE * measure;
+    tn = fmin(tn, temper); tx = fmax(tx, temper);
+    dn = fmin(dn, rho); dx = fmax(dx, rho);
+    pn = fmin(pn, press); px = fmax(px, press);
+  }
+  double *o = a.out + (long long)e * 9;
+  o[0] = m_i; o[1] = k_i; o[2] = e_i;
+  o[3] = pn; o[4] = px; o[5] = tn; o[6] = tx; o[7] = dn; o[8] = dx;
+  if (bad) atomicOr(a.status, STATUS_EOS);
 }
 
 // ---------------------------------------------------------------------------
