@@ -338,6 +338,10 @@ def run_ours(args):
         # per conserved field: density, the momentum vector, total energy
         groups = [[0], [1, 2, 3], [4]]
         ferr = [float(((yb[g] - ya[g]).pow(2).sum() / ya[g].pow(2).sum()).sqrt()) for g in groups]
+        # kinetic-energy integral (IntegralMeasures) after the run, both paths
+        ke0 = op.IntegralMeasures(u64)["ke"]
+        ke64 = op.IntegralMeasures(ya)["ke"]
+        ke32 = op.IntegralMeasures(yb)["ke"]
         ph32 = np.zeros(4)
         for _ in range(3):
             ph32 += np.array(op32.profile(u64, d32))
@@ -354,7 +358,9 @@ def run_ours(args):
                     "final_solution_rel_l2_vs_fp64": {
                         "density": ferr[0], "momentum": ferr[1], "energy": ferr[2],
                         "max": max(ferr),
-                        "per_component": [float(x) for x in serr.tolist()]}},
+                        "per_component": [float(x) for x in serr.tolist()]},
+                    "kinetic_energy": {"t0": ke0, "fp64": ke64, "fp32_mixed": ke32,
+                                       "rel_diff": abs(ke32 - ke64) / abs(ke64)}},
             "phase_ms": {k: float(v) for k, v in zip(["blend", "grad", "face", "volume"], ph32)}}
         del op32
 
@@ -428,7 +434,14 @@ def run_serving(args):
     eng = BatchEngine(precision="fp32", steps_per_launch=args.chunk, **flux)
     host = {}
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        _, lat, makespan = serve(eng, reqs, on_result=keep, host=host)
+        try:
+            _, lat, makespan = serve(eng, reqs, on_result=keep, host=host)
+        except Exception:
+            free, total = torch.cuda.mem_get_info()
+            print(json.dumps({"serving_failed": True, "engine": eng.stats(), "host_seconds": host,
+                              "device_free_bytes": free, "device_total_bytes": total,
+                              "budget_bytes": eng.hbm_budget}), file=sys.stderr, flush=True)
+            raise
     st = eng.stats()
     eng.close()
     nodes = [r.mesh.num_nodes for r in reqs]

@@ -160,6 +160,10 @@ typedef struct thx_operator_s *thx_handle;
 /* ---- version and status ------------------------------------------------- */
 const char *thx_version(void);
 const char *thx_status_string(int status);
+/* The CUDA runtime call that last failed inside the library on the calling
+ * thread, with the runtime's error name ("" if none has).  Diagnostic only;
+ * no counterpart in the reference. */
+const char *thx_last_cuda_failure(void);
 /* Default configuration (CPG air, Chandrashekar volume / Chandrashekar surface,
  * blending off, FP64). */
 void thx_config_default(thx_config *cfg);
@@ -310,6 +314,13 @@ typedef struct {
   int64_t bytes_in_use;      /* footprint of the active cases */
   int64_t launches;          /* graph launches so far */
   int64_t cases_done;        /* cases fetched */
+  double admit_lock_s;       /* host seconds admissions waited for the engine lock */
+  double admit_setup_s;      /* host seconds in case set-up (packing, allocations) */
+  double admit_copy_s;       /* host seconds issuing the initial-state upload */
+  double advance_s;          /* host seconds inside advance (lock held) */
+  double fetch_copy_s;       /* host seconds copying results to the host */
+  int64_t pool_reserved_bytes;  /* device memory the engine's pool holds */
+  int64_t pool_used_bytes;      /* of which allocated to cases */
 } thx_engine_stats;
 
 /* Device bytes one case needs (state, stage copies, scratch, geometry). */

@@ -20,7 +20,7 @@ import numpy as np
 
 from ._abi import (Config, Geometry, LteTable, IdgParams, make_config, flux_id,  # noqa: F401
                    FLUX, FLUX_NAMES, FLOW_EULER, FLOW_NAVIER_STOKES, PRECISION_FP64,
-                   PRECISION_FP32_MIXED, THX_OK, STATUS_NONPOSITIVE, STATUS_NONFINITE,
+                   PRECISION_FP32_MIXED, THX_OK, THX_ERR_CUDA, THX_ERR_OUT_OF_MEMORY, STATUS_NONPOSITIVE, STATUS_NONFINITE,
                    STATUS_LAUNCH, STATUS_EOS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -46,6 +46,7 @@ def library():
         lib = C.CDLL(LIB_PATH)
         lib.thx_version.restype = C.c_char_p
         lib.thx_status_string.restype = C.c_char_p
+        lib.thx_last_cuda_failure.restype = C.c_char_p
         lib.thx_create.argtypes = [C.POINTER(Geometry), C.POINTER(Config), C.POINTER(C.c_void_p)]
         lib.thx_create_lte.argtypes = [C.POINTER(Geometry), C.POINTER(Config), C.POINTER(LteTable),
                                        C.POINTER(C.c_void_p)]
@@ -68,6 +69,10 @@ def library():
 def _check(st, what):
     if st != THX_OK:
         msg = library().thx_status_string(st).decode()
+        if st in (THX_ERR_CUDA, THX_ERR_OUT_OF_MEMORY):
+            detail = library().thx_last_cuda_failure().decode()
+            if detail:
+                msg += f" [{detail}]"
         raise THXError(f"{what}: {msg} (status {st})")
 
 

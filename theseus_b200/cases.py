@@ -32,7 +32,7 @@ def isentropic_vortex(coords, gamma=1.4, strength=5.0, center=(0.0, 0.0), rho_in
     f = np.exp(0.5 * (1.0 - r2))
     du = -strength / (2 * np.pi) * y * f
     dv = strength / (2 * np.pi) * x * f
-    T = T_inf - (gamma - 1.0) * strength ** 2 / (8.0 * gamma * np.pi ** 2) * np.exp(1.0 - r2)
+    T = T_inf - (gamma - 1.0) * strength ** 2 / (8.0 * gamma * np.pi ** 2) * (f * f)
     rho = rho_inf * (T / T_inf) ** (1.0 / (gamma - 1.0))
     p = rho * T
     vel = [u_inf[0] + du, u_inf[1] + dv]

@@ -105,9 +105,8 @@ int dev_alloc(T **p, size_t n, std::vector<void *> &track) {
       ? cudaMallocFromPoolAsync((void **)p, n * sizeof(T), t_alloc_owner->pool, t_alloc_owner->setup_stream)
       : cudaMalloc((void **)p, n * sizeof(T));
   if (e != cudaSuccess) {
-    cudaGetLastError();
     *p = nullptr;
-    return THX_ERR_OUT_OF_MEMORY;
+    return cuda_failed(e, pool_mode() ? "cudaMallocFromPoolAsync" : "cudaMalloc", THX_ERR_OUT_OF_MEMORY);
   }
   track.push_back(*p);
   return THX_OK;
@@ -116,6 +115,8 @@ int dev_alloc(T **p, size_t n, std::vector<void *> &track) {
 // Host-to-device copy of set-up data; stream-ordered in pool mode (pageable
 // sources are staged before the call returns).
 int to_device(void *dst, const void *src, size_t bytes) {
+  if (pool_mode() && t_alloc_owner->ring)
+    return t_alloc_owner->ring->copy(dst, src, bytes, t_alloc_owner->setup_stream);
   const cudaError_t e = pool_mode()
       ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, t_alloc_owner->setup_stream)
       : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
@@ -557,13 +558,14 @@ namespace {
 // volume+lift.  stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
 template <typename R>
 int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
-            double *um, double *y, float *yf, cudaEvent_t *ev = nullptr) {
+            double *um, double *y, float *yf, cudaEvent_t *ev = nullptr, double *du64 = nullptr) {
   R *tag = nullptr;
   if (ev) cudaEventRecord(ev[0], s);
   GradArgs<R> ga;
   FaceArgs<R> fa;
   VolArgs<R> va;
   op_args<R>(h, u, du, stage, dt, um, y, yf, ga, fa, va);
+  va.du64 = du64;
   if constexpr (!IsF32<R>::value) {
     if (h->lte) {
       cudaError_t te = h->dim == 2
@@ -614,14 +616,10 @@ int to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
 }
 
 int rhs_mixed(thx_operator_s *h, const double *u, double *dudt, cudaStream_t s, cudaEvent_t *ev) {
-  const long long n = h->L * h->neq;
+  // the volume kernel writes the FP32 rate widened to FP64 directly
   int st;
-  if (!h->kf && (st = dev_alloc(&h->kf, (size_t)n, h->allocs))) return st;
   if ((st = to_working_copy(h, u, s))) return st;
-  if ((st = run_rhs<float>(h, h->yf, h->kf, s, 0, 0.0, nullptr, nullptr, nullptr, ev))) return st;
-  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  widen<<<grid, 256, 0, s>>>(n, h->kf, dudt);
-  return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
+  return run_rhs<float>(h, h->yf, nullptr, s, 0, 0.0, nullptr, nullptr, nullptr, ev, dudt);
 }
 
 }  // namespace
@@ -648,6 +646,8 @@ int op_to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
 extern "C" {
 
 const char *thx_version(void) { return "theseus-b200 0.1 (sm_100a)"; }
+
+const char *thx_last_cuda_failure(void) { return thx::last_cuda_failure; }
 
 const char *thx_status_string(int status) {
   switch (status) {

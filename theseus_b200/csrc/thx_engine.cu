@@ -20,6 +20,7 @@
 #include "thx_operator.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -65,6 +66,7 @@ struct EngineCase {
   size_t bytes = 0;
   cudaEvent_t done = nullptr;
   bool finished = false;   // all steps enqueued; done recorded
+  bool fetching = false;   // a fetch is copying the result
 };
 
 struct EngineBase {
@@ -128,12 +130,12 @@ class Engine final : public EngineBase {
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = device_;
-    if (cudaMemPoolCreate(&pool_, &props) != cudaSuccess) return THX_ERR_CUDA;
+    THX_CU(cudaMemPoolCreate(&pool_, &props));
     uint64_t keep = ~uint64_t(0);  // keep freed memory in the pool
     cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
-    if (cudaStreamCreateWithFlags(&setup_, cudaStreamNonBlocking) != cudaSuccess) return THX_ERR_CUDA;
-    if (cudaStreamCreateWithFlags(&fetch_, cudaStreamNonBlocking) != cudaSuccess) return THX_ERR_CUDA;
-    if (cudaEventCreateWithFlags(&setup_done_, cudaEventDisableTiming) != cudaSuccess) return THX_ERR_CUDA;
+    THX_CU(cudaStreamCreateWithFlags(&setup_, cudaStreamNonBlocking));
+    if (ring_.init(size_t(64) << 20) != THX_OK) return THX_ERR_OUT_OF_MEMORY;
+    THX_CU(cudaEventCreateWithFlags(&setup_done_, cudaEventDisableTiming));
     return THX_OK;
   }
 
@@ -150,11 +152,8 @@ class Engine final : public EngineBase {
       cudaStreamSynchronize(setup_);
       cudaStreamDestroy(setup_);
     }
-    if (fetch_) {
-      cudaStreamSynchronize(fetch_);
-      cudaStreamDestroy(fetch_);
-    }
     if (setup_done_) cudaEventDestroy(setup_done_);
+    for (Bounce &b : bounce_) cudaFreeHost(b.ptr);
     if (pool_) cudaMemPoolDestroy(pool_);
   }
 
@@ -174,11 +173,14 @@ class Engine final : public EngineBase {
       return THX_ERR_INVALID_ARGUMENT;
     if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
     const size_t bytes = case_bytes(g, &cfg_, c->flow_model);
+    const double t0 = now();
     {
       std::lock_guard<std::mutex> lock(mu_);
+      t_lock_ += now() - t0;
       if (bytes_ + bytes > budget_) return THX_ERR_BUSY;
       bytes_ += bytes;  // reserved
     }
+    const double t1 = now();
     auto unreserve = [&](int st) {
       std::lock_guard<std::mutex> lock(mu_);
       bytes_ -= bytes;
@@ -195,6 +197,7 @@ class Engine final : public EngineBase {
     h->device = device_;
     h->pool = pool_;
     h->setup_stream = setup_;
+    h->ring = &ring_;
     ec->h = h;
     auto fail = [&](int st) {
       op_free(h);
@@ -208,13 +211,18 @@ class Engine final : public EngineBase {
     if ((st = alloc(h, &ec->u, n)) || (st = alloc(h, &h->y, n)) ||
         (h->mixed && (st = alloc(h, &h->yf, n))))
       return fail(st);
-    if (cudaMemcpyAsync(ec->u, u0, n * sizeof(double), cudaMemcpyHostToDevice, setup_) != cudaSuccess ||
+    const double t2 = now();
+    if (ring_.copy(ec->u, u0, n * sizeof(double), setup_) != THX_OK ||
         (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
         cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       return fail(THX_ERR_CUDA);
     }
+    const double t3 = now();
     std::lock_guard<std::mutex> lock(mu_);
+    t_lock_ += now() - t3;
+    t_setup_ += t2 - t1;
+    t_copy_ += t3 - t2;
     // the groups wait on the latest record before their next launch
     if (cudaEventRecord(setup_done_, setup_) != cudaSuccess) {
       cudaGetLastError();
@@ -243,10 +251,12 @@ class Engine final : public EngineBase {
 
   int advance() override {
     std::lock_guard<std::mutex> lock(mu_);
+    const double t0 = now();
     for (auto &kv : groups_) {
       int st = advance_group(*kv.second);
       if (st) return st;
     }
+    t_advance_ += now() - t0;
     return THX_OK;
   }
 
@@ -256,30 +266,50 @@ class Engine final : public EngineBase {
     int n = 0;
     for (auto &kv : cases_) {
       EngineCase *c = kv.second.get();
-      if (!c->finished || n >= cap) continue;
+      if (!c->finished || c->fetching || n >= cap) continue;
       const cudaError_t q = cudaEventQuery(c->done);
       if (q == cudaSuccess) ids[n++] = c->id;
-      else if (q != cudaErrorNotReady) { cudaGetLastError(); return THX_ERR_CUDA; }
+      else if (q != cudaErrorNotReady) return cuda_failed(q, "cudaEventQuery(case done)");
     }
     *count = n;
     return THX_OK;
   }
 
+  // The copy to the host runs outside the engine lock, so that fetching one
+  // case does not hold up advancing the others.
   int fetch(int64_t id, double *u_host) override {
+    EngineCase *c = nullptr;
+    size_t n = 0;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      auto it = cases_.find(id);
+      if (it == cases_.end() || !u_host) return THX_ERR_INVALID_ARGUMENT;
+      c = it->second.get();
+      if (!c->finished || c->fetching) return THX_ERR_BUSY;
+      c->fetching = true;
+      n = (size_t)c->h->L * c->h->neq;
+    }
+    const double t0 = now();
+    // through a pinned bounce buffer (a device-to-pageable copy would take the
+    // driver's slow path)
+    const size_t bytes = n * sizeof(double);
+    Bounce b = take_bounce(bytes);
+    cudaStream_t fs = nullptr;
+    cudaError_t e = b.ptr ? cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking) : cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(fs, c->done, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.ptr, c->u, bytes, cudaMemcpyDeviceToHost, fs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(fs);
+    if (e == cudaSuccess) std::memcpy(u_host, b.ptr, bytes);
+    if (fs) cudaStreamDestroy(fs);
+    give_bounce(b);
     std::lock_guard<std::mutex> lock(mu_);
-    auto it = cases_.find(id);
-    if (it == cases_.end() || !u_host) return THX_ERR_INVALID_ARGUMENT;
-    EngineCase *c = it->second.get();
-    if (!c->finished) return THX_ERR_BUSY;
-    const size_t n = (size_t)c->h->L * c->h->neq;
-    if (cudaStreamWaitEvent(fetch_, c->done, 0) != cudaSuccess ||
-        cudaMemcpyAsync(u_host, c->u, n * sizeof(double), cudaMemcpyDeviceToHost, fetch_) != cudaSuccess ||
-        cudaStreamSynchronize(fetch_) != cudaSuccess) {
-      cudaGetLastError();
-      return THX_ERR_CUDA;
+    t_fetch_ += now() - t0;
+    if (e != cudaSuccess) {
+      c->fetching = false;
+      return cuda_failed(e, "result copy");
     }
     release(c, true);
-    cases_.erase(it);
+    cases_.erase(id);
     ++done_;
     return THX_OK;
   }
@@ -291,17 +321,56 @@ class Engine final : public EngineBase {
     st->bytes_in_use = (int64_t)bytes_;
     st->launches = launches_;
     st->cases_done = done_;
+    st->admit_lock_s = t_lock_;
+    st->admit_setup_s = t_setup_;
+    st->admit_copy_s = t_copy_;
+    st->advance_s = t_advance_;
+    st->fetch_copy_s = t_fetch_;
+    uint64_t v = 0;
+    st->pool_reserved_bytes =
+        cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReservedMemCurrent, &v) == cudaSuccess ? (int64_t)v : -1;
+    v = 0;
+    st->pool_used_bytes =
+        cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrUsedMemCurrent, &v) == cudaSuccess ? (int64_t)v : -1;
   }
 
  private:
   using Key = std::tuple<int, int, bool>;
 
+  struct Bounce {
+    unsigned char *ptr = nullptr;
+    size_t size = 0;
+  };
+  Bounce take_bounce(size_t bytes) {
+    {
+      std::lock_guard<std::mutex> lock(bounce_mu_);
+      for (size_t i = 0; i < bounce_.size(); ++i)
+        if (bounce_[i].size >= bytes) {
+          Bounce b = bounce_[i];
+          bounce_.erase(bounce_.begin() + i);
+          return b;
+        }
+    }
+    Bounce b;
+    b.size = std::max(bytes, size_t(8) << 20);
+    if (cudaHostAlloc((void **)&b.ptr, b.size, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      b.ptr = nullptr;
+    }
+    return b;
+  }
+  void give_bounce(const Bounce &b) {
+    if (!b.ptr) return;
+    std::lock_guard<std::mutex> lock(bounce_mu_);
+    bounce_.push_back(b);
+  }
+
   template <typename T>
   int alloc(thx_operator_s *h, T **p, size_t n) {
-    if (cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool_, setup_) != cudaSuccess) {
-      cudaGetLastError();
+    const cudaError_t e = cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool_, setup_);
+    if (e != cudaSuccess) {
       *p = nullptr;
-      return THX_ERR_OUT_OF_MEMORY;
+      return cuda_failed(e, "cudaMallocFromPoolAsync(case state)", THX_ERR_OUT_OF_MEMORY);
     }
     h->allocs.push_back(*p);
     return THX_OK;
@@ -391,7 +460,7 @@ class Engine final : public EngineBase {
     bool grow = nc > G.cap_cases || nwv > G.cap_wv || nwf > G.cap_wf;
     if (grow) {
       // buffers may be read by a launch in flight: wait, then reallocate
-      if (cudaStreamSynchronize(G.stream) != cudaSuccess) return THX_ERR_CUDA;
+      THX_CU(cudaStreamSynchronize(G.stream));
       auto grow_to = [](int need, int have) { return std::max(need, std::max(16, 2 * have)); };
       const int cc = nc > G.cap_cases ? grow_to(nc, G.cap_cases) : G.cap_cases;
       const int cv = nwv > G.cap_wv ? grow_to(nwv, G.cap_wv) : G.cap_wv;
@@ -403,10 +472,8 @@ class Engine final : public EngineBase {
           cudaMalloc(&G.dgrad, sizeof(GradArgs<R>) * 3 * cc) != cudaSuccess ||
           cudaMalloc(&G.dwv, sizeof(BatchWork) * cv) != cudaSuccess ||
           cudaMalloc(&G.dwf, sizeof(BatchWork) * cf) != cudaSuccess ||
-          (!G.dcount && cudaMalloc(&G.dcount, sizeof(int) * 2) != cudaSuccess)) {
-        cudaGetLastError();
-        return THX_ERR_OUT_OF_MEMORY;
-      }
+          (!G.dcount && cudaMalloc(&G.dcount, sizeof(int) * 2) != cudaSuccess))
+        return cuda_failed(cudaGetLastError(), "cudaMalloc(group tables)", THX_ERR_OUT_OF_MEMORY);
       G.cap_cases = cc;
       G.cap_wv = cv;
       G.cap_wf = cf;
@@ -419,15 +486,15 @@ class Engine final : public EngineBase {
     const size_t bg = sizeof(GradArgs<R>) * 3 * nc;
     const size_t bw = sizeof(BatchWork) * (size_t)(nwv + nwf);
     const size_t need = bv + bf + bg + bw + 2 * sizeof(int) + 64;
-    if (cudaEventSynchronize(G.staged) != cudaSuccess) return THX_ERR_CUDA;  // staging free again
+    THX_CU(cudaEventSynchronize(G.staged));  // staging free again
     if (need > G.staging_bytes) {
       if (G.staging) cudaFreeHost(G.staging);
       G.staging = nullptr;
       G.staging_bytes = std::max(need, 2 * G.staging_bytes);
-      if (cudaHostAlloc((void **)&G.staging, G.staging_bytes, cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
+      const cudaError_t e = cudaHostAlloc((void **)&G.staging, G.staging_bytes, cudaHostAllocDefault);
+      if (e != cudaSuccess) {
         G.staging_bytes = 0;
-        return THX_ERR_OUT_OF_MEMORY;
+        return cuda_failed(e, "cudaHostAlloc(table staging)", THX_ERR_OUT_OF_MEMORY);
       }
     }
     VolArgs<R> *hv = reinterpret_cast<VolArgs<R> *>(G.staging);
@@ -465,13 +532,13 @@ class Engine final : public EngineBase {
                           sizeof(FaceArgs<R>) * nc, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
           cudaMemcpyAsync(G.dgrad + (size_t)stage * G.cap_cases, hg + (size_t)stage * nc,
                           sizeof(GradArgs<R>) * nc, cudaMemcpyHostToDevice, G.stream) != cudaSuccess)
-        return THX_ERR_CUDA;
+        return cuda_failed(cudaGetLastError(), "argument table upload");
     }
     if ((nwv && cudaMemcpyAsync(G.dwv, hw, sizeof(BatchWork) * nwv, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
         (nwf && cudaMemcpyAsync(G.dwf, hw + nwv, sizeof(BatchWork) * nwf, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
         cudaMemcpyAsync(G.dcount, hc, sizeof(int) * 2, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
         cudaEventRecord(G.staged, G.stream) != cudaSuccess)
-      return THX_ERR_CUDA;
+      return cuda_failed(cudaGetLastError(), "work list upload");
     G.nwv = nwv;
     G.nwf = nwf;
     G.dirty = false;
@@ -485,7 +552,7 @@ class Engine final : public EngineBase {
     }
     const int gf = 8 * sms_, gg = 2 * sms_;
     cudaGraph_t graph = nullptr;
-    if (cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return THX_ERR_CUDA;
+    THX_CU(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaSuccess;
     for (int step = 0; step < k_ && e == cudaSuccess; ++step)
       for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
@@ -496,16 +563,15 @@ class Engine final : public EngineBase {
       }
     const cudaError_t ee = cudaStreamEndCapture(G.stream, &graph);
     if (e != cudaSuccess || ee != cudaSuccess || !graph) {
-      cudaGetLastError();
       if (graph) cudaGraphDestroy(graph);
-      return THX_ERR_CUDA;
+      return e != cudaSuccess ? cuda_failed(e, "batched launch under capture")
+                              : cuda_failed(ee, "cudaStreamEndCapture");
     }
     e = cudaGraphInstantiate(&G.exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
-      cudaGetLastError();
       G.exec = nullptr;
-      return THX_ERR_CUDA;
+      return cuda_failed(e, "cudaGraphInstantiate");
     }
     G.exec_grid = grid;
     return THX_OK;
@@ -534,14 +600,14 @@ class Engine final : public EngineBase {
     for (size_t i = 0; i < G.cases.size();) {
       EngineCase *c = G.cases[i];
       if (c->steps_left < k_) {
-        if (cudaStreamWaitEvent(G.stream, setup_done_, 0) != cudaSuccess) return THX_ERR_CUDA;
+        THX_CU(cudaStreamWaitEvent(G.stream, setup_done_, 0));
         if (c->steps_left > 0) {
           int st = thx_rk3_steps(c->h, c->u, c->dt, c->steps_left, G.stream);
           if (st) return st;
         }
         c->steps_left = 0;
         c->finished = true;
-        if (cudaEventRecord(c->done, G.stream) != cudaSuccess) return THX_ERR_CUDA;
+        THX_CU(cudaEventRecord(c->done, G.stream));
         G.cases.erase(G.cases.begin() + i);
         G.dirty = true;
       } else {
@@ -552,9 +618,9 @@ class Engine final : public EngineBase {
     {
       const cudaError_t q = cudaEventQuery(G.ring[G.ring_pos]);
       if (q == cudaErrorNotReady) return THX_OK;  // two launches still queued
-      if (q != cudaSuccess) { cudaGetLastError(); return THX_ERR_CUDA; }
+      if (q != cudaSuccess) return cuda_failed(q, "cudaEventQuery(launch ring)");
     }
-    if (cudaStreamWaitEvent(G.stream, setup_done_, 0) != cudaSuccess) return THX_ERR_CUDA;
+    THX_CU(cudaStreamWaitEvent(G.stream, setup_done_, 0));
     int st;
     if (G.dirty && (st = upload_tables(G))) return st;
     int cand = -1, grid;
@@ -570,24 +636,21 @@ class Engine final : public EngineBase {
       if ((st = capture(G, grid))) return st;
     }
     if (cand >= 0) cudaEventRecord(G.t0, G.stream);
-    if (cudaGraphLaunch(G.exec, G.stream) != cudaSuccess) {
-      cudaGetLastError();
-      return THX_ERR_CUDA;
-    }
+    THX_CU(cudaGraphLaunch(G.exec, G.stream));
     if (cand >= 0) {
       cudaEventRecord(G.t1, G.stream);
       G.timing_candidate = cand;
       G.timing_work = (long long)G.nwv * k_;
     }
     ++launches_;
-    if (cudaEventRecord(G.ring[G.ring_pos], G.stream) != cudaSuccess) return THX_ERR_CUDA;
+    THX_CU(cudaEventRecord(G.ring[G.ring_pos], G.stream));
     G.ring_pos ^= 1;
     for (size_t i = 0; i < G.cases.size();) {
       EngineCase *c = G.cases[i];
       c->steps_left -= k_;
       if (c->steps_left == 0) {
         c->finished = true;
-        if (cudaEventRecord(c->done, G.stream) != cudaSuccess) return THX_ERR_CUDA;
+        THX_CU(cudaEventRecord(c->done, G.stream));
         G.cases.erase(G.cases.begin() + i);
         G.dirty = true;
       } else {
@@ -603,12 +666,19 @@ class Engine final : public EngineBase {
   int device_ = 0, sms_ = 148;
   cudaMemPool_t pool_ = nullptr;
   cudaStream_t setup_ = nullptr;
-  cudaStream_t fetch_ = nullptr;  // result copies to the host
   cudaEvent_t setup_done_ = nullptr;
+  HostRing ring_;                 // pinned staging of admission uploads
+  std::mutex bounce_mu_;
+  std::vector<Bounce> bounce_;    // pinned buffers of result copies
   std::map<Key, std::unique_ptr<Group<R>>> groups_;
   std::map<int64_t, std::unique_ptr<EngineCase>> cases_;
   size_t bytes_ = 0;
   int64_t next_id_ = 1, launches_ = 0, done_ = 0;
+  // host time accounting (seconds)
+  double t_lock_ = 0, t_setup_ = 0, t_copy_ = 0, t_advance_ = 0, t_fetch_ = 0;
+  static double now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  }
   std::mutex mu_;
 };
 

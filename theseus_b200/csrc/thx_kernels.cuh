@@ -103,8 +103,10 @@ struct VolSmem {
   static constexpr int VISC = NS ? S::EPB * DIM * (S::NEQ - 1) * S::ND : 0;
   static constexpr int SHARED = REGION > VISC ? REGION : VISC;
   static constexpr int STATE = NEEDQ ? S::EPB * S::NEQ * S::ND : 0;
+  // pair table: (lower node | upper node << 16) of every pair, per direction
+  static constexpr int PTAB = (DIM * S::PAIRS * 4 + (int)sizeof(R) - 1) / (int)sizeof(R);
   __host__ __device__ static constexpr size_t bytes(bool metric_per_node) {
-    return sizeof(R) * ((size_t)S::OPS + SHARED + STATE +
+    return sizeof(R) * ((size_t)S::OPS + SHARED + STATE + PTAB +
                         (size_t)S::EPB * (metric_per_node ? S::ND * DIM * DIM : DIM * DIM));
   }
 };
@@ -113,6 +115,7 @@ template <typename R>
 struct VolArgs {
   const R *u;
   R *du;
+  double *du64;  // stage 0: write the rate widened to FP64 here instead of du
   int ne;
   const R *jac;
   long long jac_es, jac_ns;
@@ -175,7 +178,8 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   R *sPrim = sOps + S::OPS;                               // [EPB][NPRIM][ND]
   R *sFB = sPrim + EPB * NPRIM * ND;                      // [EPB][PAIRS][NEQ]
   R *sQ = sPrim + L_::SHARED;                             // [EPB][NEQ][ND] if NEEDQ
-  R *sMet = sQ + L_::STATE;                               // per node or once per element
+  unsigned *sPT = reinterpret_cast<unsigned *>(sQ + L_::STATE);  // [DIM][PAIRS]
+  R *sMet = sQ + L_::STATE + L_::PTAB;                    // per node or once per element
   R *sFv = sPrim;                                         // [EPB][DIM][NEQ-1][ND] (NS)
   const int mns = a.met_ns != 0 ? MB : 0;                 // metric node stride in smem
   const int mbk = a.met_ns != 0 ? ND * MB : MB;           // metric element block in smem
@@ -184,6 +188,13 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   const int e0 = block * EPB;
   const long long L = (long long)a.ne * ND;
   for (int i = tid; i < 2 * N * N + N; i += blockDim.x) sOps[i] = a.ops[i];
+  for (int i = tid; i < DIM * PAIRS; i += blockDim.x) {
+    const int dir = i / PAIRS, pidx = i % PAIRS;
+    int pa, pb;
+    pair_decode<N>(pidx % S::NP, pa, pb);
+    const int line = pidx / S::NP;
+    sPT[i] = (unsigned)line_node<DIM, N>(dir, line, pa) | ((unsigned)line_node<DIM, N>(dir, line, pb) << 16);
+  }
   const R *sD2 = sOps;
   const R *sDh = sOps + N * N;
   const R *sW = sOps + 2 * N * N;
@@ -249,19 +260,23 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     for (int t = tid; t < EPB * PAIRS; t += blockDim.x) {
       const int pel = t / PAIRS, pidx = t % PAIRS;
       if (e0 + pel >= a.ne) continue;
-      const int line = pidx / S::NP;
-      int pa, pb;
-      pair_decode<N>(pidx % S::NP, pa, pb);
-      const int na = line_node<DIM, N>(dir, line, pa), nb = line_node<DIM, N>(dir, line, pb);
+      const unsigned nn = sPT[dir * PAIRS + pidx];
+      const int na = (int)(nn & 0xffffu), nb = (int)(nn >> 16);
       R A[NPRIM], B[NPRIM], met[DIM], F[NEQ];
 #pragma unroll
       for (int k = 0; k < NPRIM; ++k) {
         A[k] = sPrim[(pel * NPRIM + k) * ND + na];
         B[k] = sPrim[(pel * NPRIM + k) * ND + nb];
       }
+      if (mns == 0) {
+        // one metric per element: 0.5*(m+m) == m
 #pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        met[d] = R(0.5) * (sMet[pel * mbk + na * mns + dir * DIM + d] + sMet[pel * mbk + nb * mns + dir * DIM + d]);
+        for (int d = 0; d < DIM; ++d) met[d] = sMet[pel * mbk + dir * DIM + d];
+      } else {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          met[d] = R(0.5) * (sMet[pel * mbk + na * mns + dir * DIM + d] + sMet[pel * mbk + nb * mns + dir * DIM + d]);
+      }
       if constexpr (VOL == VOL_LTEEC) {
         // include/LTEECFlux.hpp:11-84: the averaged metric passed as both rows
         // (0.5*(m+m) == m exactly)
@@ -459,8 +474,13 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   }
   const long long base = (long long)e * ND + n;
   if (a.stage == 0) {
+    if (a.du64) {
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) a.du[k * L + base] = du[k];
+      for (int k = 0; k < NEQ; ++k) a.du64[k * L + base] = (double)du[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) a.du[k * L + base] = du[k];
+    }
   } else {
     // fused SSP-RK3 stage in the arithmetic order of mfem::RK3SSPSolver::Step
     const double dt = a.dt;
@@ -491,16 +511,17 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const Vo
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
 }
 
-// The same with four CTAs per SM required: used for FP64 without blending,
-// where it measured 8 % faster than the compiler's three.
-template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 4) volume_kernel_occ4(const VolArgs<R> a) {
+// The same with MINB CTAs per SM required.  FP64 without blending takes four
+// (8 % faster than the compiler's three); the LTEEC flux takes two (left
+// alone the compiler gives it the whole register file and one CTA).
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int MINB>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
 }
 
 template <typename R, int VOL, bool BLEND>
-struct VolOcc4 {
-  static constexpr bool value = !IsF32<R>::value && VOL != VOL_LTEEC && !BLEND;
+struct VolMinBlocks {
+  static constexpr int value = VOL == VOL_LTEEC ? 2 : (!IsF32<R>::value && !BLEND ? 4 : 0);
 };
 
 // ---------------------------------------------------------------------------
@@ -865,11 +886,6 @@ static __global__ void to_working(long long L, int neq, const double *src, float
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L * neq; i += stride)
     dst[i] = (float)(src[i] - off.v[i / L]);
-}
-static __global__ void widen(long long n, const float *src, double *dst) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-    dst[i] = (double)src[i];
 }
 
 // ---------------------------------------------------------------------------

@@ -35,11 +35,11 @@ template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 cudaError_t launch_volume(const VolArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
   static_assert(S::PAIRS >= S::ND, "subcell FV rate aliases the pair-flux buffer");
-  constexpr bool OCC4 = VolOcc4<R, VOL, BLEND>::value;
+  constexpr int MINB = VolMinBlocks<R, VOL, BLEND>::value;
   if (prepare) {
     const int bytes = (int)volume_smem_bytes<R, DIM, N, VOL, NS, BLEND>(true);
-    if constexpr (OCC4)
-      return cudaFuncSetAttribute(volume_kernel_occ4<R, DIM, N, VOL, NS, BLEND>,
+    if constexpr (MINB > 0)
+      return cudaFuncSetAttribute(volume_kernel_mb<R, DIM, N, VOL, NS, BLEND, MINB>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     else
       return cudaFuncSetAttribute(volume_kernel<R, DIM, N, VOL, NS, BLEND>,
@@ -48,7 +48,7 @@ cudaError_t launch_volume(const VolArgs<R> &a, cudaStream_t s, int prepare) {
   if (a.ne <= 0) return cudaSuccess;
   const size_t smem = volume_smem_bytes<R, DIM, N, VOL, NS, BLEND>(a.met_ns != 0);
   const int grid = (a.ne + S::EPB - 1) / S::EPB;
-  if constexpr (OCC4) volume_kernel_occ4<R, DIM, N, VOL, NS, BLEND><<<grid, S::THREADS, smem, s>>>(a);
+  if constexpr (MINB > 0) volume_kernel_mb<R, DIM, N, VOL, NS, BLEND, MINB><<<grid, S::THREADS, smem, s>>>(a);
   else volume_kernel<R, DIM, N, VOL, NS, BLEND><<<grid, S::THREADS, smem, s>>>(a);
   return cudaGetLastError();
 }

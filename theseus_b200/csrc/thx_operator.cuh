@@ -4,10 +4,98 @@
 #include "thx_launch.cuh"
 #include "theseus_b200.h"
 
+#include <cstring>
 #include <string>
 #include <vector>
 
+#include <cstdio>
+#include <deque>
+#include <mutex>
+
+#include "thx_ring.h"
+
 namespace thx {
+
+// The CUDA call that failed last on this thread inside the library, with the
+// runtime's error name ("" until one fails); read by thx_last_cuda_failure.
+inline thread_local char last_cuda_failure[192] = "";
+inline int cuda_failed(cudaError_t e, const char *call, int status = THX_ERR_CUDA) {
+  std::snprintf(last_cuda_failure, sizeof(last_cuda_failure), "%s: %s", call, cudaGetErrorName(e));
+  cudaGetLastError();
+  return status;
+}
+#define THX_CU(call)                                           \
+  do {                                                         \
+    const cudaError_t thx_e_ = (call);                         \
+    if (thx_e_ != cudaSuccess) return thx::cuda_failed(thx_e_, #call); \
+  } while (0)
+
+// Pinned host staging ring for stream-ordered uploads: a copy is written into
+// the ring on the host and sent with cudaMemcpyAsync, so the call neither
+// waits for the stream nor goes through the driver's pageable path.  Space
+// is reclaimed in FIFO order once each copy's event has completed.
+class HostRing {
+ public:
+  ~HostRing() {
+    for (cudaEvent_t ev : busy_) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : spare_) cudaEventDestroy(ev);
+    if (buf_) cudaFreeHost(buf_);
+  }
+  int init(size_t bytes) {
+    if (cudaHostAlloc((void **)&buf_, bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      buf_ = nullptr;
+      return THX_ERR_OUT_OF_MEMORY;
+    }
+    space_.reset(bytes);
+    return THX_OK;
+  }
+  // host -> device copy of `bytes` on stream s through the ring (copies of
+  // more than half the ring go directly)
+  int copy(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    const size_t need = (bytes + 255) & ~size_t(255);
+    if (!buf_ || need > space_.capacity() / 2) {
+      const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+      return e == cudaSuccess ? THX_OK : cuda_failed(e, "cudaMemcpyAsync(upload)");
+    }
+    size_t off;
+    while (!space_.place(need, &off)) {  // wait for the oldest copy
+      const cudaError_t e = cudaEventSynchronize(busy_.front());
+      if (e != cudaSuccess) return cuda_failed(e, "cudaEventSynchronize(upload ring)");
+      spare_.push_back(busy_.front());
+      busy_.pop_front();
+      space_.pop();
+    }
+    std::memcpy(buf_ + off, src, bytes);
+    cudaError_t e = cudaMemcpyAsync(dst, buf_ + off, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_failed(e, "cudaMemcpyAsync(upload ring)");
+    cudaEvent_t ev;
+    if (!spare_.empty()) {
+      ev = spare_.back();
+      spare_.pop_back();
+    } else if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) {
+      return cuda_failed(e, "cudaEventCreate(upload ring)");
+    }
+    // the span is live from here on: its bytes are read by the queued copy
+    busy_.push_back(ev);
+    space_.push(off, need);
+    if ((e = cudaEventRecord(ev, s)) != cudaSuccess) {
+      // unrecorded: the event would report complete at once, so wait for the
+      // stream before the span can be reused
+      cudaStreamSynchronize(s);
+      return cuda_failed(e, "cudaEventRecord(upload ring)");
+    }
+    return THX_OK;
+  }
+
+ private:
+  std::mutex mu_;
+  unsigned char *buf_ = nullptr;
+  RingSpace space_;
+  std::deque<cudaEvent_t> busy_;  // one per live span, oldest first
+  std::vector<cudaEvent_t> spare_;
+};
 
 // Strides of the (possibly compressed) geometry arrays on the device.
 struct Layout {
@@ -36,7 +124,6 @@ struct thx_operator_s {
   unsigned long long *stab = nullptr;
   double *y = nullptr;
   float *yf = nullptr;
-  float *kf = nullptr;   // FP32 right-hand side scratch of thx_rhs (mixed mode)
   thx::Offsets off{};    // FP32 working-copy offsets (mixed mode)
   thx::VolLaunch<double> vol64 = nullptr;
   thx::GradLaunch<double> grad64 = nullptr;
@@ -57,6 +144,7 @@ struct thx_operator_s {
   // buffers come from it on setup_stream and uploads are asynchronous there
   cudaMemPool_t pool = nullptr;
   cudaStream_t setup_stream = nullptr;
+  thx::HostRing *ring = nullptr;  // pinned staging of uploads (may be null)
   std::string desc;
 };
 

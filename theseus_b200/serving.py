@@ -37,7 +37,10 @@ class CaseDesc(C.Structure):
 
 class EngineStats(C.Structure):
     _fields_ = [("active_cases", C.c_int32), ("groups", C.c_int32), ("bytes_in_use", C.c_int64),
-                ("launches", C.c_int64), ("cases_done", C.c_int64)]
+                ("launches", C.c_int64), ("cases_done", C.c_int64), ("admit_lock_s", C.c_double),
+                ("admit_setup_s", C.c_double), ("admit_copy_s", C.c_double),
+                ("advance_s", C.c_double), ("fetch_copy_s", C.c_double),
+                ("pool_reserved_bytes", C.c_int64), ("pool_used_bytes", C.c_int64)]
 
 
 def _bind(lib):
@@ -170,26 +173,47 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
     Admission (building the initial state, the library's set-up of the case)
     runs on a second host thread, in arrival order; a request that does not
     fit waits until a result is fetched.  The calling thread keeps the GPU
-    fed: it advances the running groups and fetches finished cases."""
+    fed: it advances the running groups and hands finished cases to two
+    fetching threads."""
     import threading
     n = len(requests)
     results = [None] * n
     latency = np.zeros(n)
     running = {}               # engine id -> request index
     cv = threading.Condition()
-    box = {"admitted": 0, "error": None, "admit_s": 0.0}
+    box = {"admitted": 0, "error": None, "admit_s": 0.0, "state_s": 0.0, "call_s": 0.0}
     t0 = clock()
+
+    # initial states are built ahead of admission by a small thread pool
+    # (numpy releases the interpreter lock in its array work)
+    from concurrent.futures import ThreadPoolExecutor
+    import os
+    pool = ThreadPoolExecutor(max_workers=max(1, min(8, (os.cpu_count() or 2) - 2)))
+    depth = 64
+    futures = {}
+    submitted = [0]
+
+    def prefetch(upto):
+        while submitted[0] < min(upto, n):
+            j = submitted[0]
+            futures[j] = pool.submit(requests[j].state)
+            submitted[0] += 1
 
     def admitter():
         try:
             for i, r in enumerate(requests):
+                prefetch(i + depth)
                 wait = r.arrival - (clock() - t0)
                 if wait > 0:
                     time.sleep(wait)
                 ta = clock()
-                r.state()
+                futures.pop(i).result()
+                tb = clock()
+                box["state_s"] += tb - ta
                 while True:
+                    tc = clock()
                     cid = engine.admit(r)
+                    box["call_s"] += clock() - tc
                     if cid is not None:
                         break
                     with cv:               # no room: wait for a fetch
@@ -201,45 +225,76 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
         except Exception as exc:           # surfaced by the serving thread
             box["error"] = exc
 
+    import queue
+    fetch_q = queue.Queue()
+    queued = set()
+    tf = {"s": 0.0, "finished": 0}
+
+    def fetcher():
+        try:
+            while True:
+                cid = fetch_q.get()
+                if cid is None:
+                    return
+                with cv:
+                    i = running[cid]
+                r = requests[i]
+                ta = clock()
+                out = engine.fetch(cid, r.u0.shape)
+                latency[i] = (clock() - t0) - r.arrival
+                with cv:
+                    running.pop(cid)
+                    tf["finished"] += 1
+                    tf["s"] += clock() - ta
+                if on_result is None:
+                    results[i] = out
+                else:
+                    on_result(i, out)
+                    r.u0 = None if r.factory is not None else r.u0
+                with cv:
+                    cv.notify_all()
+        except Exception as exc:
+            box["error"] = exc
+
     th = threading.Thread(target=admitter, daemon=True)
+    fetchers = [threading.Thread(target=fetcher, daemon=True) for _ in range(2)]
     th.start()
-    t_adv = t_fetch = 0.0
-    finished = 0
-    while finished < n:
-        if box["error"] is not None:
-            th.join()
-            raise box["error"]
+    for f in fetchers:
+        f.start()
+    t_adv = 0.0
+
+    def stop():
+        for _ in fetchers:
+            fetch_q.put(None)
+        for f in fetchers:
+            f.join()
+        th.join()
+        pool.shutdown(wait=True)
+
+    while True:
         with cv:
-            busy = bool(running)
+            if tf["finished"] >= n:
+                break
+            busy = len(running) > len(queued & running.keys())
+        if box["error"] is not None:
+            stop()
+            raise box["error"]
         if not busy:
             time.sleep(idle_sleep)
             continue
         ta = clock()
         engine.advance()
-        done = engine.poll()
+        done = [cid for cid in engine.poll() if cid not in queued]
         t_adv += clock() - ta
+        for cid in done:
+            queued.add(cid)
+            fetch_q.put(cid)
         if not done:
             time.sleep(idle_sleep)
-            continue
-        ta = clock()
-        for cid in done:
-            with cv:
-                i = running.pop(cid)
-            r = requests[i]
-            out = engine.fetch(cid, r.u0.shape)
-            latency[i] = (clock() - t0) - r.arrival
-            finished += 1
-            if on_result is None:
-                results[i] = out
-            else:
-                on_result(i, out)
-                r.u0 = None if r.factory is not None else r.u0
-            with cv:
-                cv.notify_all()
-        t_fetch += clock() - ta
-    th.join()
+    stop()
     if isinstance(host, dict):
-        host.update(admit_s=box["admit_s"], advance_poll_s=t_adv, fetch_s=t_fetch)
+        host.update(admit_s=box["admit_s"], admit_state_wait_s=box["state_s"],
+                    admit_call_s=box["call_s"], advance_poll_s=t_adv, fetch_s=tf["s"])
     return results, latency, clock() - t0
 
 
