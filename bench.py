@@ -546,6 +546,94 @@ def run_lte(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sedov(args):
+    """Sedov-type blast: 64^3 hexes, p=3 (16.8 M nodes), Euler, Chandrashekar
+    volume / LLF surface flux, Persson-Peraire indicator with subcell
+    finite-volume (LLF) blending (alpha_max 0.5, alpha_min 0.001), rho = 1,
+    p = 1e-5, energy 1.0 as a normalised Gaussian of width 0.05 on the periodic
+    [-1, 1]^3.  FP64 and FP32-mixed RHS throughput, per-kernel times, the
+    fraction of blended elements, the GPU RHS against the FP64 oracle on a
+    4^3 sub-mesh, and a fixed-dt SSP-RK3 run (dt from CFL 0.5 at t = 0) in both
+    precisions with the final-solution difference."""
+    import torch
+    import theseus_b200 as T
+    from theseus_b200 import cases
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.sedov_n
+    kw = dict(numerical_flux="chandrashekar", surface_flux="llf", fv_flux="llf", blending=True,
+              alpha_max=0.5, alpha_min=0.001)
+    m = T.periodic_box(3, 3, (n, n, n), [-1.0] * 3, [1.0] * 3)
+    u = cases.sedov(m.coords, width=0.05)
+    stream = torch.cuda.current_stream()
+    out = {}
+    for prec in ("fp64", "fp32"):
+        op = T.EulerOperator(m, precision=prec, **kw)
+        ud = torch.as_tensor(u, device="cuda").contiguous()
+        du = torch.empty_like(ud)
+        for _ in range(max(args.warmup, 3)):
+            op.Mult(ud, du)
+        torch.cuda.synchronize()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                op.Mult(ud, du)
+            b.record(stream)
+            torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        ph = np.mean([op.profile(ud, du) for _ in range(3)], axis=0)
+        alpha, _ = op.blending_coefficients()
+        dt = op.estimate_dt(ud, 0.5) if prec == "fp64" else out["fp64"]["rk3"]["dt"]
+        y = ud.clone()
+        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ta.record(stream)
+        op.rk3_steps(y, dt, args.sedov_steps)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        rk_ms = ta.elapsed_time(tb)
+        out[prec] = {"dof_rhs_per_s": m.num_nodes / (ms * 1e-3), "ms_per_rhs": ms,
+                     "phase_ms": {"indicator": ph[0], "face": ph[2], "volume+fv": ph[3]},
+                     "blended_fraction": float((alpha > 0).float().mean().item()),
+                     "status": op.read_status(), "clocks": clk.summary(),
+                     "rk3": {"steps": args.sedov_steps, "dt": dt, "ms": rk_ms,
+                             "dof_rhs_per_s": 3 * args.sedov_steps * m.num_nodes / (rk_ms * 1e-3)},
+                     "_final": y.cpu().numpy()}
+        del op, ud, du, y
+        torch.cuda.empty_cache()
+    r64, r32 = out["fp64"].pop("_final"), out["fp32"].pop("_final")
+    groups = [[0], [1, 2, 3], [4]]
+    fin = {name: float(np.sqrt(((r32[g] - r64[g]) ** 2).sum() / (r64[g] ** 2).sum()))
+           for name, g in zip(("density", "momentum", "energy"), groups)}
+    # parity on a sub-mesh against the oracle (same state formula)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ms_ = T.periodic_box(3, 3, (4, 4, 4), [-1.0] * 3, [1.0] * 3)
+    us = cases.sedov(ms_.coords, width=0.05)
+    ops = T.EulerOperator(ms_, **kw)
+    us_d = torch.as_tensor(us, device="cuda").contiguous()
+    dus = torch.empty_like(us_d)
+    ops.Mult(us_d, dus)
+    om = O.Mesh(ms_.dim, ms_.order, ms_.jac, ms_.metric, ms_.face_elem, ms_.face_lface,
+                ms_.face_normal, ms_.face_wminus, ms_.face_wplus)
+    cfg = T.make_config(flow="euler", volume_flux="chandrashekar", surface_flux="llf", fv_flux="llf",
+                        blending=True, alpha_max=0.5, alpha_min=0.001)
+    ref, _, _ = O.rhs(om, cfg, us, nthreads=O.max_threads(), want_alpha=True)
+    got = dus.cpu().numpy()
+    rel = np.sqrt(((got - ref) ** 2).reshape(5, -1).sum(1) / (ref ** 2).reshape(5, -1).sum(1))
+    line = {"metric": "DOF*RHS/s (Euler, Persson-Peraire + subcell FV blending)",
+            "value": out["fp64"]["dof_rhs_per_s"], "unit": "DOF*RHS/s", "n_gpus": 1,
+            "ms_per_step": out["fp64"]["ms_per_rhs"], "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sedov_{n}^3_p3", "nodes": m.num_nodes, "rho": 1.0, "p": 1e-5,
+                       "energy": 1.0, "width": 0.05, "fluxes": {"volume": "chandrashekar",
+                                                                "surface": "llf", "fv": "llf"},
+                       "alpha_max": 0.5, "alpha_min": 0.001, "cfl": 0.5},
+            "fp64": out["fp64"], "fp32_mixed": out["fp32"],
+            "fp32_speedup": out["fp32"]["dof_rhs_per_s"] / out["fp64"]["dof_rhs_per_s"],
+            "final_solution_rel_l2_fp32_vs_fp64": dict(fin, max=max(fin.values())),
+            "rhs_rel_l2_vs_oracle_4cubed": [float(x) for x in rel]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -557,9 +645,11 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
-    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving", "lte"],
+    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving", "lte", "sedov"],
                     help="rhs: the headline RHS throughput; serving: the batched case stream; "
-                         "lte: the LTE-gas Taylor-Green vortex")
+                         "lte: the LTE-gas Taylor-Green vortex; sedov: the blended blast")
+    ap.add_argument("--sedov-n", type=int, default=64, help="sedov: elements per direction")
+    ap.add_argument("--sedov-steps", type=int, default=300, help="sedov: SSP-RK3 steps")
     ap.add_argument("--lte-n", type=int, default=24, help="lte: elements per direction")
     ap.add_argument("--cases", type=int, default=4096, help="serving: cases in the stream")
     ap.add_argument("--sample", type=int, default=256, help="serving: cases also run one at a time")
@@ -571,6 +661,8 @@ def main():
         run_serving(args)
     elif args.workload == "lte":
         run_lte(args)
+    elif args.workload == "sedov":
+        run_sedov(args)
     else:
         run_ours(args)
 

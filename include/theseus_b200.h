@@ -43,7 +43,8 @@ typedef enum {
   THX_ERR_NO_DEVICE = 4,          /* no CUDA device visible: there is no CPU fallback */
   THX_ERR_OUT_OF_MEMORY = 5,
   THX_ERR_NUMERICS = 6,           /* device-side status flag set (non-positive state, Newton failure) */
-  THX_ERR_BUSY = 7                /* batch engine: the case does not fit the memory budget now */
+  THX_ERR_BUSY = 7,               /* batch engine: the case does not fit the memory budget now */
+  THX_ERR_IO = 8                  /* checkpoint file could not be created, opened, read or written */
 } thx_status;
 
 /* Two-point volume fluxes and surface (Riemann) fluxes.  The numbering is the
@@ -354,6 +355,49 @@ int thx_describe(thx_handle h, char *buf, size_t len);
  * milliseconds: ms[0] indicator, ms[1] gradient, ms[2] face fluxes,
  * ms[3] volume + lift (0 for phases the configuration does not run). */
 int thx_rhs_profile(thx_handle h, const void *u, void *dudt, void *stream, double *ms);
+
+/* ---- checkpoint interchange (host only) ---------------------------------
+ * The reference's restart format (src/Simulation.cpp:1477-1603,
+ * include/CheckpointConfig.hpp): per rank
+ *   <dir>/Cycle<c>/checkpoint_cycle_<c>.<rank:08d>.chk =
+ *     "THESEUS_CHECKPOINT_RAW_V1\n", uint64 count, count doubles (the state
+ *     L-vector, native byte order)
+ * and once per cycle <dir>/Cycle<c>/checkpoint_cycle_<c>.json with the
+ * compatibility record below (format_version 2).  `dir` is the run's
+ * checkpoints folder (runTime.checkpoints_folder under the output directory).
+ * Failure reasons are written to msg (may be NULL) with the reference's
+ * wording. */
+typedef struct {               /* CheckpointCompatibility (CheckpointConfig.hpp:19-29) */
+  int32_t mpi_ranks;
+  int32_t order;
+  int32_t dimension;
+  int32_t num_equations;
+  int32_t real_bytes;          /* 8: FP64 states */
+  int32_t axisymmetric;
+  int64_t global_elements;
+  int64_t global_dofs;         /* the global state-vector length (num_equations x nodes) */
+} thx_checkpoint_compat;
+
+/* The metadata JSON text of a cycle (CheckpointConfig::Metadata). */
+int thx_checkpoint_metadata(double time, int cycle, const thx_checkpoint_compat *c, char *buf,
+                            size_t len);
+/* CheckpointConfig::ValidateMetadata: THX_OK with *current_format = 1, or 0
+ * for legacy metadata (time and cycle only); THX_ERR_INVALID_ARGUMENT when
+ * incompatible. */
+int thx_checkpoint_validate(const char *json, const thx_checkpoint_compat *expected,
+                            int *current_format, char *msg, size_t msg_len);
+/* Simulation::SaveCheckpoint for one rank: the state file, and the metadata
+ * when write_metadata != 0 (rank 0 in the reference, after every rank's
+ * state is complete). */
+int thx_checkpoint_save(const char *dir, int cycle, int rank, double time,
+                        const thx_checkpoint_compat *compat, const double *state, int64_t count,
+                        int write_metadata, char *msg, size_t msg_len);
+/* Simulation::LoadCheckpoint for one rank: checks the cycle, the time entry
+ * and the compatibility record, then reads `count` doubles into state (host)
+ * and the simulation time.  Legacy (MFEM grid-function) states return
+ * THX_ERR_UNSUPPORTED. */
+int thx_checkpoint_load(const char *dir, int cycle, int rank, const thx_checkpoint_compat *expected,
+                        double *time, double *state, int64_t count, char *msg, size_t msg_len);
 
 #ifdef __cplusplus
 }

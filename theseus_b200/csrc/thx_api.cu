@@ -658,6 +658,8 @@ const char *thx_status_string(int status) {
     case THX_ERR_NO_DEVICE: return "no CUDA device (no CPU fallback exists)";
     case THX_ERR_OUT_OF_MEMORY: return "out of device memory";
     case THX_ERR_NUMERICS: return "numerical status flag set";
+    case THX_ERR_BUSY: return "busy: the case does not fit the memory budget now";
+    case THX_ERR_IO: return "checkpoint file I/O failed";
   }
   return "unknown status";
 }
