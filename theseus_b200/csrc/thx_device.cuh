@@ -42,6 +42,13 @@ template <typename R> struct IsF32 { static constexpr bool value = false; };
 template <> struct IsF32<float> { static constexpr bool value = true; };
 template <typename R, int DIM> constexpr int nprim() { return DIM + 3 + (IsF32<R>::value ? 1 : 0); }
 
+// FP32 division: the fast reciprocal form (2 ulp), one special-function
+// instruction instead of the IEEE sequence, which shortens the
+// instruction-issue-bound FP32 kernels.  FP64 keeps IEEE division, so the
+// FP64 path is unchanged.
+template <typename R> __device__ __forceinline__ R fdiv(R a, R b) { return a / b; }
+template <> __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
 template <typename R> __device__ __forceinline__ R rsqrt_(R x);
 template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
@@ -63,20 +70,23 @@ __device__ __forceinline__ double log_mean(double x, double y) {
   }
   return (y - x) / log(xi);
 }
-// FP32 path: the near-equal series is evaluated in FP64.  Its argument
-// u = ((xi-1)/(xi+1))^2 < 1e-4 only scales corrections of relative size u/3,
-// so it is formed in FP32; and with eps = u (35 + u (21 + 15 u)) / 105 <= 3.4e-5,
-// (x+y) 52.5 / (105 (1 + eps)) = (x+y)/2 (1 - eps + eps^2) to a relative
-// 4e-14, far below the FP32 result's rounding, without an FP64 division.
+// FP32 path: the same function with f = (xi-1)/(xi+1) = (y-x)/(y+x) formed
+// directly (one division; y-x is exact for near-equal arguments) and
+// u = f^2.  The near-equal series is evaluated in FP64: its argument u < 1e-4
+// only scales corrections of relative size u/3, so it is formed in FP32; and
+// with eps = u (35 + u (21 + 15 u)) / 105 <= 3.4e-5, 52.5 / (105 (1 + eps)) =
+// (1 - eps + eps^2) / 2 to a relative 4e-14, far below the FP32 result's
+// rounding, without an FP64 division.
 __device__ __forceinline__ float log_mean(float x, float y) {
-  const float xi = y / x;
-  const float u = (xi * (xi - 2.0f) + 1.0f) / (xi * (xi + 2.0f) + 1.0f);
+  const float s = x + y, d = y - x;
+  const float f = fdiv(d, s);
+  const float u = f * f;
   if (u < 1e-4f) {
     const double ud = u;
     const double eps = ud * (35.0 + ud * (21.0 + 15.0 * ud)) * (1.0 / 105.0);
-    return (float)(((double)x + (double)y) * 0.5 * (1.0 - eps + eps * eps));
+    return s * (float)(0.5 * (1.0 - eps + eps * eps));
   }
-  return (y - x) / logf(xi);
+  return fdiv(d, logf(fdiv(y, x)));
 }
 
 // ---- gas functions on a conserved state q[DIM+2] -------------------------
@@ -85,7 +95,7 @@ __device__ __forceinline__ R ke_density(const R *q) {
   R m2 = R(0);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
-  return R(0.5) * m2 / q[0];
+  return fdiv(R(0.5) * m2, q[0]);
 }
 template <typename R, int DIM>
 __device__ __forceinline__ R pressure(const GasT<R> &g, const R *q) {
@@ -126,11 +136,11 @@ __device__ __forceinline__ void node_prims(const GasT<R> &g, const R *raw, R *ou
     const R p = g.p_ref + pp;
     out[0] = rho;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) out[1 + d] = q[1 + d] / rho;
+    for (int d = 0; d < DIM; ++d) out[1 + d] = fdiv(q[1 + d], rho);
     out[DIM + 1] = p;
-    if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = R(0.5) * rho / p;
-    else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = (p * g.gm1_inv) / rho + p / rho;
-    else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * (R(1) / rho);
+    if (VOL == VOL_CHANDRASHEKAR) out[DIM + 2] = fdiv(R(0.5) * rho, p);
+    else if (VOL == VOL_PIROZZOLI) out[DIM + 2] = fdiv(p * g.gm1_inv, rho) + fdiv(p, rho);
+    else if (VOL == VOL_CENTRAL) out[DIM + 2] = (q[DIM + 1] + p) * fdiv(R(1), rho);
     else out[DIM + 2] = R(0);
     out[DIM + 3] = pp;
   } else {
@@ -178,11 +188,11 @@ __device__ __forceinline__ void vol_chandrashekar(const GasT<R> &g, const R *a, 
   }
   const R beta1 = a[DIM + 2], beta2 = b[DIM + 2];
   const R beta_ln = log_mean(beta1, beta2);
-  const R p_hat = R(0.5) * (rho1 + rho2) / (beta1 + beta2);
-  h_hat += R(0.5) / beta_ln * g.gm1_av_inv + p_hat / rho_ln;
+  const R p_hat = fdiv(R(0.5) * (rho1 + rho2), beta1 + beta2);
+  h_hat += fdiv(R(0.5), beta_ln) * g.gm1_av_inv + fdiv(p_hat, rho_ln);
   // FP32: p_hat - p_ref = (beta1 pp1 + beta2 pp2)/(beta1 + beta2), exactly
   R p_mom = p_hat;
-  if constexpr (IsF32<R>::value) p_mom = (beta1 * a[DIM + 3] + beta2 * b[DIM + 3]) / (beta1 + beta2);
+  if constexpr (IsF32<R>::value) p_mom = fdiv(beta1 * a[DIM + 3] + beta2 * b[DIM + 3], beta1 + beta2);
   F[0] = rho_ln * vn;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) F[1 + d] = vn * mom_hat[d] + p_mom * met[d];
@@ -207,7 +217,7 @@ __device__ __forceinline__ void vol_ranocha(const GasT<R> &g, const R *a, const 
     ke += R(0.5) * (v1 * v2);
     fe += (R(0.5) * (p1 * v2 + p2 * v1)) * met[d];
   }
-  const R inv_beta_ln = (p1 * p2) / log_mean(rho1 * p2, rho2 * p1);
+  const R inv_beta_ln = fdiv(p1 * p2, log_mean(rho1 * p2, rho2 * p1));
   const R ie = inv_beta_ln * g.inv_gm1;
   const R p_mom = IsF32<R>::value ? R(0.5) * (mom_p<R, DIM>(a) + mom_p<R, DIM>(b)) : pbar;
   F[0] = rho_ln * vn;
@@ -245,7 +255,7 @@ __device__ __forceinline__ void vol_pirozzoli(const GasT<R> &g, const R *a, cons
 template <typename R, int DIM>
 __device__ __forceinline__ void vol_central(const R *qa, const R *qb, const R *a, const R *b,
                                             const R *met, R *F) {
-  const R ia = R(1) / a[0], ib = R(1) / b[0];
+  const R ia = fdiv(R(1), a[0]), ib = fdiv(R(1), b[0]);
   R acc0 = R(0), accE = R(0);
   R accm[DIM];
 #pragma unroll
@@ -632,8 +642,8 @@ __device__ __forceinline__ void viscous_flux(const GasT<R> &g, const R *q, const
   const R kappa = mu * g.cp * g.Pr_inv;
   const R rho = q[0];
   const R p = pressure<R, DIM>(g, q);
-  const R pressor = p / rho;
-  const R fac = g.gm1_inv / (g.cv * rho);
+  const R pressor = fdiv(p, rho);
+  const R fac = fdiv(g.gm1_inv, g.cv * rho);
   R div = R(0);
 #pragma unroll
   for (int i = 0; i < DIM; ++i) div += dp[i * NEQ + 1 + i];
@@ -650,7 +660,7 @@ __device__ __forceinline__ void viscous_flux(const GasT<R> &g, const R *q, const
       vf[(1 + mom) * DIM + dir] = tau;
     }
 #pragma unroll
-    for (int mom = 0; mom < DIM; ++mom) ef += (q[1 + mom] / rho) * vf[(1 + mom) * DIM + dir];
+    for (int mom = 0; mom < DIM; ++mom) ef += fdiv(q[1 + mom], rho) * vf[(1 + mom) * DIM + dir];
     vf[E * DIM + dir] = ef;
   }
 }
@@ -662,11 +672,11 @@ __device__ __forceinline__ void entropy_vars(const GasT<R> &g, const R *q, R *w)
   const R ke = ke_density<R, DIM>(q);
   const R p = g.gm1 * (q[DIM + 1] - ke);
   const R s = rlog(p) - g.gamma * rlog(rho);
-  const R beta = rho / p;
-  const R v2o2 = ke / rho;
-  w[0] = (g.gamma - s) / (g.gamma - R(1)) - beta * v2o2;
+  const R beta = fdiv(rho, p);
+  const R v2o2 = fdiv(ke, rho);
+  w[0] = fdiv(g.gamma - s, g.gamma - R(1)) - beta * v2o2;
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) w[1 + d] = beta * (q[1 + d] / rho);
+  for (int d = 0; d < DIM; ++d) w[1 + d] = beta * fdiv(q[1 + d], rho);
   w[DIM + 1] = -beta;
 }
 
@@ -681,12 +691,12 @@ __device__ __forceinline__ void grad_entropy_to_prim(const GasT<R> &g, const R *
   R drho = R(0);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    dP[1 + d] = p / rho * (dE[1 + d] + (q[1 + d] / rho) * dE[E]);
+    dP[1 + d] = fdiv(p, rho) * (dE[1 + d] + fdiv(q[1 + d], rho) * dE[E]);
     drho += q[1 + d] * dP[1 + d];
   }
-  drho = rho * dE[0] - dE[E] * (ke - ie) + rho * drho / p;
+  drho = rho * dE[0] - dE[E] * (ke - ie) + fdiv(rho * drho, p);
   dP[0] = drho;
-  dP[E] = p / rho * (dP[0] + p * dE[E]);
+  dP[E] = fdiv(p, rho) * (dP[0] + p * dE[E]);
 }
 
 // Local face index lf (0:x-,1:x+,2:y-,3:y+,4:z-,5:z+) and face point fp ->

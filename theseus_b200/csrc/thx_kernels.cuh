@@ -513,7 +513,12 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const Vo
 
 // The same with MINB CTAs per SM required.  FP64 without blending takes four
 // (8 % faster than the compiler's three); the LTEEC flux takes two (left
-// alone the compiler gives it the whole register file and one CTA).
+// alone the compiler gives it the whole register file and one CTA).  With
+// blending the subcell finite-volume branch, which only blended elements
+// run, would set the register count (160 in FP64, 115 in FP32) and leave one
+// or two CTAs per SM for the whole kernel: bounding it at three (FP64) or
+// four (FP32) CTAs spills in that branch only and halves the Sedov-blast
+// volume time.
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int MINB>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
@@ -521,7 +526,10 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb
 
 template <typename R, int VOL, bool BLEND>
 struct VolMinBlocks {
-  static constexpr int value = VOL == VOL_LTEEC ? 2 : (!IsF32<R>::value && !BLEND ? 4 : 0);
+  static constexpr int value = VOL == VOL_LTEEC ? 2
+                             : BLEND             ? (IsF32<R>::value ? 4 : 3)
+                             : IsF32<R>::value   ? 0
+                                                 : 4;
 };
 
 // ---------------------------------------------------------------------------
