@@ -176,10 +176,12 @@ bool pick_order_kernels(thx_operator_s *h, int vk) {
       h->vol64 = reinterpret_cast<VolLaunch<double>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad64 = reinterpret_cast<GradLaunch<double>>(k.grad);             \
       h->blend64 = reinterpret_cast<BlendLaunch<double>>(k.blend);          \
+      h->fv64 = reinterpret_cast<VolLaunch<double>>(k.fv);                  \
     } else {                                                                \
       h->vol32 = reinterpret_cast<VolLaunch<float>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad32 = reinterpret_cast<GradLaunch<float>>(k.grad);              \
       h->blend32 = reinterpret_cast<BlendLaunch<float>>(k.blend);           \
+      h->fv32 = reinterpret_cast<VolLaunch<float>>(k.fv);                   \
     }                                                                       \
     return true;                                                            \
   }
@@ -414,6 +416,18 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   if ((st = dev_alloc(&h->eta, h->ne, A))) return st;
   if ((st = dev_zero(h->alpha, sizeof(double) * h->ne))) return st;
   if ((st = dev_zero(h->eta, sizeof(double) * h->ne))) return st;
+  if (h->blend) {
+    const size_t nfv = (size_t)h->L * h->neq;
+    if (h->mixed) {
+      float *p;
+      if ((st = dev_alloc(&p, nfv, A))) return st;
+      h->fvrate = p;
+    } else {
+      double *p;
+      if ((st = dev_alloc(&p, nfv, A))) return st;
+      h->fvrate = p;
+    }
+  }
   // blending: modal transform and subcell metrics
   h->threshold = cfg->modal_threshold > 0 ? cfg->modal_threshold
                                           : 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->order, 0.25));
@@ -460,11 +474,13 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     GradArgs<float> ga{};
     ce = h->vol32(va, 0, 1);
     if (ce == cudaSuccess && h->ns) ce = h->grad32(ga, 0, 1);
+    if (ce == cudaSuccess && h->blend) ce = h->fv32(va, 0, 1);
   } else {
     VolArgs<double> va{};
     GradArgs<double> ga{};
     ce = h->vol64(va, 0, 1);
     if (ce == cudaSuccess && h->ns) ce = h->grad64(ga, 0, 1);
+    if (ce == cudaSuccess && h->blend && h->fv64) ce = h->fv64(va, 0, 1);
   }
   if (ce != cudaSuccess) { cudaGetLastError(); return THX_ERR_CUDA; }
   char buf[512];
@@ -495,6 +511,8 @@ VolLaunch<float> volk(thx_operator_s *h, float *) { return h->vol32; }
 GradLaunch<double> gradk(thx_operator_s *h, double *) { return h->grad64; }
 GradLaunch<float> gradk(thx_operator_s *h, float *) { return h->grad32; }
 BlendLaunch<double> blendk(thx_operator_s *h, double *) { return h->blend64; }
+VolLaunch<double> fvk(thx_operator_s *h, double *) { return h->fv64; }
+VolLaunch<float> fvk(thx_operator_s *h, float *) { return h->fv32; }
 BlendLaunch<float> blendk(thx_operator_s *h, float *) { return h->blend32; }
 FaceLaunch<double> facek(thx_operator_s *h, double *) { return h->face64; }
 FaceLaunch<float> facek(thx_operator_s *h, float *) { return h->face32; }
@@ -534,6 +552,7 @@ void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double 
   va.wm = G.wm; va.wp = G.wp; va.w_fs = h->lay.w_fs; va.w_ps = h->lay.w_ps;
   va.vflux = vfl;
   va.alpha = h->blend ? h->alpha : nullptr;
+  va.fvrate = h->blend ? reinterpret_cast<R *>(h->fvrate) : nullptr;
   for (int d = 0; d < 3; ++d) { va.sub[d] = G.sub[d]; va.sub_es[d] = h->lay.sub_es[d]; }
   va.fv_flux = h->cfg.fv_flux;
   va.gas = g;
@@ -587,6 +606,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if (ev) cudaEventRecord(ev[2], s);
   if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[3], s);
+  if (h->blend && fvk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (volk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[4], s);
   return THX_OK;

@@ -37,6 +37,7 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   k.vol[VOL_CENTRAL][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, true>;
   k.grad = &launch_grad<R, THX_DIM, THX_N>;
   k.blend = &launch_blend<R, THX_DIM, THX_N>;
+  k.fv = &launch_fv<R, THX_DIM, THX_N>;
 #define THX_SETB(V)                                                              \
   k.volb[V][0] = &launch_volume_batched<R, THX_DIM, THX_N, V, false>;             \
   k.volb[V][1] = &launch_volume_batched<R, THX_DIM, THX_N, V, true>;

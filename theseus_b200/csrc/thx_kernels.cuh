@@ -97,7 +97,7 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes() {
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 struct VolSmem {
   using S = Shape<DIM, N>;
-  static constexpr bool NEEDQ = (VOL == VOL_CENTRAL) || BLEND;
+  static constexpr bool NEEDQ = VOL == VOL_CENTRAL;
   static constexpr int PRIM = VOL == VOL_LTEEC ? S::NEQ + LTE_P_COUNT : nprim<R, DIM>();
   static constexpr int REGION = S::EPB * (PRIM * S::ND + S::PAIRS * S::NEQ);
   static constexpr int VISC = NS ? S::EPB * DIM * (S::NEQ - 1) * S::ND : 0;
@@ -130,6 +130,7 @@ struct VolArgs {
   const R *sub[3];        // subcell metrics (reference layout), element stride sub_es
   long long sub_es[3];
   int fv_flux;            // SurfKind for the subcell FV fluxes
+  R *fvrate;              // subcell FV rate [elem][eq][node] of blended elements (fv_kernel)
   GasT<R> gas;
   const R *ops;           // [Dhat2 N*N | Dhat N*N | w N]
   // fused SSP-RK3 stage (stage==0: plain dudt)
@@ -142,9 +143,10 @@ struct VolArgs {
   unsigned *status;
 };
 
-// Surface flux with a run-time selector (used on subcell faces).
+// Surface flux with a run-time selector (used on subcell faces).  Inlined:
+// a call would pass the states and the gas record through local memory.
 template <typename R, int DIM>
-__device__ __noinline__ void surface_flux_rt(int kind, const GasT<R> &g, const FState<R, DIM> &A,
+__device__ __forceinline__ void surface_flux_rt(int kind, const GasT<R> &g, const FState<R, DIM> &A,
                                              const FState<R, DIM> &B, const R *n, R *F) {
   switch (kind) {
     case SURF_CHANDRASHEKAR: surface_flux<R, DIM, SURF_CHANDRASHEKAR>(g, A, B, n, F); break;
@@ -328,73 +330,14 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     for (int k = 0; k < NEQ; ++k) du[k] = s * rate[k];
   }
 
-  // subcell finite-volume blend (include/DGSEMIntegrator.hpp:338-483,
-  // include/EulerOperator_impl.hpp:134-152)
-  if (BLEND && a.alpha != nullptr) {
-    bool any = false;
-    for (int k = 0; k < EPB; ++k)
-      if (e0 + k < a.ne && a.alpha[e0 + k] > 1e-16) any = true;
-    if (any) {
-      R *sRfv = sFB;  // [EPB][NEQ][ND]
-#pragma unroll 1
-      for (int dir = 0; dir < DIM; ++dir) {
-        for (int t = tid; t < EPB * S::NLINE; t += blockDim.x) {
-          const int lel = t / S::NLINE, line = t % S::NLINE;
-          const int le = e0 + lel;
-          if (le >= a.ne || !(a.alpha[le] > 1e-16)) continue;
-          const R *sub = a.sub[dir] + (long long)le * a.sub_es[dir];
-          R raw[NEQ], fn[NEQ], dus[NEQ];
-          FState<R, DIM> s1, s2;
-          int id1 = line_node<DIM, N>(dir, line, 0);
+  // subcell finite-volume blend (include/EulerOperator_impl.hpp:134-152):
+  // fv_kernel has stored the FV rate of every blended element
+  if (BLEND && a.alpha != nullptr && active) {
+    const double al = a.alpha[e];
+    if (al > 1e-16) {
+      const R af = (R)al, ad = (R)(1.0 - al);
 #pragma unroll
-          for (int k = 0; k < NEQ; ++k) { dus[k] = R(0); raw[k] = sQ[(lel * NEQ + k) * ND + id1]; }
-          make_fstate<R, DIM>(a.gas, raw, s1);
-          for (int i = 0; i < N; ++i) {
-            R Ji = a.jac[(long long)le * a.jac_es + (long long)id1 * a.jac_ns];
-            if (i < N - 1) {
-              const int id2 = line_node<DIM, N>(dir, line, i + 1);
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) raw[k] = sQ[(lel * NEQ + k) * ND + id2];
-              make_fstate<R, DIM>(a.gas, raw, s2);
-              R nrm[DIM];
-#pragma unroll
-              for (int d = 0; d < DIM; ++d) nrm[d] = sub[id2 * DIM + d];
-              surface_flux_rt<R, DIM>(a.fv_flux, a.gas, s1, s2, nrm, fn);
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) dus[k] -= fn[k];
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) dus[k] /= (Ji * sW[i]);
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) {
-                R &dst = sRfv[(lel * NEQ + k) * ND + id1];
-                dst = dir == 0 ? dus[k] : dst + dus[k];
-              }
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) dus[k] = fn[k];
-              s1 = s2;
-              id1 = id2;
-            } else {
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) dus[k] /= (Ji * sW[N - 1]);
-#pragma unroll
-              for (int k = 0; k < NEQ; ++k) {
-                R &dst = sRfv[(lel * NEQ + k) * ND + id1];
-                dst = dir == 0 ? dus[k] : dst + dus[k];
-              }
-            }
-          }
-        }
-        __syncthreads();
-      }
-      if (active) {
-        const double al = a.alpha[e];
-        if (al > 1e-16) {
-          const R af = (R)al, ad = (R)(1.0 - al);
-#pragma unroll
-          for (int k = 0; k < NEQ; ++k) du[k] = ad * du[k] + af * sRfv[(el * NEQ + k) * ND + n];
-        }
-      }
-      __syncthreads();
+      for (int k = 0; k < NEQ; ++k) du[k] = ad * du[k] + af * a.fvrate[((long long)e * NEQ + k) * ND + n];
     }
   }
 
@@ -506,19 +449,110 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   }
 }
 
+// Subcell finite-volume rate of the blended elements (include/DGSEMIntegrator.hpp:338-483):
+// along every tensor line, first-order fluxes F_j between neighbouring
+// subcells j, j+1 with the run-time FV face flux; node i of the line gets
+// (F_{i-1} - F_i) / (J_i w_i) (F_{-1} = F_{N-1} = 0), summed over directions
+// in direction order.  All subcell faces of a block are evaluated in
+// parallel, then each node forms its rate.  Blocks without a blended element
+// return at once; the volume kernel blends the stored rate in.  Kept apart
+// from the volume kernel, whose register count it would otherwise set.
+template <typename R, int DIM, int N>
+struct FvSmem {
+  using S = Shape<DIM, N>;
+  static constexpr int FACES = DIM * S::NLINE * (N - 1);  // subcell faces per element
+  static constexpr size_t bytes() {
+    return sizeof(R) * (8 + (size_t)S::EPB * S::NEQ * S::ND + (size_t)S::EPB * FACES * S::NEQ);
+  }
+};
+
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) fv_kernel(const VolArgs<R> a) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NL = S::NLINE;
+  constexpr int FACES = FvSmem<R, DIM, N>::FACES;
+  const int e0 = blockIdx.x * EPB;
+  bool any = false;
+  for (int k = 0; k < EPB; ++k)
+    if (e0 + k < a.ne && a.alpha[e0 + k] > 1e-16) any = true;
+  if (!any) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (dynamic_smem_bytes() < FvSmem<R, DIM, N>::bytes()) {
+    if (threadIdx.x == 0) atomicOr(a.status, STATUS_LAUNCH);
+    return;
+  }
+  R *sW = reinterpret_cast<R *>(smem_raw);  // quadrature weights (8 slots)
+  R *sQ = sW + 8;                           // [EPB][NEQ][ND] state
+  R *sF = sQ + EPB * NEQ * ND;              // [EPB][DIM][NL][N-1][NEQ] subcell fluxes
+  const int tid = threadIdx.x;
+  const long long L = (long long)a.ne * ND;
+  for (int i = tid; i < N; i += blockDim.x) sW[i] = a.ops[2 * N * N + i];
+  const int el = tid / ND, n = tid % ND;
+  const int e = e0 + el;
+  const bool active = (el < EPB) && (e < a.ne);
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = a.u[k * L + (long long)e * ND + n];
+  }
+  __syncthreads();
+  // subcell face fluxes: face j of a line lies between its nodes j and j+1,
+  // with the subcell normal stored at node j+1
+  for (int t = tid; t < EPB * FACES; t += blockDim.x) {
+    const int fel = t / FACES;
+    const int r = t - fel * FACES;
+    const int dir = r / (NL * (N - 1));
+    const int r2 = r - dir * (NL * (N - 1));
+    const int line = r2 / (N - 1), j = r2 - line * (N - 1);
+    const int fe = e0 + fel;
+    if (fe >= a.ne || !(a.alpha[fe] > 1e-16)) continue;
+    const int id1 = line_node<DIM, N>(dir, line, j), id2 = line_node<DIM, N>(dir, line, j + 1);
+    R raw[NEQ], fn[NEQ], nrm[DIM];
+    FState<R, DIM> s1, s2;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) raw[k] = sQ[(fel * NEQ + k) * ND + id1];
+    make_fstate<R, DIM>(a.gas, raw, s1);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) raw[k] = sQ[(fel * NEQ + k) * ND + id2];
+    make_fstate<R, DIM>(a.gas, raw, s2);
+    const R *sub = a.sub[dir] + (long long)fe * a.sub_es[dir];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nrm[d] = sub[id2 * DIM + d];
+    surface_flux_rt<R, DIM>(a.fv_flux, a.gas, s1, s2, nrm, fn);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sF[((long long)fel * FACES + r) * NEQ + k] = fn[k];
+  }
+  __syncthreads();
+  if (!active || !(a.alpha[e] > 1e-16)) return;
+  int c[3];
+  node_coords<DIM, N>(n, c);
+  const R J = a.jac[(long long)e * a.jac_es + (long long)n * a.jac_ns];
+  R rate[NEQ];
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const int i = c[dir];
+    const int line = line_of<DIM, N>(dir, c);
+    const R *Fl = sF + ((long long)el * FACES + (dir * NL + line) * (N - 1)) * NEQ;
+    const R s = J * sW[i];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      const R fm = i > 0 ? Fl[(i - 1) * NEQ + k] : R(0);
+      const R fp = i < N - 1 ? Fl[i * NEQ + k] : R(0);
+      const R d = (fm - fp) / s;
+      rate[k] = dir == 0 ? d : rate[k] + d;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) a.fvrate[((long long)e * NEQ + k) * ND + n] = rate[k];
+}
+
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
 }
 
-// The same with MINB CTAs per SM required.  FP64 without blending takes four
-// (8 % faster than the compiler's three); the LTEEC flux takes two (left
-// alone the compiler gives it the whole register file and one CTA).  With
-// blending the subcell finite-volume branch, which only blended elements
-// run, would set the register count (160 in FP64, 115 in FP32) and leave one
-// or two CTAs per SM for the whole kernel: bounding it at three (FP64) or
-// four (FP32) CTAs spills in that branch only and halves the Sedov-blast
-// volume time.
+// The same with MINB CTAs per SM required.  FP64 takes four (8 % faster
+// than the compiler's three); the LTEEC flux takes two (left alone the
+// compiler gives it the whole register file and one CTA).
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int MINB>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
@@ -526,10 +560,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb
 
 template <typename R, int VOL, bool BLEND>
 struct VolMinBlocks {
-  static constexpr int value = VOL == VOL_LTEEC ? 2
-                             : BLEND             ? (IsF32<R>::value ? 4 : 3)
-                             : IsF32<R>::value   ? 0
-                                                 : 4;
+  static constexpr int value = VOL == VOL_LTEEC ? 2 : (!IsF32<R>::value ? 4 : 0);
 };
 
 // ---------------------------------------------------------------------------

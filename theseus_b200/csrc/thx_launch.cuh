@@ -120,6 +120,18 @@ cudaError_t launch_face_batched(const FaceArgs<R> *args, const BatchWork *work, 
 }
 
 template <typename R, int DIM, int N>
+cudaError_t launch_fv(const VolArgs<R> &a, cudaStream_t s, int prepare) {
+  using S = Shape<DIM, N>;
+  constexpr size_t smem = FvSmem<R, DIM, N>::bytes();
+  if (prepare)
+    return cudaFuncSetAttribute(fv_kernel<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (a.ne <= 0 || !a.alpha || !a.fvrate) return cudaSuccess;
+  const int grid = (a.ne + S::EPB - 1) / S::EPB;
+  fv_kernel<R, DIM, N><<<grid, S::THREADS, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int N>
 cudaError_t launch_blend(const BlendArgs<R> &a, cudaStream_t s) {
   using S = Shape<DIM, N>;
   if (a.ne <= 0) return cudaSuccess;
@@ -133,6 +145,7 @@ struct OrderKernelsT {
   VolLaunch<R> vol[4][2][2];     // [volume flux][ns][blend]
   GradLaunch<R> grad;
   BlendLaunch<R> blend;
+  VolLaunch<R> fv;               // subcell FV rate of blended elements
   VolBatchLaunch<R> volb[4][2];  // [volume flux][ns]
   GradBatchLaunch<R> gradb;
 };

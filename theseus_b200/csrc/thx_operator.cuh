@@ -120,6 +120,7 @@ struct thx_operator_s {
   int *face_elem = nullptr, *face_lface = nullptr, *elem_face = nullptr;
   void *fstar = nullptr, *vflux = nullptr;  // face fluxes; NS physical viscous flux
   double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
+  void *fvrate = nullptr;  // subcell FV rate of blended elements (blending only)
   unsigned *status = nullptr;
   unsigned long long *stab = nullptr;
   double *y = nullptr;
@@ -128,10 +129,12 @@ struct thx_operator_s {
   thx::VolLaunch<double> vol64 = nullptr;
   thx::GradLaunch<double> grad64 = nullptr;
   thx::BlendLaunch<double> blend64 = nullptr;
+  thx::VolLaunch<double> fv64 = nullptr;
   thx::FaceLaunch<double> face64 = nullptr;
   thx::VolLaunch<float> vol32 = nullptr;
   thx::GradLaunch<float> grad32 = nullptr;
   thx::BlendLaunch<float> blend32 = nullptr;
+  thx::VolLaunch<float> fv32 = nullptr;
   thx::FaceLaunch<float> face32 = nullptr;
   thx::GasT<double> g64;
   thx::GasT<float> g32;
