@@ -67,6 +67,10 @@ struct EngineCase {
   cudaEvent_t done = nullptr;
   bool finished = false;   // all steps enqueued; done recorded
   bool fetching = false;   // a fetch is copying the result
+  // the case's kernel arguments of SSP-RK3 stages 1..3 (VolArgs, FaceArgs,
+  // GradArgs per stage), packed once at admission: they do not change while
+  // the case runs, so rewriting a group's tables is a copy
+  std::vector<unsigned char> packed;
 };
 
 struct EngineBase {
@@ -93,10 +97,14 @@ struct Group {
   BatchWork *dwv = nullptr, *dwf = nullptr;
   int *dcount = nullptr;  // [0] volume/gradient work, [1] face work
   int cap_cases = 0, cap_wv = 0, cap_wf = 0;
-  // pinned staging of the tables
-  unsigned char *staging = nullptr;
-  size_t staging_bytes = 0;
-  cudaEvent_t staged = nullptr;
+  // pinned staging of the tables, a ring of three: with at most two launches
+  // queued, the copies out of the slot about to be refilled have finished,
+  // so a rewrite does not wait for the GPU (with the engine lock held)
+  static constexpr int kStaging = 3;
+  unsigned char *staging[kStaging] = {nullptr, nullptr, nullptr};
+  size_t staging_bytes[kStaging] = {0, 0, 0};
+  cudaEvent_t staged[kStaging] = {nullptr, nullptr, nullptr};
+  int stage_pos = 0;
   int nwv = 0, nwf = 0;
   // kernels and graph
   VolBatchLaunch<R> volb = nullptr;
@@ -119,6 +127,8 @@ struct Group {
 
 template <typename R>
 class Engine final : public EngineBase {
+  static constexpr size_t kPackedStage = sizeof(VolArgs<R>) + sizeof(FaceArgs<R>) + sizeof(GradArgs<R>);
+
  public:
   Engine(const thx_config &cfg, size_t budget, int k) : cfg_(cfg), budget_(budget), k_(k) {}
 
@@ -211,6 +221,21 @@ class Engine final : public EngineBase {
     if ((st = alloc(h, &ec->u, n)) || (st = alloc(h, &h->y, n)) ||
         (h->mixed && (st = alloc(h, &h->yf, n))))
       return fail(st);
+    ec->dt = c->dt;
+    ec->packed.resize(3 * kPackedStage);
+    for (int stage = 1; stage <= 3; ++stage) {
+      VolArgs<R> va;
+      FaceArgs<R> fa;
+      GradArgs<R> ga;
+      const R *in;
+      if constexpr (IsF32<R>::value) in = h->yf;
+      else in = stage == 1 ? ec->u : h->y;
+      op_args<R>(h, in, nullptr, stage, ec->dt, ec->u, h->y, h->yf, ga, fa, va);
+      unsigned char *pk = ec->packed.data() + (size_t)(stage - 1) * kPackedStage;
+      std::memcpy(pk, &va, sizeof(va));
+      std::memcpy(pk + sizeof(va), &fa, sizeof(fa));
+      std::memcpy(pk + sizeof(va) + sizeof(fa), &ga, sizeof(ga));
+    }
     const double t2 = now();
     if (ring_.copy(ec->u, u0, n * sizeof(double), setup_) != THX_OK ||
         (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
@@ -239,7 +264,6 @@ class Engine final : public EngineBase {
       return st;
     }
     ec->id = next_id_++;
-    ec->dt = c->dt;
     ec->steps_left = c->nsteps;
     ec->bytes = bytes;
     G->cases.push_back(ec.get());
@@ -415,7 +439,9 @@ class Engine final : public EngineBase {
       return THX_ERR_CUDA;
     }
     if (cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&G->staged, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->staged[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->staged[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->staged[2], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&G->t0) != cudaSuccess || cudaEventCreate(&G->t1) != cudaSuccess ||
         cudaEventCreateWithFlags(&G->ring[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&G->ring[1], cudaEventDisableTiming) != cudaSuccess) {
@@ -440,8 +466,10 @@ class Engine final : public EngineBase {
     cudaFree(G.dwv);
     cudaFree(G.dwf);
     cudaFree(G.dcount);
-    if (G.staging) cudaFreeHost(G.staging);
-    if (G.staged) cudaEventDestroy(G.staged);
+    for (int i = 0; i < Group<R>::kStaging; ++i) {
+      if (G.staging[i]) cudaFreeHost(G.staging[i]);
+      if (G.staged[i]) cudaEventDestroy(G.staged[i]);
+    }
     if (G.t0) cudaEventDestroy(G.t0);
     if (G.t1) cudaEventDestroy(G.t1);
     for (cudaEvent_t ev : G.ring)
@@ -486,32 +514,35 @@ class Engine final : public EngineBase {
     const size_t bg = sizeof(GradArgs<R>) * 3 * nc;
     const size_t bw = sizeof(BatchWork) * (size_t)(nwv + nwf);
     const size_t need = bv + bf + bg + bw + 2 * sizeof(int) + 64;
-    THX_CU(cudaEventSynchronize(G.staged));  // staging free again
-    if (need > G.staging_bytes) {
-      if (G.staging) cudaFreeHost(G.staging);
-      G.staging = nullptr;
-      G.staging_bytes = std::max(need, 2 * G.staging_bytes);
-      const cudaError_t e = cudaHostAlloc((void **)&G.staging, G.staging_bytes, cudaHostAllocDefault);
+    const int slot = G.stage_pos;
+    THX_CU(cudaEventSynchronize(G.staged[slot]));  // this slot's last copies are done
+    if (need > G.staging_bytes[slot]) {
+      if (G.staging[slot]) cudaFreeHost(G.staging[slot]);
+      G.staging[slot] = nullptr;
+      G.staging_bytes[slot] = std::max(need, 2 * G.staging_bytes[slot]);
+      const cudaError_t e =
+          cudaHostAlloc((void **)&G.staging[slot], G.staging_bytes[slot], cudaHostAllocDefault);
       if (e != cudaSuccess) {
-        G.staging_bytes = 0;
+        G.staging_bytes[slot] = 0;
         return cuda_failed(e, "cudaHostAlloc(table staging)", THX_ERR_OUT_OF_MEMORY);
       }
     }
-    VolArgs<R> *hv = reinterpret_cast<VolArgs<R> *>(G.staging);
-    FaceArgs<R> *hf = reinterpret_cast<FaceArgs<R> *>(G.staging + bv);
-    GradArgs<R> *hg = reinterpret_cast<GradArgs<R> *>(G.staging + bv + bf);
-    BatchWork *hw = reinterpret_cast<BatchWork *>(G.staging + bv + bf + bg);
-    int *hc = reinterpret_cast<int *>(G.staging + bv + bf + bg + bw);
+    unsigned char *stg = G.staging[slot];
+    VolArgs<R> *hv = reinterpret_cast<VolArgs<R> *>(stg);
+    FaceArgs<R> *hf = reinterpret_cast<FaceArgs<R> *>(stg + bv);
+    GradArgs<R> *hg = reinterpret_cast<GradArgs<R> *>(stg + bv + bf);
+    BatchWork *hw = reinterpret_cast<BatchWork *>(stg + bv + bf + bg);
+    int *hc = reinterpret_cast<int *>(stg + bv + bf + bg + bw);
     int wv = 0, wf = 0;
     for (int i = 0; i < nc; ++i) {
       EngineCase *c = G.cases[i];
       thx_operator_s *h = c->h;
       for (int stage = 1; stage <= 3; ++stage) {
         const int j = (stage - 1) * nc + i;
-        const R *in;
-        if constexpr (IsF32<R>::value) in = h->yf;
-        else in = stage == 1 ? c->u : h->y;
-        op_args<R>(h, in, nullptr, stage, c->dt, c->u, h->y, h->yf, hg[j], hf[j], hv[j]);
+        const unsigned char *pk = c->packed.data() + (size_t)(stage - 1) * kPackedStage;
+        std::memcpy(&hv[j], pk, sizeof(VolArgs<R>));
+        std::memcpy(&hf[j], pk + sizeof(VolArgs<R>), sizeof(FaceArgs<R>));
+        std::memcpy(&hg[j], pk + sizeof(VolArgs<R>) + sizeof(FaceArgs<R>), sizeof(GradArgs<R>));
       }
       const int nb = (h->ne + G.epb - 1) / G.epb;
       for (int b = 0; b < nb; ++b) hw[wv++] = BatchWork{i, b};
@@ -537,8 +568,9 @@ class Engine final : public EngineBase {
     if ((nwv && cudaMemcpyAsync(G.dwv, hw, sizeof(BatchWork) * nwv, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
         (nwf && cudaMemcpyAsync(G.dwf, hw + nwv, sizeof(BatchWork) * nwf, cudaMemcpyHostToDevice, G.stream) != cudaSuccess) ||
         cudaMemcpyAsync(G.dcount, hc, sizeof(int) * 2, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
-        cudaEventRecord(G.staged, G.stream) != cudaSuccess)
+        cudaEventRecord(G.staged[slot], G.stream) != cudaSuccess)
       return cuda_failed(cudaGetLastError(), "work list upload");
+    G.stage_pos = (slot + 1) % Group<R>::kStaging;
     G.nwv = nwv;
     G.nwf = nwf;
     G.dirty = false;

@@ -162,7 +162,8 @@ class BatchEngine:
         return {k: getattr(s, k) for k, _ in EngineStats._fields_}
 
 
-def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None, host=None):
+def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None, host=None,
+          admitters=1):
     """Continuous batching: requests (sorted by .arrival, seconds from start)
     are admitted as they arrive and the budget allows, advanced together, and
     fetched when done.  Returns (results, latencies, makespan): results[i] is
@@ -171,8 +172,10 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
     host seconds spent admitting, advancing/polling and fetching.
 
     Admission (building the initial state, the library's set-up of the case)
-    runs on a second host thread, in arrival order; a request that does not
-    fit waits until a result is fetched.  The calling thread keeps the GPU
+    runs on a second host thread in arrival order, first come first served: a
+    request that does not fit waits, and the ones behind it with it, until a
+    result is fetched.  admitters > 1 spreads the set-up over more threads
+    (request i on thread i mod admitters) and gives up the strict order.  The calling thread keeps the GPU
     fed: it advances the running groups and hands finished cases to two
     fetching threads."""
     import threading
@@ -190,30 +193,34 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
     import os
     pool = ThreadPoolExecutor(max_workers=max(1, min(8, (os.cpu_count() or 2) - 2)))
     depth = 64
-    futures = {}
-    submitted = [0]
+    admitters = max(1, int(admitters))
+    lock = threading.Lock()
 
-    def prefetch(upto):
-        while submitted[0] < min(upto, n):
-            j = submitted[0]
-            futures[j] = pool.submit(requests[j].state)
-            submitted[0] += 1
+    def admitter(k):
+        mine = list(range(k, n, admitters))
+        futures = {}
+        submitted = [0]
 
-    def admitter():
+        def prefetch(upto):
+            while submitted[0] < min(upto, len(mine)):
+                j = mine[submitted[0]]
+                futures[j] = pool.submit(requests[j].state)
+                submitted[0] += 1
         try:
-            for i, r in enumerate(requests):
-                prefetch(i + depth)
+            for pos, i in enumerate(mine):
+                r = requests[i]
+                prefetch(pos + depth // admitters)
                 wait = r.arrival - (clock() - t0)
                 if wait > 0:
                     time.sleep(wait)
                 ta = clock()
                 futures.pop(i).result()
                 tb = clock()
-                box["state_s"] += tb - ta
+                call = 0.0
                 while True:
                     tc = clock()
                     cid = engine.admit(r)
-                    box["call_s"] += clock() - tc
+                    call += clock() - tc
                     if cid is not None:
                         break
                     with cv:               # no room: wait for a fetch
@@ -221,7 +228,10 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
                 with cv:
                     running[cid] = i
                     box["admitted"] += 1
-                box["admit_s"] += clock() - ta
+                with lock:
+                    box["state_s"] += tb - ta
+                    box["call_s"] += call
+                    box["admit_s"] += clock() - ta
         except Exception as exc:           # surfaced by the serving thread
             box["error"] = exc
 
@@ -256,9 +266,10 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
         except Exception as exc:
             box["error"] = exc
 
-    th = threading.Thread(target=admitter, daemon=True)
+    ths = [threading.Thread(target=admitter, args=(k,), daemon=True) for k in range(admitters)]
     fetchers = [threading.Thread(target=fetcher, daemon=True) for _ in range(2)]
-    th.start()
+    for th in ths:
+        th.start()
     for f in fetchers:
         f.start()
     t_adv = 0.0
@@ -268,7 +279,8 @@ def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=
             fetch_q.put(None)
         for f in fetchers:
             f.join()
-        th.join()
+        for th in ths:
+            th.join()
         pool.shutdown(wait=True)
 
     while True:
