@@ -119,7 +119,41 @@ typedef struct {
  * Face point fp enumerates the trace nodes of both sides in the same
  * lexicographic order of the two (one) tangential reference coordinates,
  * i.e. faces are conforming and aligned.  This replaces MFEM's interior face
- * restriction (include/dgsem_cache_utilities.hpp:67-79). */
+ * restriction (include/dgsem_cache_utilities.hpp:67-79).
+ *
+ * Boundary faces (all zero/NULL for a periodic mesh), in the layout of the
+ * reference's boundary cache (include/dgsem_cache_utilities.hpp:355-440):
+ *  bdr_elem[b], bdr_lface[b]           the element and local face of boundary face b
+ *  bdr_normal[b][fp][dim]              outward CalcOrtho normal (face Jacobian scaled)
+ *  bdr_weight[b][fp]                   1/(w0*J) of the element at the trace
+ *  bdr_bc[b]                           index into bcs[] (the face's boundary marker)
+ *  bcs[i]                              condition type and offset of its payload in
+ *                                      bc_data (src/Simulation.cpp:540-860)
+ * Boundary face points use the same lexicographic face-point order.  A node's
+ * boundary-face lifts are summed in boundary-face order and added after the
+ * interior faces' (include/EulerOperator_impl.hpp:292-392). */
+
+/* Boundary condition types: the reference's BCType numbering
+ * (include/bc_cache_utilities.hpp:11-23).  Payloads in bc_data:
+ * SUPERSONIC_INFLOW / PRESCRIBED_STATE: the exterior conserved state (dim+2);
+ * NOSLIP_ADIABATIC: wall velocity (dim), wall heat flux; NOSLIP_ISOTHERMAL:
+ * wall velocity (dim), wall temperature. */
+enum {
+  THX_BC_SLIP_WALL = 0,
+  THX_BC_SUPERSONIC_INFLOW = 1,
+  THX_BC_SUPERSONIC_OUTFLOW = 2,
+  THX_BC_PRESCRIBED_STATE = 3,
+  THX_BC_SYMMETRY = 4,
+  THX_BC_AXIS = 5,               /* axisymmetric builds only: not supported */
+  THX_BC_NOSLIP_ADIABATIC = 6,
+  THX_BC_NOSLIP_ISOTHERMAL = 7
+};
+
+typedef struct {               /* BCDescriptor (include/bc_cache_utilities.hpp:36-44) */
+  int32_t type;
+  int32_t data_index;          /* offset of the payload in bc_data */
+} thx_bc;
+
 typedef struct {
   int32_t dim;               /* 2 or 3 */
   int32_t order;             /* polynomial order p (Np = p+1 nodes per direction) */
@@ -132,6 +166,17 @@ typedef struct {
   const double *face_normal;
   const double *face_wminus;
   const double *face_wplus;
+  /* boundary faces (see above) */
+  int32_t num_bdr_faces;
+  const int32_t *bdr_elem;
+  const int32_t *bdr_lface;
+  const double *bdr_normal;
+  const double *bdr_weight;
+  const int32_t *bdr_bc;
+  int32_t num_bcs;
+  const thx_bc *bcs;
+  int32_t bc_data_len;
+  const double *bc_data;
 } thx_geometry;
 
 /* LTE Helmholtz gas table in the reference's six-plane layout

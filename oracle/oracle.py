@@ -69,7 +69,7 @@ class Mesh:
     """Geometry arrays in the thx_geometry layout, kept alive for ctypes."""
 
     def __init__(self, dim, order, jac, metric, face_elem, face_lface, face_normal,
-                 face_wminus, face_wplus, coords=None, shape=None):
+                 face_wminus, face_wplus, coords=None, shape=None, boundary=None):
         self.dim, self.order = dim, order
         self.jac = np.ascontiguousarray(jac, dtype=np.float64)
         self.metric = np.ascontiguousarray(metric, dtype=np.float64)
@@ -80,6 +80,7 @@ class Mesh:
         self.face_wplus = np.ascontiguousarray(face_wplus, dtype=np.float64)
         self.coords = coords
         self.shape = shape
+        self.boundary = boundary   # theseus_b200._abi.Boundary (a plain data record) or None
         self.num_elements = self.jac.shape[0]
         self.num_faces = self.face_elem.shape[0]
         self.nd, self.nfp, self.neq = sizes(dim, order)
@@ -92,6 +93,8 @@ class Mesh:
         g.face_elem, g.face_lface = _ip(self.face_elem), _ip(self.face_lface)
         g.face_normal = _dp(self.face_normal)
         g.face_wminus, g.face_wplus = _dp(self.face_wminus), _dp(self.face_wplus)
+        if self.boundary is not None:
+            self.boundary.fill(g)
         self._g = g
         return g
 

@@ -16,6 +16,7 @@
 #include "LaxFriedrichsFlux.hpp"
 #include "LTEGasModel.hpp"
 #include "LTEECFlux.hpp"
+#include "bc_kernels.hpp"
 
 #include "theseus_b200.h"
 
@@ -63,6 +64,7 @@ struct CtxT {
   GasT gas;
   FluxT iflux;
   const double *D_d, *Dhat_d, *Dhat2_d, *subcell_weights_d;
+  const double *bc_vector_d = nullptr, *bc_scalar_d = nullptr;  // boundary payloads
   int iface_idx(int side, int fp, int eq) const {
     return (side * num_equations + eq) * num_face_points + fp;
   }
@@ -297,6 +299,31 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
           acc[q * L + (size_t)e * nd + trace_node(dim, N, lf, fp)] += rf[(s * neq + q) * nfp + fp];
     }
   for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += acc[i];
+  // boundary faces (include/EulerOperator_impl.hpp:292-392) with the
+  // reference's own boundary kernel; restr_b transpose in boundary-face order
+  if (geo->num_bdr_faces > 0) {
+    if (ns) return THX_ERR_UNSUPPORTED;
+    C bctx = ctx;
+    bctx.bc_vector_d = geo->bc_data;
+    std::vector<double> accb((size_t)neq * L, 0.0);
+    for (int b = 0; b < geo->num_bdr_faces; ++b) {
+      const thx_bc &tb = geo->bcs[geo->bdr_bc[b]];
+      Theseus::BCDescriptor bd{};
+      bd.type = tb.type;
+      bd.data_index = tb.data_index;
+      const int e = geo->bdr_elem[b], lf = geo->bdr_lface[b];
+      for (int fp = 0; fp < nfp; ++fp) {
+        const int a = trace_node(dim, N, lf, fp);
+        double state1[Theseus::MAXEQ], fluxN[Theseus::MAXEQ];
+        for (int q = 0; q < neq; ++q) state1[q] = Ue[((size_t)e * neq + q) * nd + a];
+        const double *nr = geo->bdr_normal + ((size_t)b * nfp + fp) * dim;
+        Theseus::BC::ApplyBoundaryConditionInviscid(bctx, bd, state1, nr, fluxN);
+        const double scale = -geo->bdr_weight[(size_t)b * nfp + fp];
+        for (int q = 0; q < neq; ++q) accb[q * L + (size_t)e * nd + a] += scale * fluxN[q];
+      }
+    }
+    for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += accb[i];
+  }
   return 0;
 }
 

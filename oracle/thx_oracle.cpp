@@ -1184,6 +1184,106 @@ static void gradient(const Disc &c, const double *u, double *grad, int nthreads)
 // Full RHS: include/RHSOperator_impl.hpp:719-793 with EulerOperator::FlowMult
 // (include/EulerOperator_impl.hpp:28-421) or NSOperator::FlowMult
 // (include/NSOperator_impl.hpp:161-1105).
+// ---------------------------------------------------------------------------
+// Boundary conditions.
+// Momentum component c of the wall-rotated state (include/Flow.hpp:77-150):
+// along the unit normal, then the tangent picked by the smallest normal
+// component, then normal x tangent.
+static double wall_momentum(int dim, const double *q, const double *n, double inv, int c) {
+  const double nx = n[0] * inv, ny = n[1] * inv, nz = dim > 2 ? n[2] * inv : 0.0;
+  double x = nx, y = ny, z = nz;
+  if (c > 0) {
+    double tx, ty, tz;
+    if (dim == 2) {
+      tx = -ny; ty = nx; tz = 0.0;
+    } else if (std::abs(nx) <= std::abs(ny) && std::abs(nx) <= std::abs(nz)) {
+      tx = 0.0; ty = nz; tz = -ny;
+    } else if (std::abs(ny) <= std::abs(nx) && std::abs(ny) <= std::abs(nz)) {
+      tx = -nz; ty = 0.0; tz = nx;
+    } else {
+      tx = ny; ty = -nx; tz = 0.0;
+    }
+    if (c == 1) {
+      x = tx; y = ty; z = tz;
+    } else {
+      x = ny * tz - nz * ty;
+      y = nz * tx - nx * tz;
+      z = nx * ty - ny * tx;
+    }
+  }
+  double r = 0.0;
+  r += q[1] * x;
+  r += q[2] * y;
+  if (dim == 3) r += q[3] * z;
+  return r;
+}
+
+// Slip-wall pressure p* on the face-rotated state (include/Flow.hpp:54-75,
+// 155-170).
+static double slipwall_pstar_normal(const Gas &g, const double *q, const double *n) {
+  const int dim = g.dim;
+  double mag2 = 0.0;
+  for (int d = 0; d < dim; ++d) mag2 += n[d] * n[d];
+  if (mag2 == 0.0) return 0.0;
+  const double inv = 1.0 / std::sqrt(mag2);
+  double qr[MAXEQ];
+  qr[0] = q[0];
+  for (int c = 0; c < dim; ++c) qr[1 + c] = wall_momentum(dim, q, n, inv, c);
+  qr[dim + 1] = q[dim + 1];
+  const double rho = qr[0];
+  const double c = sound_speed(g, qr);
+  const double p = pressure(g, qr);
+  const double v = qr[1] / qr[0];
+  const double gamma = g.gamma;
+  const double gammaP1 = gamma + 1.;
+  const double gammaM1 = gamma - 1.;
+  const double gammaP1Inverse = 1.0 / gammaP1;
+  const double gammaM1Inverse = 1.0 / gammaM1;
+  if (v > 0.0)
+    return (p + 0.25 * v * gammaP1 * rho *
+                    (v + std::sqrt(v * v + 8.0 * gammaP1Inverse * p * (gammaM1 * gammaP1Inverse + 1.0) / rho)));
+  return p * std::pow(std::max(1.0 + 0.5 * gammaM1 * v / c, 0.0001), 2.0 * gamma * gammaM1Inverse);
+}
+
+// Inviscid boundary flux of one boundary face point (include/bc_kernels.hpp:138-152,
+// 219-279); sf is the configured surface flux.
+static void bc_inviscid(const Gas &g, FaceFn sf, const thx_bc &bc, const double *data, const double *q,
+                        const double *n, double *F) {
+  const int dim = g.dim, neq = dim + 2;
+  switch (bc.type) {
+    case THX_BC_SLIP_WALL: {
+      const double ps = slipwall_pstar_normal(g, q, n);
+      for (int k = 0; k < neq; ++k) F[k] = 0.0;
+      for (int d = 0; d < dim; ++d) F[1 + d] = ps * n[d];
+      return;
+    }
+    case THX_BC_SUPERSONIC_OUTFLOW:
+      sf(g, q, q, n, F);
+      return;
+    case THX_BC_PRESCRIBED_STATE:
+    case THX_BC_SUPERSONIC_INFLOW:
+      sf(g, q, data + bc.data_index, n, F);
+      return;
+    case THX_BC_SYMMETRY: {
+      double qb[MAXEQ], un[MAXDIM], mom[MAXDIM];
+      for (int k = 0; k < neq; ++k) qb[k] = q[k];
+      for (int d = 0; d < dim; ++d) { un[d] = n[d]; mom[d] = q[1 + d]; }
+      double fac = 0.0;
+      for (int d = 0; d < dim; ++d) fac += (un[d] * un[d]);
+      fac = 1.0 / std::sqrt(fac);
+      for (int d = 0; d < dim; ++d) un[d] *= fac;
+      double nv = 0.0;
+      for (int d = 0; d < dim; ++d) nv += mom[d] * un[d];
+      for (int d = 0; d < dim; ++d) qb[1 + d] = -2.0 * nv * un[d] + mom[d];
+      sf(g, q, qb, n, F);
+      return;
+    }
+    default:
+      for (int k = 0; k < neq; ++k) F[k] = 0.0;
+      return;
+  }
+}
+
 static int rhs(const Disc &c, const double *u, double *dudt, int nthreads,
                double *alpha_out, double *eta_out) {
   const int dim = c.dim, N = c.Np, nd = c.nd, neq = c.neq, ne = c.ne;
@@ -1320,6 +1420,26 @@ static int rhs(const Disc &c, const double *u, double *dudt, int nthreads,
     }
   }
   for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += acc[i];
+  // boundary faces (include/EulerOperator_impl.hpp:292-392): flux per point,
+  // -w * flux scattered in boundary-face order, then added
+  const thx_geometry *g = c.geom;
+  if (g->num_bdr_faces > 0) {
+    std::vector<double> accb((size_t)neq * L, 0.0);
+    for (int b = 0; b < g->num_bdr_faces; ++b) {
+      const int e = g->bdr_elem[b], lf = g->bdr_lface[b];
+      const thx_bc &bc = g->bcs[g->bdr_bc[b]];
+      for (int fp = 0; fp < c.nfp; ++fp) {
+        const size_t nm = (size_t)e * nd + trace_node(c, lf, fp);
+        double q[MAXEQ], F[MAXEQ];
+        for (int k = 0; k < neq; ++k) q[k] = u[k * L + nm];
+        const double *nrm = g->bdr_normal + ((size_t)b * c.nfp + fp) * dim;
+        bc_inviscid(c.gas, sf, bc, g->bc_data, q, nrm, F);
+        const double scale = -g->bdr_weight[(size_t)b * c.nfp + fp];
+        for (int k = 0; k < neq; ++k) accb[k * L + nm] += scale * F[k];
+      }
+    }
+    for (size_t i = 0; i < (size_t)neq * L; ++i) dudt[i] += accb[i];
+  }
   return THX_OK;
 }
 
@@ -1416,6 +1536,7 @@ int orc_rhs(const thx_geometry *g, const thx_config *cfg, const double *u, doubl
   Disc c;
   int st = setup(c, g, cfg);
   if (st) return st;
+  if (g->num_bdr_faces > 0 && cfg->flow_model == THX_FLOW_NAVIER_STOKES) return THX_ERR_UNSUPPORTED;
   if (nthreads < 1) nthreads = 1;
   return rhs(c, u, dudt, nthreads, alpha, eta);
 }

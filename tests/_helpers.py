@@ -9,7 +9,8 @@ from theseus_b200 import cases
 def oracle_mesh(m):
     """The product mesh's arrays wrapped for the oracle (same inputs on both sides)."""
     return O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
-                  m.face_wminus, m.face_wplus, coords=m.coords, shape=m.shape)
+                  m.face_wminus, m.face_wplus, coords=m.coords, shape=m.shape,
+                  boundary=getattr(m, "boundary", None))
 
 
 def box(dim, order, n, lo=None, hi=None):
@@ -28,8 +29,16 @@ def random_geometry(m, seed=0, amp=0.05):
         amp * np.abs(m.face_normal).max() * rng.uniform(-1, 1, m.face_normal.shape)
     wm = m.face_wminus * (1.0 + amp * rng.uniform(-1, 1, m.face_wminus.shape))
     wp = m.face_wplus * (1.0 + amp * rng.uniform(-1, 1, m.face_wplus.shape))
+    bdr = getattr(m, "boundary", None)
+    if bdr is not None:
+        from theseus_b200._abi import Boundary
+        # oblique boundary normals: every branch of the wall rotation runs
+        bn = bdr.normal + amp * 4 * np.abs(bdr.normal).max() * rng.uniform(-1, 1, bdr.normal.shape)
+        bw = bdr.weight * (1.0 + amp * rng.uniform(-1, 1, bdr.weight.shape))
+        bdr = Boundary(bdr.elem, bdr.lface, bn, bw, bdr.bc,
+                       [(b.type, b.data_index) for b in bdr.bcs[:bdr.num_bcs]], bdr.bc_data[:bdr.bc_data_len])
     return T.Mesh(m.dim, m.order, jac, met, m.face_elem, m.face_lface, nrm, wm, wp,
-                  coords=m.coords, shape=m.shape)
+                  coords=m.coords, shape=m.shape, boundary=bdr)
 
 
 def smooth_state(m, seed=0, amp=0.05):

@@ -85,7 +85,7 @@ class Mesh:
     """Geometric factors in the thx_geometry layout (host numpy arrays)."""
 
     def __init__(self, dim, order, jac, metric, face_elem, face_lface, face_normal, face_wminus,
-                 face_wplus, coords=None, shape=None):
+                 face_wplus, coords=None, shape=None, boundary=None):
         self.dim, self.order = int(dim), int(order)
         self.jac = np.ascontiguousarray(jac, np.float64)
         self.metric = np.ascontiguousarray(metric, np.float64)
@@ -96,6 +96,7 @@ class Mesh:
         self.face_wplus = np.ascontiguousarray(face_wplus, np.float64)
         self.coords = coords
         self.shape = shape
+        self.boundary = boundary   # _abi.Boundary or None (periodic)
         self.num_elements = self.jac.shape[0]
         self.num_faces = self.face_elem.shape[0]
         self.nd, self.nfp, self.neq = sizes(self.dim, self.order)
@@ -117,6 +118,8 @@ class Mesh:
         g.face_normal = self.face_normal.ctypes.data_as(_D)
         g.face_wminus = self.face_wminus.ctypes.data_as(_D)
         g.face_wplus = self.face_wplus.ctypes.data_as(_D)
+        if self.boundary is not None:
+            self.boundary.fill(g)
         self._g = g
         return g
 
@@ -146,6 +149,24 @@ def periodic_box(dim, order, n, lo, hi, coords=True):
                                 wp.ctypes.data_as(_D),
                                 xyz.ctypes.data_as(_D) if coords else None), "thx_box_geometry")
     return Mesh(dim, order, jac, metric, fe, fl, fn, wm, wp, coords=xyz, shape=tuple(n[:dim]))
+
+
+def box(dim, order, n, lo, hi, periodic=None, boundary=None, coords=True):
+    """Cartesian box mesh with periodic sides or boundary conditions.
+    periodic: one flag per direction (default all periodic); boundary maps each
+    side of a non-periodic direction ("x-", "x+", "y-", "y+", "z-", "z+") to
+    a condition named as in the reference's runtime JSON ("slip",
+    "supersonic-outflow", "symmetry", ("supersonic-inflow", q),
+    ("exterior-state", q) with q the exterior conserved state,
+    ("no-slip-adiabatic", v..., heat), ("no-slip-isothermal", v..., T))."""
+    from ._abi import box_boundary
+    m = periodic_box(dim, order, n, lo, hi, coords)
+    periodic = tuple(periodic) if periodic is not None else (True,) * dim
+    if all(periodic[:dim]):
+        return m
+    faces, bdr = box_boundary(dim, n, m.face_elem, m.face_lface, m.face_normal, m.face_wminus,
+                              m.face_wplus, periodic, boundary or {})
+    return Mesh(dim, order, m.jac, m.metric, *faces, coords=m.coords, shape=m.shape, boundary=bdr)
 
 
 def lgl(np_):

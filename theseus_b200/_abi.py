@@ -33,6 +33,16 @@ class Config(C.Structure):
     ]
 
 
+class BC(C.Structure):
+    _fields_ = [("type", C.c_int32), ("data_index", C.c_int32)]
+
+
+# Boundary condition names of the reference's runtime JSON (src/Simulation.cpp:540-860)
+# and their BCType numbers (include/bc_cache_utilities.hpp:11-23).
+BC_TYPES = {"slip": 0, "supersonic-inflow": 1, "supersonic-outflow": 2, "exterior-state": 3,
+            "symmetry": 4, "axis": 5, "no-slip-adiabatic": 6, "no-slip-isothermal": 7}
+
+
 class Geometry(C.Structure):
     _fields_ = [
         ("dim", C.c_int32), ("order", C.c_int32), ("num_elements", C.c_int32),
@@ -41,7 +51,104 @@ class Geometry(C.Structure):
         ("face_elem", C.POINTER(C.c_int32)), ("face_lface", C.POINTER(C.c_int32)),
         ("face_normal", C.POINTER(C.c_double)), ("face_wminus", C.POINTER(C.c_double)),
         ("face_wplus", C.POINTER(C.c_double)),
+        ("num_bdr_faces", C.c_int32),
+        ("bdr_elem", C.POINTER(C.c_int32)), ("bdr_lface", C.POINTER(C.c_int32)),
+        ("bdr_normal", C.POINTER(C.c_double)), ("bdr_weight", C.POINTER(C.c_double)),
+        ("bdr_bc", C.POINTER(C.c_int32)),
+        ("num_bcs", C.c_int32), ("bcs", C.POINTER(BC)),
+        ("bc_data_len", C.c_int32), ("bc_data", C.POINTER(C.c_double)),
     ]
+
+
+class Boundary:
+    """Boundary faces in the thx_geometry layout: elem[b], lface[b], outward
+    normal[b][fp][dim], lift weight[b][fp], bc[b] (index into bcs), bcs as
+    (type, data_index) pairs and the packed payloads bc_data."""
+
+    def __init__(self, elem, lface, normal, weight, bc, bcs, bc_data):
+        import numpy as np
+        self.elem = np.ascontiguousarray(elem, np.int32)
+        self.lface = np.ascontiguousarray(lface, np.int32)
+        self.normal = np.ascontiguousarray(normal, np.float64)
+        self.weight = np.ascontiguousarray(weight, np.float64)
+        self.bc = np.ascontiguousarray(bc, np.int32)
+        self.bcs = (BC * max(1, len(bcs)))(*[BC(int(t), int(i)) for t, i in bcs])
+        self.num_bcs = len(bcs)
+        self.bc_data = np.ascontiguousarray(bc_data if len(bc_data) else [0.0], np.float64)
+        self.bc_data_len = len(bc_data)
+
+    @property
+    def num_faces(self):
+        return int(self.elem.shape[0])
+
+    def fill(self, g):
+        D, I = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        g.num_bdr_faces = self.num_faces
+        g.bdr_elem = self.elem.ctypes.data_as(I)
+        g.bdr_lface = self.lface.ctypes.data_as(I)
+        g.bdr_normal = self.normal.ctypes.data_as(D)
+        g.bdr_weight = self.weight.ctypes.data_as(D)
+        g.bdr_bc = self.bc.ctypes.data_as(I)
+        g.num_bcs = self.num_bcs
+        g.bcs = C.cast(self.bcs, C.POINTER(BC))
+        g.bc_data_len = self.bc_data_len
+        g.bc_data = self.bc_data.ctypes.data_as(D)
+
+
+def box_boundary(dim, n, face_elem, face_lface, face_normal, face_wminus, face_wplus, periodic,
+                 boundary):
+    """Split the wrap faces of a periodic box's non-periodic directions into
+    boundary faces.  The box numbers faces direction by direction, element by
+    element (x fastest), the face of element e in direction d joining it to
+    its +d neighbour; the wrap faces are those of the last element layer.
+    boundary maps a side ("x-", "x+", "y-", "y+", "z-", "z+") to a condition:
+    a name of BC_TYPES, or (name, payload) with the exterior conserved state
+    for "supersonic-inflow"/"exterior-state" and (velocity..., heat or
+    temperature) for the no-slip walls.  Returns the kept interior faces'
+    arrays and the Boundary; boundary faces are numbered direction by
+    direction, so that a node's boundary faces are in direction order."""
+    import numpy as np
+    nn = list(n) + [1] * (3 - len(n))
+    ne = int(np.prod(nn[:dim]))
+    e = np.arange(ne)
+    ix = [e % nn[0], (e // nn[0]) % nn[1], e // (nn[0] * nn[1])]
+    keep = np.ones(dim * ne, bool)
+    sides = {}
+    for d in range(dim):
+        if periodic[d]:
+            continue
+        for s in (f"{'xyz'[d]}-", f"{'xyz'[d]}+"):
+            if s not in boundary:
+                raise ValueError(f"side {s} is not periodic and has no boundary condition")
+        keep[d * ne:(d + 1) * ne] &= ix[d] != nn[d] - 1
+    bcs, data, side_bc = [], [], {}
+    for side in sorted(boundary, key=lambda s: ("xyz".index(s[0]), s[1] == "+")):
+        spec = boundary[side]
+        name, payload = (spec, ()) if isinstance(spec, str) else (spec[0], tuple(np.ravel(spec[1:])))
+        if name not in BC_TYPES:
+            raise ValueError(f"unknown boundary condition {name!r}")
+        side_bc[side] = len(bcs)
+        bcs.append((BC_TYPES[name], len(data)))
+        data.extend(float(x) for x in payload)
+    elem, lface, normal, weight, bci = [], [], [], [], []
+    for d in range(dim):
+        if periodic[d]:
+            continue
+        wrap = np.nonzero(ix[d] == nn[d] - 1)[0] + d * ne      # face of the last layer
+        lo_e = face_elem[wrap, 1]                               # first layer: its -d face
+        hi_e = face_elem[wrap, 0]                               # last layer: its +d face
+        for f, eb, lf, sgn, w, side in ((wrap, lo_e, 2 * d, -1.0, face_wplus, f"{'xyz'[d]}-"),
+                                        (wrap, hi_e, 2 * d + 1, 1.0, face_wminus, f"{'xyz'[d]}+")):
+            order_ = np.argsort(eb, kind="stable")
+            elem.append(eb[order_])
+            lface.append(np.full(len(f), lf, np.int32))
+            normal.append(face_normal[f[order_]] if sgn > 0 else 0.0 - face_normal[f[order_]])
+            weight.append(w[f[order_]])
+            bci.append(np.full(len(f), side_bc[side], np.int32))
+    bdr = Boundary(np.concatenate(elem), np.concatenate(lface), np.concatenate(normal),
+                   np.concatenate(weight), np.concatenate(bci), bcs, data)
+    return (face_elem[keep], face_lface[keep], face_normal[keep], face_wminus[keep],
+            face_wplus[keep]), bdr
 
 
 def flux_id(name_or_id):

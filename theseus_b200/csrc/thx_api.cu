@@ -220,6 +220,7 @@ void pick_face_kernels(thx_operator_s *h) {
   if (!h->mixed) {
     FaceKernels0 k = h->dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
     h->face64 = k.face[s][ns];
+    h->bnd64 = k.bnd[s];
   } else {
     FaceKernels1 k = h->dim == 2 ? face_kernels_1_2() : face_kernels_1_3();
     h->face32 = k.face[s][ns];
@@ -306,6 +307,24 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   h->mixed = cfg->precision == THX_PRECISION_FP32_MIXED;
   h->ns = cfg->flow_model == THX_FLOW_NAVIER_STOKES;
   h->blend = cfg->blending != 0;
+  h->nbf = g->num_bdr_faces > 0 ? g->num_bdr_faces : 0;
+  if (h->nbf > 0) {
+    // boundary faces: the inviscid conditions, FP64, ideal gas
+    if (!g->bdr_elem || !g->bdr_lface || !g->bdr_normal || !g->bdr_weight || !g->bdr_bc || !g->bcs ||
+        g->num_bcs <= 0 || g->bc_data_len < 0 || (g->bc_data_len > 0 && !g->bc_data))
+      return THX_ERR_INVALID_ARGUMENT;
+    if (h->ns || h->mixed || table) return THX_ERR_UNSUPPORTED;
+    for (int i = 0; i < g->num_bcs; ++i) {
+      const thx_bc &bc = g->bcs[i];
+      if (bc.type < THX_BC_SLIP_WALL || bc.type > THX_BC_NOSLIP_ISOTHERMAL) return THX_ERR_INVALID_ARGUMENT;
+      if (bc.type == THX_BC_AXIS) return THX_ERR_UNSUPPORTED;
+      if ((bc.type == THX_BC_PRESCRIBED_STATE || bc.type == THX_BC_SUPERSONIC_INFLOW) &&
+          (bc.data_index < 0 || bc.data_index + g->dim + 2 > g->bc_data_len))
+        return THX_ERR_INVALID_ARGUMENT;
+    }
+    for (int b = 0; b < h->nbf; ++b)
+      if (g->bdr_bc[b] < 0 || g->bdr_bc[b] >= g->num_bcs) return THX_ERR_INVALID_ARGUMENT;
+  }
   h->g64 = make_gas<double>(*cfg, g->dim);
   h->g32 = make_gas<float>(*cfg, g->dim);
   for (int k = 0; k < 5; ++k) h->off.v[k] = (k < g->dim + 2) ? cfg->state_offset[k] : 0.0;
@@ -382,7 +401,22 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
         if (e < 0 || e >= h->ne || lf < 0 || lf >= 2 * dim) return THX_ERR_INVALID_ARGUMENT;
         ef[(size_t)e * 2 * dim + lf] = 2 * f + s;
       }
+    // boundary faces take face slots nf .. nf+nbf-1 (minus side only)
+    for (int b = 0; b < h->nbf; ++b) {
+      const int e = g->bdr_elem[b], lf = g->bdr_lface[b];
+      if (e < 0 || e >= h->ne || lf < 0 || lf >= 2 * dim) return THX_ERR_INVALID_ARGUMENT;
+      ef[(size_t)e * 2 * dim + lf] = 2 * (h->nf + b);
+    }
     if ((st = upload(&h->elem_face, ef.data(), ef.size(), A))) return st;
+  }
+  if (h->nbf > 0) {
+    if ((st = upload(&h->bdr_elem, g->bdr_elem, (size_t)h->nbf, A))) return st;
+    if ((st = upload(&h->bdr_lface, g->bdr_lface, (size_t)h->nbf, A))) return st;
+    if ((st = upload(&h->bdr_bc, g->bdr_bc, (size_t)h->nbf, A))) return st;
+    if ((st = upload(&h->bdr_nrm, g->bdr_normal, (size_t)h->nbf * nfp * dim, A))) return st;
+    if ((st = upload(&h->bdr_w, g->bdr_weight, (size_t)h->nbf * nfp, A))) return st;
+    if ((st = upload(&h->bcs, g->bcs, (size_t)g->num_bcs, A))) return st;
+    if ((st = upload(&h->bc_data, g->bc_data, (size_t)std::max(1, (int)g->bc_data_len), A))) return st;
   }
   // operators
   std::vector<double> x(N), w(N), D(N * N), Dh(N * N), Dh2(N * N);
@@ -397,7 +431,7 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if ((st = upload_both(D, &h->D64, &h->D32, w32, A))) return st;
   }
   // scratch
-  const size_t fsz = (size_t)h->nf * h->neq * nfp;
+  const size_t fsz = (size_t)(h->nf + h->nbf) * h->neq * nfp;
   if (h->mixed) {
     float *p;
     if ((st = dev_alloc(&p, fsz, A))) return st;
@@ -551,6 +585,9 @@ void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double 
   va.elem_face = h->elem_face; va.fstar = fst;
   va.wm = G.wm; va.wp = G.wp; va.w_fs = h->lay.w_fs; va.w_ps = h->lay.w_ps;
   va.vflux = vfl;
+  va.nf_int = h->nf;
+  if constexpr (IsF32<R>::value) va.bw = nullptr;
+  else va.bw = h->bdr_w;
   va.alpha = h->blend ? h->alpha : nullptr;
   va.fvrate = h->blend ? reinterpret_cast<R *>(h->fvrate) : nullptr;
   for (int d = 0; d < 3; ++d) { va.sub[d] = G.sub[d]; va.sub_es[d] = h->lay.sub_es[d]; }
@@ -605,6 +642,16 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if (h->ns && gradk(h, tag)(ga, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[2], s);
   if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;
+  if constexpr (!IsF32<R>::value) {
+    if (h->nbf > 0) {
+      BndArgs ba;
+      ba.u = u; ba.ne = h->ne; ba.N = h->N; ba.nbf = h->nbf; ba.f0 = h->nf;
+      ba.bdr_elem = h->bdr_elem; ba.bdr_lface = h->bdr_lface; ba.bdr_bc = h->bdr_bc;
+      ba.normal = h->bdr_nrm; ba.bcs = h->bcs; ba.bc_data = h->bc_data;
+      ba.fstar = reinterpret_cast<double *>(h->fstar); ba.gas = h->g64;
+      if (h->bnd64(ba, s) != cudaSuccess) return THX_ERR_CUDA;
+    }
+  }
   if (ev) cudaEventRecord(ev[3], s);
   if (h->blend && fvk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (volk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
@@ -881,6 +928,7 @@ int thx_integral_measures(thx_handle h, const double *u, double *out) {
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, double *rates_out) {
   if (!h || !u || !dt_out) return THX_ERR_INVALID_ARGUMENT;
   if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
+  if (h->nbf > 0) return THX_ERR_UNSUPPORTED;  // the boundary-face rate term is not built
   DeviceGuard dg(h->device);
   if (!dg.ok) return THX_ERR_CUDA;
   StabArgs a;

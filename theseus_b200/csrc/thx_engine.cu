@@ -182,6 +182,7 @@ class Engine final : public EngineBase {
                                             !g->face_wminus || !g->face_wplus)))
       return THX_ERR_INVALID_ARGUMENT;
     if (g->order + 1 < 3 || g->order + 1 > 6) return THX_ERR_UNSUPPORTED;
+    if (g->num_bdr_faces > 0) return THX_ERR_UNSUPPORTED;  // batched kernels: periodic meshes
     const size_t bytes = case_bytes(g, &cfg_, c->flow_model);
     const double t0 = now();
     {

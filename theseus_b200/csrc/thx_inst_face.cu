@@ -26,6 +26,16 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
   THX_SET(SURF_LLF)
   THX_SET(SURF_ROE)
 #undef THX_SET
+#if THX_PREC == 0
+  k.bnd[SURF_CHANDRASHEKAR] = &launch_bnd<THX_DIM, SURF_CHANDRASHEKAR>;
+  k.bnd[SURF_RANOCHA] = &launch_bnd<THX_DIM, SURF_RANOCHA>;
+  k.bnd[SURF_PIROZZOLI] = &launch_bnd<THX_DIM, SURF_PIROZZOLI>;
+  k.bnd[SURF_HLL] = &launch_bnd<THX_DIM, SURF_HLL>;
+  k.bnd[SURF_LLF] = &launch_bnd<THX_DIM, SURF_LLF>;
+  k.bnd[SURF_ROE] = &launch_bnd<THX_DIM, SURF_ROE>;
+#else
+  for (auto &b : k.bnd) b = nullptr;
+#endif
   return k;
 }
 

@@ -125,6 +125,8 @@ struct VolArgs {
   const R *fstar;         // [f][eq][fp]
   const R *wm, *wp;       // lift weights
   long long w_fs, w_ps;
+  int nf_int;             // faces at or past nf_int are boundary faces
+  const R *bw;            // boundary lift weights [b][fp], face slot nf_int + b
   const R *vflux;         // NS physical viscous flux [dir][eq-1][elem][node]
   const double *alpha;    // per-element blending coefficient or nullptr
   const R *sub[3];        // subcell metrics (reference layout), element stride sub_es
@@ -389,12 +391,13 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   }
 
   if (!active) return;
-  // surface lift: faces summed first, then added (restr_f transpose; +=)
+  // surface lift: interior faces summed first, then added (restr_f
+  // transpose; +=); then the boundary faces the same way (restr_b)
   {
-    R acc[NEQ];
+    R acc[NEQ], accb[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) acc[k] = R(0);
-    bool any = false;
+    for (int k = 0; k < NEQ; ++k) acc[k] = accb[k] = R(0);
+    bool any = false, anyb = false;
 #pragma unroll
     for (int dir = 0; dir < DIM; ++dir) {
       const int me = c[dir];
@@ -404,6 +407,13 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
       if (fs < 0) continue;
       const int f = fs >> 1, side = fs & 1;
       const int fp = face_point<DIM, N>(dir, c);
+      if (a.bw && f >= a.nf_int) {
+        const R w = -a.bw[(long long)(f - a.nf_int) * S::NFP + fp];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) accb[k] += w * a.fstar[((long long)f * NEQ + k) * S::NFP + fp];
+        anyb = true;
+        continue;
+      }
       const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
       const R w = side == 0 ? -a.wm[wi] : a.wp[wi];
 #pragma unroll
@@ -413,6 +423,10 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     if (any) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) du[k] += acc[k];
+    }
+    if (anyb) {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) du[k] += accb[k];
     }
   }
   const long long base = (long long)e * ND + n;

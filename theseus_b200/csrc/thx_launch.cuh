@@ -2,6 +2,7 @@
 // the per-(precision, dimension, order) instantiation units.
 #pragma once
 #include "thx_kernels.cuh"
+#include "thx_bc.cuh"
 
 #include <algorithm>
 
@@ -119,6 +120,17 @@ cudaError_t launch_face_batched(const FaceArgs<R> *args, const BatchWork *work, 
   return cudaGetLastError();
 }
 
+using BndLaunch = cudaError_t (*)(const BndArgs &, cudaStream_t);
+
+template <int DIM, int SURF>
+cudaError_t launch_bnd(const BndArgs &a, cudaStream_t s) {
+  const int nfp = DIM == 2 ? a.N : a.N * a.N;
+  const long long total = (long long)a.nbf * nfp;
+  if (total <= 0) return cudaSuccess;
+  bnd_face_kernel<DIM, SURF><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename R, int DIM, int N>
 cudaError_t launch_fv(const VolArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
@@ -153,6 +165,7 @@ template <typename R>
 struct FaceKernelsT {
   FaceLaunch<R> face[6][2];      // [surface flux][ns]
   FaceBatchLaunch<R> faceb[6][2];
+  BndLaunch bnd[6];              // boundary faces [surface flux] (FP64)
 };
 using OrderKernels0 = OrderKernelsT<double>;
 using OrderKernels1 = OrderKernelsT<float>;

@@ -79,6 +79,7 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
     return THX_ERR_INVALID_ARGUMENT;
   if (g->dim < 2 || g->dim > 3 || g->num_elements <= 0 || g->num_faces <= 0)
     return THX_ERR_INVALID_ARGUMENT;
+  if (g->num_bdr_faces > 0) return THX_ERR_UNSUPPORTED;  // periodic meshes only
   if (cfg->flow_model != THX_FLOW_EULER || cfg->precision != THX_PRECISION_FP64 || cfg->blending)
     return THX_ERR_UNSUPPORTED;
   if (cfg->volume_flux < 0 || cfg->volume_flux >= THX_FLUX_LTEEC || cfg->surface_flux < 0 ||
@@ -162,6 +163,7 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   va.met = g->metric; va.met_es = (long long)nd * dim * dim; va.met_ns = dim * dim;
   va.elem_face = elem_face; va.fstar = fstar;
   va.wm = g->face_wminus; va.wp = g->face_wplus; va.w_fs = nfp; va.w_ps = 1;
+  va.nf_int = nf; va.bw = nullptr;  // periodic: every face is interior
   va.vflux = nullptr; va.alpha = nullptr;
   va.fv_flux = cfg->fv_flux; va.gas = gas; va.ops = ops;
   va.stage = 0; va.status = status;

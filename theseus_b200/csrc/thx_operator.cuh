@@ -121,6 +121,11 @@ struct thx_operator_s {
   void *fstar = nullptr, *vflux = nullptr;  // face fluxes; NS physical viscous flux
   double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
   void *fvrate = nullptr;  // subcell FV rate of blended elements (blending only)
+  // boundary faces: face slots nf .. nf+nbf-1 of fstar/elem_face
+  int nbf = 0;
+  int *bdr_elem = nullptr, *bdr_lface = nullptr, *bdr_bc = nullptr;
+  double *bdr_nrm = nullptr, *bdr_w = nullptr, *bc_data = nullptr;
+  thx_bc *bcs = nullptr;
   unsigned *status = nullptr;
   unsigned long long *stab = nullptr;
   double *y = nullptr;
@@ -131,6 +136,7 @@ struct thx_operator_s {
   thx::BlendLaunch<double> blend64 = nullptr;
   thx::VolLaunch<double> fv64 = nullptr;
   thx::FaceLaunch<double> face64 = nullptr;
+  thx::BndLaunch bnd64 = nullptr;   // boundary faces (FP64 Euler)
   thx::VolLaunch<float> vol32 = nullptr;
   thx::GradLaunch<float> grad32 = nullptr;
   thx::BlendLaunch<float> blend32 = nullptr;
