@@ -208,6 +208,36 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
                   rf[(size_t)c * 2 * neq * nfp + (s * neq + q) * nfp + fp];
       }
     for (size_t i = 0; i < gradE.size(); ++i) gradE[i] += acc[i];
+    // boundary faces: the reference's boundary point kernel per face point,
+    // restr_b transpose in boundary-face order, then added
+    if (geo->num_bdr_faces > 0) {
+      C bctx = ctx;
+      bctx.bc_vector_d = geo->bc_data;
+      std::vector<double> accb((size_t)dim * neq * L, 0.0);
+      std::vector<double> uf((size_t)neq * nfp), rb((size_t)3 * neq * nfp);
+      for (int b = 0; b < geo->num_bdr_faces; ++b) {
+        const thx_bc &tb = geo->bcs[geo->bdr_bc[b]];
+        Theseus::BCDescriptor bd{};
+        bd.type = tb.type;
+        bd.data_index = tb.data_index;
+        const int e = geo->bdr_elem[b], lf = geo->bdr_lface[b];
+        for (int fp = 0; fp < nfp; ++fp)
+          for (int q = 0; q < neq; ++q)
+            uf[q * nfp + fp] = Se[((size_t)e * neq + q) * nd + trace_node(dim, N, lf, fp)];
+        std::fill(rb.begin(), rb.end(), 0.0);
+        double *rp[3] = {rb.data(), rb.data() + neq * nfp, rb.data() + 2 * neq * nfp};
+        for (int fp = 0; fp < nfp; ++fp)
+          Theseus::DGSEMIntegrator::AssembleGradBoundaryPointKernel(
+              bctx, bd, uf.data(), geo->bdr_normal + ((size_t)b * nfp + fp) * dim,
+              geo->bdr_weight[(size_t)b * nfp + fp], fp, rp);
+        for (int c = 0; c < dim; ++c)
+          for (int fp = 0; fp < nfp; ++fp)
+            for (int q = 0; q < neq; ++q)
+              accb[(size_t)c * neq * L + ((size_t)e * neq + q) * nd + trace_node(dim, N, lf, fp)] +=
+                  rp[c][q * nfp + fp];
+      }
+      for (size_t i = 0; i < gradE.size(); ++i) gradE[i] += accb[i];
+    }
     // entropy gradient -> primitive gradient
     for (int c = 0; c < dim; ++c)
 #pragma omp parallel for schedule(static)
@@ -302,7 +332,6 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
   // boundary faces (include/EulerOperator_impl.hpp:292-392) with the
   // reference's own boundary kernel; restr_b transpose in boundary-face order
   if (geo->num_bdr_faces > 0) {
-    if (ns) return THX_ERR_UNSUPPORTED;
     C bctx = ctx;
     bctx.bc_vector_d = geo->bc_data;
     std::vector<double> accb((size_t)neq * L, 0.0);
@@ -317,7 +346,17 @@ int rhs_impl(const C &ctx, const C &fvctx, const thx_geometry *geo, const thx_co
         double state1[Theseus::MAXEQ], fluxN[Theseus::MAXEQ];
         for (int q = 0; q < neq; ++q) state1[q] = Ue[((size_t)e * neq + q) * nd + a];
         const double *nr = geo->bdr_normal + ((size_t)b * nfp + fp) * dim;
-        Theseus::BC::ApplyBoundaryConditionInviscid(bctx, bd, state1, nr, fluxN);
+        if (ns) {
+          double gx[Theseus::MAXEQ], gy[Theseus::MAXEQ], gz[Theseus::MAXEQ] = {0};
+          for (int q = 0; q < neq; ++q) {
+            gx[q] = gradE[((size_t)e * neq + q) * nd + a];
+            gy[q] = gradE[(size_t)neq * L + ((size_t)e * neq + q) * nd + a];
+            if (dim > 2) gz[q] = gradE[2 * (size_t)neq * L + ((size_t)e * neq + q) * nd + a];
+          }
+          Theseus::BC::ApplyViscousBoundaryCondition(bctx, bd, state1, gx, gy, gz, nr, 0.0, fluxN);
+        } else {
+          Theseus::BC::ApplyBoundaryConditionInviscid(bctx, bd, state1, nr, fluxN);
+        }
         const double scale = -geo->bdr_weight[(size_t)b * nfp + fp];
         for (int q = 0; q < neq; ++q) accb[q * L + (size_t)e * nd + a] += scale * fluxN[q];
       }

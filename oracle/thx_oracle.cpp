@@ -1093,6 +1093,43 @@ static void volume_element(const Disc &c, VolFn vf, const double *ue, const doub
 // BR1 gradient of entropy variables, then conversion to primitive gradients
 // (include/NSOperator_impl.hpp:11-159, include/DGSEMIntegrator.hpp:764-850,1011-1044).
 // grad[c][eq][e][node] (byNODES per direction).
+// Boundary jump of the entropy variables w for the BR1 lift
+// (include/bc_kernels.hpp:32-135, ComputeBdrFaceGradFlux): exterior minus
+// interior entropy state; zero for the conditions without one.
+static void bc_grad_flux(const Gas &g, const thx_bc &bc, const double *data, const double *w,
+                         double *F) {
+  const int dim = g.dim, neq = dim + 2;
+  for (int q = 0; q < neq; ++q) F[q] = 0.0;
+  switch (bc.type) {
+    case THX_BC_PRESCRIBED_STATE: {
+      double e[MAXEQ];
+      entropy_vars(g, data + bc.data_index, e);
+      for (int q = 0; q < neq; ++q) F[q] = e[q] - w[q];
+      return;
+    }
+    case THX_BC_NOSLIP_ADIABATIC: {
+      const double *vwall = data + bc.data_index;
+      const double v = -w[dim + 1];
+      F[0] = w[0];
+      for (int d = 0; d < dim; ++d) F[1 + d] = vwall[d] * v;
+      F[dim + 1] = -v;
+      for (int q = 0; q < neq; ++q) F[q] -= w[q];
+      return;
+    }
+    case THX_BC_NOSLIP_ISOTHERMAL: {
+      const double *bd = data + bc.data_index;
+      const double beta = 1.0 / (g.R * bd[dim]);   // include/EOS.hpp:41-46
+      F[0] = w[0];
+      for (int d = 0; d < dim; ++d) F[1 + d] = bd[d] * beta;
+      F[dim + 1] = -beta;
+      for (int q = 0; q < neq; ++q) F[q] -= w[q];
+      return;
+    }
+    default:
+      return;
+  }
+}
+
 static void gradient(const Disc &c, const double *u, double *grad, int nthreads) {
   const int dim = c.dim, N = c.Np, nd = c.nd, neq = c.neq, ne = c.ne;
   const size_t L = (size_t)ne * nd;
@@ -1167,6 +1204,30 @@ static void gradient(const Disc &c, const double *u, double *grad, int nthreads)
     }
     double *gc = grad + (size_t)cdir * neq * L;
     for (size_t i = 0; i < (size_t)neq * L; ++i) gc[i] += acc[i];
+  }
+  // boundary faces (include/NSOperator_impl.hpp:285-404,
+  // include/DGSEMIntegrator.hpp:1068-1094): scale * jump * n per point, in
+  // boundary-face order, then added per direction
+  const thx_geometry *gg = c.geom;
+  if (gg->num_bdr_faces > 0) {
+    for (int cdir = 0; cdir < dim; ++cdir) {
+      std::fill(acc.begin(), acc.end(), 0.0);
+      for (int b = 0; b < gg->num_bdr_faces; ++b) {
+        const int e = gg->bdr_elem[b], lf = gg->bdr_lface[b];
+        const thx_bc &bc = gg->bcs[gg->bdr_bc[b]];
+        for (int fp = 0; fp < c.nfp; ++fp) {
+          const size_t nm = (size_t)e * nd + trace_node(c, lf, fp);
+          double w[MAXEQ], fl[MAXEQ];
+          for (int q = 0; q < neq; ++q) w[q] = S[q * L + nm];
+          bc_grad_flux(c.gas, bc, gg->bc_data, w, fl);
+          const double scale = gg->bdr_weight[(size_t)b * c.nfp + fp];
+          const double nd_ = gg->bdr_normal[((size_t)b * c.nfp + fp) * dim + cdir];
+          for (int q = 0; q < neq; ++q) acc[q * L + nm] += scale * (fl[q] * nd_);
+        }
+      }
+      double *gc = grad + (size_t)cdir * neq * L;
+      for (size_t i = 0; i < (size_t)neq * L; ++i) gc[i] += acc[i];
+    }
   }
   // entropy gradient -> primitive gradient, per direction
   for (int cdir = 0; cdir < dim; ++cdir) {
@@ -1278,6 +1339,90 @@ static void bc_inviscid(const Gas &g, FaceFn sf, const thx_bc &bc, const double 
       sf(g, q, qb, n, F);
       return;
     }
+    default:
+      for (int k = 0; k < neq; ++k) F[k] = 0.0;
+      return;
+  }
+}
+
+// Normal viscous flux n . F_v from the primitive gradients
+// (include/NavierStokesFlux.hpp:296-355, Cartesian).
+static void viscous_normal_flux(const Gas &g, const double *q, const double *const dp[3],
+                                const double *n, double *flux) {
+  const int dim = g.dim, neq = dim + 2, E = dim + 1;
+  const double mu = viscosity(g, q);
+  const double kappa = conductivity(g, q);
+  const double mu_bulk = g.mu_bulk;
+  double grho[MAXDIM] = {}, gth[MAXDIM] = {}, gT[MAXDIM] = {};
+  double divergence = 0.0;
+  for (int d = 0; d < dim; ++d) {
+    grho[d] = dp[d][0];
+    gth[d] = dp[d][E];
+    divergence += dp[d][1 + d];
+  }
+  grad_temperature(g, q, grho, gth, gT);
+  for (int k = 0; k < neq; ++k) flux[k] = 0.0;
+  double energy_flux = 0.0;
+  for (int comp = 0; comp < dim; ++comp) {
+    double traction = 0.0;
+    for (int dir = 0; dir < dim; ++dir) {
+      const double stress = comp == dir ? mu * (2.0 * dp[dir][1 + comp] - mu_bulk * divergence)
+                                        : mu * (dp[dir][1 + comp] + dp[comp][1 + dir]);
+      traction += n[dir] * stress;
+    }
+    flux[1 + comp] = traction;
+    energy_flux += vel(q, comp) * traction;
+  }
+  for (int dir = 0; dir < dim; ++dir) energy_flux += n[dir] * kappa * gT[dir];
+  flux[E] = energy_flux;
+}
+
+// Viscous boundary flux of one boundary face point (include/bc_kernels.hpp:154-217,
+// 281-374): inviscid conditions as above; the exterior state minus the
+// interior viscous flux; the no-slip walls from the wall pressure p* and the
+// normal viscous flux with the wall's heat flux or temperature.
+static void bc_viscous(const Gas &g, FaceFn sf, const thx_bc &bc, const double *data, const double *q,
+                       const double *const dp[3], const double *n, double *F) {
+  const int dim = g.dim, neq = dim + 2, E = dim + 1;
+  switch (bc.type) {
+    case THX_BC_PRESCRIBED_STATE: {
+      bc_inviscid(g, sf, bc, data, q, n, F);
+      double vfl[MAXEQ][MAXDIM];
+      viscous_flux(g, q, dp, vfl);
+      for (int k = 0; k < neq; ++k)
+        for (int d = 0; d < dim; ++d) F[k] -= vfl[k][d] * n[d];
+      return;
+    }
+    case THX_BC_NOSLIP_ADIABATIC: {
+      const double *vwall = data + bc.data_index;
+      const double qwall = vwall[dim];
+      const double ps = slipwall_pstar_normal(g, q, n);
+      viscous_normal_flux(g, q, dp, n, F);
+      double mag2 = 0.0;
+      for (int d = 0; d < dim; ++d) mag2 += n[d] * n[d];
+      double ef = qwall * std::sqrt(mag2);
+      for (int d = 0; d < dim; ++d) ef += vwall[d] * F[1 + d];
+      F[E] = ef;
+      for (int k = 0; k < neq; ++k) F[k] = -F[k];
+      for (int d = 0; d < dim; ++d) F[1 + d] += ps * n[d];
+      return;
+    }
+    case THX_BC_NOSLIP_ISOTHERMAL: {
+      const double *vwall = data + bc.data_index;
+      const double ps = slipwall_pstar_normal(g, q, n);
+      viscous_normal_flux(g, q, dp, n, F);
+      for (int d = 0; d < dim; ++d) F[E] -= vel(q, d) * F[1 + d];
+      for (int d = 0; d < dim; ++d) F[E] += vwall[d] * F[1 + d];
+      for (int k = 0; k < neq; ++k) F[k] = -F[k];
+      for (int d = 0; d < dim; ++d) F[1 + d] += ps * n[d];
+      return;
+    }
+    case THX_BC_SLIP_WALL:
+    case THX_BC_SUPERSONIC_INFLOW:
+    case THX_BC_SUPERSONIC_OUTFLOW:
+    case THX_BC_SYMMETRY:
+      bc_inviscid(g, sf, bc, data, q, n, F);
+      return;
     default:
       for (int k = 0; k < neq; ++k) F[k] = 0.0;
       return;
@@ -1433,7 +1578,15 @@ static int rhs(const Disc &c, const double *u, double *dudt, int nthreads,
         double q[MAXEQ], F[MAXEQ];
         for (int k = 0; k < neq; ++k) q[k] = u[k * L + nm];
         const double *nrm = g->bdr_normal + ((size_t)b * c.nfp + fp) * dim;
-        bc_inviscid(c.gas, sf, bc, g->bc_data, q, nrm, F);
+        if (ns) {
+          double gd[3][MAXEQ] = {};
+          for (int d = 0; d < dim; ++d)
+            for (int k = 0; k < neq; ++k) gd[d][k] = grad[(size_t)d * neq * L + k * L + nm];
+          const double *dp[3] = {gd[0], gd[1], gd[2]};
+          bc_viscous(c.gas, sf, bc, g->bc_data, q, dp, nrm, F);
+        } else {
+          bc_inviscid(c.gas, sf, bc, g->bc_data, q, nrm, F);
+        }
         const double scale = -g->bdr_weight[(size_t)b * c.nfp + fp];
         for (int k = 0; k < neq; ++k) accb[k * L + nm] += scale * F[k];
       }
@@ -1536,7 +1689,6 @@ int orc_rhs(const thx_geometry *g, const thx_config *cfg, const double *u, doubl
   Disc c;
   int st = setup(c, g, cfg);
   if (st) return st;
-  if (g->num_bdr_faces > 0 && cfg->flow_model == THX_FLOW_NAVIER_STOKES) return THX_ERR_UNSUPPORTED;
   if (nthreads < 1) nthreads = 1;
   return rhs(c, u, dudt, nthreads, alpha, eta);
 }

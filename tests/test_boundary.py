@@ -21,6 +21,10 @@ Q_EXT = {2: [1.1, 0.35, -0.05, 2.7], 3: [1.1, 0.35, -0.05, 0.1, 2.75]}   # exter
 def spec(name, dim):
     if name in ("supersonic-inflow", "exterior-state"):
         return (name, *Q_EXT[dim])
+    if name == "no-slip-adiabatic":          # wall velocity, wall heat flux
+        return (name, *([0.2, -0.1, 0.05][:dim]), 0.03)
+    if name == "no-slip-isothermal":         # wall velocity, wall temperature
+        return (name, *([0.2, -0.1, 0.05][:dim]), 0.004)
     return name
 
 
@@ -80,6 +84,39 @@ def test_oracle_mixed_boundaries_match_reference(surf):
     m = bmesh(2, 4, (3, 4), sides, seed=7)
     u = smooth_state(m, seed=3)
     cfg = T.make_config(flow="euler", volume_flux="ranocha", surface_flux=surf)
+    om = oracle_mesh(m)
+    assert np.array_equal(O.rhs(om, cfg, u), O.ref_rhs(om, cfg, u))
+
+
+NS_CONDITIONS = ["no-slip-adiabatic", "no-slip-isothermal", "exterior-state", "slip", "symmetry",
+                 "supersonic-outflow"]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+@pytest.mark.parametrize("dim,order,n", [(2, 3, (4, 3)), (3, 2, (3, 2, 3))])
+@pytest.mark.parametrize("name", NS_CONDITIONS)
+def test_oracle_ns_boundary_matches_reference(dim, order, n, name):
+    """Gradient jump (BR1 lift) and viscous boundary flux of each condition."""
+    sides = {"x-": spec(name, dim), "x+": spec(name, dim)}
+    if dim == 3:
+        sides.update({"z-": spec(name, dim), "z+": spec(name, dim)})
+    m = bmesh(dim, order, n, sides, seed=order + 5)
+    u = smooth_state(m, seed=dim + 2)
+    cfg = T.make_config(flow="ns", volume_flux="ranocha", surface_flux="hll", mu=0.01, Pr=0.72)
+    om = oracle_mesh(m)
+    a = O.rhs(om, cfg, u)
+    b = O.ref_rhs(om, cfg, u)
+    assert np.array_equal(a, b), np.abs(a - b).max()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_oracle_ns_mixed_boundaries_match_reference():
+    sides = {"x-": spec("exterior-state", 2), "x+": "supersonic-outflow",
+             "y-": spec("no-slip-isothermal", 2), "y+": spec("no-slip-adiabatic", 2)}
+    m = bmesh(2, 4, (3, 4), sides, seed=9)
+    u = smooth_state(m, seed=4)
+    cfg = T.make_config(flow="ns", volume_flux="chandrashekar", surface_flux="roe", mu=0.02,
+                        Pr=0.71)
     om = oracle_mesh(m)
     assert np.array_equal(O.rhs(om, cfg, u), O.ref_rhs(om, cfg, u))
 
