@@ -169,9 +169,48 @@ def test_gpu_mixed_boundaries_and_blending(cuda, surf):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dim,order,n", [(2, 4, (4, 3)), (3, 3, (3, 2, 2))])
+@pytest.mark.parametrize("name", NS_CONDITIONS)
+def test_gpu_ns_boundary_conditions(cuda, dim, order, n, name):
+    """BR1 boundary jump in the gradient kernel, primitive gradients at the
+    boundary points, viscous boundary flux in the boundary kernel."""
+    import torch
+    sides = {"x-": spec(name, dim), "x+": spec(name, dim), "y-": spec(name, dim), "y+": spec(name, dim)}
+    m = bmesh(dim, order, n, sides, seed=order + 2 * dim)
+    u = smooth_state(m, seed=5)
+    op = T.NSOperator(m, numerical_flux="ranocha", surface_flux="hll", mu=0.01, Pr=0.72)
+    ud = torch.as_tensor(u, device="cuda")
+    du = torch.empty_like(ud)
+    op.Mult(ud, du)
+    cfg = T.make_config(flow="ns", volume_flux="ranocha", surface_flux="hll", mu=0.01, Pr=0.72)
+    ref = O.rhs(oracle_mesh(m), cfg, u)
+    assert rel_l2(du.cpu().numpy(), ref).max() <= TOL
+
+
+@pytest.mark.gpu
+def test_gpu_ns_mixed_walls_sutherland(cuda):
+    import torch
+    sides = {"x-": spec("exterior-state", 2), "x+": "supersonic-outflow",
+             "y-": spec("no-slip-isothermal", 2), "y+": spec("no-slip-adiabatic", 2)}
+    m = bmesh(2, 5, (3, 4), sides, seed=13)
+    u = smooth_state(m, seed=6)
+    kw = dict(mu=0.02, Pr=0.71, sutherland=True)
+    op = T.NSOperator(m, numerical_flux="chandrashekar", surface_flux="roe", **kw)
+    ud = torch.as_tensor(u, device="cuda")
+    du = torch.empty_like(ud)
+    op.Mult(ud, du)
+    cfg = T.make_config(flow="ns", volume_flux="chandrashekar", surface_flux="roe", **kw)
+    ref = O.rhs(oracle_mesh(m), cfg, u)
+    assert rel_l2(du.cpu().numpy(), ref).max() <= TOL
+
+
+@pytest.mark.gpu
 def test_gpu_boundaries_unsupported_forms_are_refused(cuda):
     m = bmesh(2, 3, (3, 3), {"x-": "slip", "x+": "slip"})
     with pytest.raises(T.THXError, match="unsupported"):
-        T.NSOperator(m, numerical_flux="chandrashekar", surface_flux="roe")
-    with pytest.raises(T.THXError, match="unsupported"):
         T.EulerOperator(m, numerical_flux="chandrashekar", surface_flux="roe", precision="fp32")
+    op = T.EulerOperator(m, numerical_flux="chandrashekar", surface_flux="roe")
+    import torch
+    u = torch.as_tensor(smooth_state(m, seed=0), device="cuda")
+    with pytest.raises(T.THXError, match="unsupported"):
+        op.estimate_dt(u, 0.5)

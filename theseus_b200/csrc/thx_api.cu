@@ -220,7 +220,7 @@ void pick_face_kernels(thx_operator_s *h) {
   if (!h->mixed) {
     FaceKernels0 k = h->dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
     h->face64 = k.face[s][ns];
-    h->bnd64 = k.bnd[s];
+    h->bnd64 = k.bnd[s][ns];
   } else {
     FaceKernels1 k = h->dim == 2 ? face_kernels_1_2() : face_kernels_1_3();
     h->face32 = k.face[s][ns];
@@ -309,11 +309,11 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   h->blend = cfg->blending != 0;
   h->nbf = g->num_bdr_faces > 0 ? g->num_bdr_faces : 0;
   if (h->nbf > 0) {
-    // boundary faces: the inviscid conditions, FP64, ideal gas
+    // boundary faces: FP64, ideal gas
     if (!g->bdr_elem || !g->bdr_lface || !g->bdr_normal || !g->bdr_weight || !g->bdr_bc || !g->bcs ||
         g->num_bcs <= 0 || g->bc_data_len < 0 || (g->bc_data_len > 0 && !g->bc_data))
       return THX_ERR_INVALID_ARGUMENT;
-    if (h->ns || h->mixed || table) return THX_ERR_UNSUPPORTED;
+    if (h->mixed || table) return THX_ERR_UNSUPPORTED;
     for (int i = 0; i < g->num_bcs; ++i) {
       const thx_bc &bc = g->bcs[i];
       if (bc.type < THX_BC_SLIP_WALL || bc.type > THX_BC_NOSLIP_ISOTHERMAL) return THX_ERR_INVALID_ARGUMENT;
@@ -417,6 +417,7 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if ((st = upload(&h->bdr_w, g->bdr_weight, (size_t)h->nbf * nfp, A))) return st;
     if ((st = upload(&h->bcs, g->bcs, (size_t)g->num_bcs, A))) return st;
     if ((st = upload(&h->bc_data, g->bc_data, (size_t)std::max(1, (int)g->bc_data_len), A))) return st;
+    if (h->ns && (st = dev_alloc(&h->bgrad, (size_t)h->nbf * nfp * dim * h->neq, A))) return st;
   }
   // operators
   std::vector<double> x(N), w(N), D(N * N), Dh(N * N), Dh2(N * N);
@@ -573,6 +574,14 @@ void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double 
   ga.normal = G.nrm; ga.n_fs = h->lay.n_fs; ga.n_ps = h->lay.n_ps;
   ga.wm = G.wm; ga.wp = G.wp; ga.w_fs = h->lay.w_fs; ga.w_ps = h->lay.w_ps;
   ga.D = G.D; ga.gas = g; ga.status = h->status;
+  ga.nf_int = h->nf;
+  if constexpr (IsF32<R>::value) {
+    ga.bw = nullptr;
+  } else {
+    ga.bw = h->nbf > 0 ? h->bdr_w : nullptr;
+    ga.bnrm = h->bdr_nrm; ga.bdr_bc = h->bdr_bc; ga.bcs = h->bcs; ga.bc_data = h->bc_data;
+    ga.bgrad = h->bgrad;
+  }
   fa = FaceArgs<R>{};
   fa.u = u; fa.ne = h->ne; fa.nf = h->nf; fa.N = h->N;
   fa.face_elem = h->face_elem; fa.face_lface = h->face_lface;
@@ -647,7 +656,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
       BndArgs ba;
       ba.u = u; ba.ne = h->ne; ba.N = h->N; ba.nbf = h->nbf; ba.f0 = h->nf;
       ba.bdr_elem = h->bdr_elem; ba.bdr_lface = h->bdr_lface; ba.bdr_bc = h->bdr_bc;
-      ba.normal = h->bdr_nrm; ba.bcs = h->bcs; ba.bc_data = h->bc_data;
+      ba.normal = h->bdr_nrm; ba.bcs = h->bcs; ba.bc_data = h->bc_data; ba.bgrad = h->bgrad;
       ba.fstar = reinterpret_cast<double *>(h->fstar); ba.gas = h->g64;
       if (h->bnd64(ba, s) != cudaSuccess) return THX_ERR_CUDA;
     }

@@ -20,9 +20,84 @@ struct BndArgs {
   const double *normal;    // [nbf][nfp][dim]
   const thx_bc *bcs;
   const double *bc_data;
+  const double *bgrad;     // NS: primitive gradients at the points [nbf][nfp][dim][dim+2]
   double *fstar;           // [f][eq][fp]
   GasT<double> gas;
 };
+
+// Exterior minus interior entropy variables w at a boundary point, the jump
+// of the BR1 lift (include/bc_kernels.hpp:32-135); zero for the conditions
+// without an exterior entropy state.
+template <int DIM>
+__device__ __forceinline__ void bc_grad_flux(const GasT<double> &g, const thx_bc &bc, const double *data,
+                                             const double *w, double *F) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) F[k] = 0.0;
+  if (bc.type == THX_BC_PRESCRIBED_STATE) {
+    double qb[NEQ], e[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) qb[k] = data[bc.data_index + k];
+    entropy_vars<double, DIM>(g, qb, e);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) F[k] = e[k] - w[k];
+  } else if (bc.type == THX_BC_NOSLIP_ADIABATIC) {
+    const double *vw = data + bc.data_index;
+    const double v = -w[E];
+    F[0] = w[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[1 + d] = vw[d] * v;
+    F[E] = -v;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) F[k] -= w[k];
+  } else if (bc.type == THX_BC_NOSLIP_ISOTHERMAL) {
+    const double *bd = data + bc.data_index;
+    const double beta = 1.0 / (g.R_gas * bd[DIM]);  // include/EOS.hpp:41-46
+    F[0] = w[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[1 + d] = bd[d] * beta;
+    F[E] = -beta;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) F[k] -= w[k];
+  }
+}
+
+// Normal viscous flux n . F_v from the primitive gradients dp[dir][eq]
+// (include/NavierStokesFlux.hpp:296-355, Cartesian), in its own order.
+template <int DIM>
+__device__ __forceinline__ void viscous_normal_flux(const GasT<double> &g, const double *q, const double *dp,
+                                                    const double *n, double *flux) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+  const double mu = viscosity<double, DIM>(g, q);
+  const double kappa = mu * g.cp * g.Pr_inv;
+  double divergence = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) divergence += dp[d * NEQ + 1 + d];
+  const double rho = q[0];
+  const double pressor = pressure<double, DIM>(g, q) / rho;
+  const double fac = g.gm1_inv / (g.cv * rho);
+  double gT[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) gT[d] = fac * (dp[d * NEQ + E] - pressor * dp[d * NEQ + 0]);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) flux[k] = 0.0;
+  double energy_flux = 0.0;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    double traction = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double stress = c == d ? mu * (2.0 * dp[d * NEQ + 1 + c] - g.mu_bulk * divergence)
+                                   : mu * (dp[d * NEQ + 1 + c] + dp[c * NEQ + 1 + d]);
+      traction += n[d] * stress;
+    }
+    flux[1 + c] = traction;
+    energy_flux += (q[1 + c] / q[0]) * traction;
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) energy_flux += n[d] * kappa * gT[d];
+  flux[E] = energy_flux;
+}
 
 // Momentum of the wall-rotated state, component c (include/Flow.hpp:77-150):
 // c = 0 along the unit normal, then the tangent chosen by the smallest
@@ -151,7 +226,65 @@ __device__ __forceinline__ void bc_inviscid(const GasT<double> &g, const thx_bc 
   }
 }
 
+// Viscous boundary flux (include/bc_kernels.hpp:154-217, 281-374): the
+// inviscid conditions; the exterior state minus the interior viscous flux;
+// the no-slip walls from the wall pressure p* and the normal viscous flux
+// with the wall's heat flux or temperature.
 template <int DIM, int SURF>
+__device__ __forceinline__ void bc_viscous(const GasT<double> &g, const thx_bc &bc, const double *data,
+                                           const double *q, const double *dp, const double *n, double *F) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+  switch (bc.type) {
+    case THX_BC_PRESCRIBED_STATE: {
+      bc_inviscid<DIM, SURF>(g, bc, data, q, n, F);
+      double vf[NEQ * DIM];
+      viscous_flux<double, DIM>(g, q, dp, vf);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) vf[d] = 0.0;  // mass row
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) F[k] -= vf[k * DIM + d] * n[d];
+      return;
+    }
+    case THX_BC_NOSLIP_ADIABATIC: {
+      const double *vw = data + bc.data_index;
+      const double ps = slipwall_pstar_normal<DIM>(g, q, n);
+      viscous_normal_flux<DIM>(g, q, dp, n, F);
+      double mag2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) mag2 += n[d] * n[d];
+      double ef = vw[DIM] * sqrt(mag2);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) ef += vw[d] * F[1 + d];
+      F[E] = ef;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) F[k] = -F[k];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) F[1 + d] += ps * n[d];
+      return;
+    }
+    case THX_BC_NOSLIP_ISOTHERMAL: {
+      const double *vw = data + bc.data_index;
+      const double ps = slipwall_pstar_normal<DIM>(g, q, n);
+      viscous_normal_flux<DIM>(g, q, dp, n, F);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) F[E] -= (q[1 + d] / q[0]) * F[1 + d];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) F[E] += vw[d] * F[1 + d];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) F[k] = -F[k];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) F[1 + d] += ps * n[d];
+      return;
+    }
+    default:
+      bc_inviscid<DIM, SURF>(g, bc, data, q, n, F);
+      return;
+  }
+}
+
+template <int DIM, int SURF, bool NS>
 __global__ void __launch_bounds__(128) bnd_face_kernel(const BndArgs a) {
   constexpr int NEQ = DIM + 2;
   const int N = a.N;
@@ -166,7 +299,11 @@ __global__ void __launch_bounds__(128) bnd_face_kernel(const BndArgs a) {
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + i];
   const double *n = a.normal + ((long long)b * nfp + fp) * DIM;
-  bc_inviscid<DIM, SURF>(a.gas, a.bcs[a.bdr_bc[b]], a.bc_data, q, n, F);
+  if constexpr (NS)
+    bc_viscous<DIM, SURF>(a.gas, a.bcs[a.bdr_bc[b]], a.bc_data, q,
+                          a.bgrad + ((long long)b * nfp + fp) * DIM * NEQ, n, F);
+  else
+    bc_inviscid<DIM, SURF>(a.gas, a.bcs[a.bdr_bc[b]], a.bc_data, q, n, F);
   const int f = a.f0 + b;
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) a.fstar[((long long)f * NEQ + k) * nfp + fp] = F[k];

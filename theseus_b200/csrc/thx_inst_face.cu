@@ -27,14 +27,18 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
   THX_SET(SURF_ROE)
 #undef THX_SET
 #if THX_PREC == 0
-  k.bnd[SURF_CHANDRASHEKAR] = &launch_bnd<THX_DIM, SURF_CHANDRASHEKAR>;
-  k.bnd[SURF_RANOCHA] = &launch_bnd<THX_DIM, SURF_RANOCHA>;
-  k.bnd[SURF_PIROZZOLI] = &launch_bnd<THX_DIM, SURF_PIROZZOLI>;
-  k.bnd[SURF_HLL] = &launch_bnd<THX_DIM, SURF_HLL>;
-  k.bnd[SURF_LLF] = &launch_bnd<THX_DIM, SURF_LLF>;
-  k.bnd[SURF_ROE] = &launch_bnd<THX_DIM, SURF_ROE>;
+#define THX_SETBND(S)                                   \
+  k.bnd[S][0] = &launch_bnd<THX_DIM, S, false>;          \
+  k.bnd[S][1] = &launch_bnd<THX_DIM, S, true>;
+  THX_SETBND(SURF_CHANDRASHEKAR)
+  THX_SETBND(SURF_RANOCHA)
+  THX_SETBND(SURF_PIROZZOLI)
+  THX_SETBND(SURF_HLL)
+  THX_SETBND(SURF_LLF)
+  THX_SETBND(SURF_ROE)
+#undef THX_SETBND
 #else
-  for (auto &b : k.bnd) b = nullptr;
+  for (auto &b : k.bnd) b[0] = b[1] = nullptr;
 #endif
   return k;
 }

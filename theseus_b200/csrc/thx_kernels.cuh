@@ -19,6 +19,7 @@
 //             divergence, surface lift from fs; writes dudt once.
 #pragma once
 #include "thx_device.cuh"
+#include "thx_bc.cuh"
 
 namespace thx {
 
@@ -393,11 +394,12 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   if (!active) return;
   // surface lift: interior faces summed first, then added (restr_f
   // transpose; +=); then the boundary faces the same way (restr_b)
-  {
-    R acc[NEQ], accb[NEQ];
+#pragma unroll 1
+  for (int pass = 0; pass < ((!IsF32<R>::value && a.bw) ? 2 : 1); ++pass) {
+    R acc[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) acc[k] = accb[k] = R(0);
-    bool any = false, anyb = false;
+    for (int k = 0; k < NEQ; ++k) acc[k] = R(0);
+    bool any = false;
 #pragma unroll
     for (int dir = 0; dir < DIM; ++dir) {
       const int me = c[dir];
@@ -407,15 +409,15 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
       if (fs < 0) continue;
       const int f = fs >> 1, side = fs & 1;
       const int fp = face_point<DIM, N>(dir, c);
-      if (a.bw && f >= a.nf_int) {
-        const R w = -a.bw[(long long)(f - a.nf_int) * S::NFP + fp];
-#pragma unroll
-        for (int k = 0; k < NEQ; ++k) accb[k] += w * a.fstar[((long long)f * NEQ + k) * S::NFP + fp];
-        anyb = true;
-        continue;
+      R w;
+      if (!IsF32<R>::value && a.bw && f >= a.nf_int) {  // boundary face (FP64 only)
+        if (pass == 0) continue;
+        w = -a.bw[(long long)(f - a.nf_int) * S::NFP + fp];
+      } else {
+        if (pass == 1) continue;
+        const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
+        w = side == 0 ? -a.wm[wi] : a.wp[wi];
       }
-      const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
-      const R w = side == 0 ? -a.wm[wi] : a.wp[wi];
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) acc[k] += w * a.fstar[((long long)f * NEQ + k) * S::NFP + fp];
       any = true;
@@ -423,10 +425,6 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     if (any) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) du[k] += acc[k];
-    }
-    if (anyb) {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) du[k] += accb[k];
     }
   }
   const long long base = (long long)e * ND + n;
@@ -663,6 +661,15 @@ struct GradArgs {
   const R *D;  // N*N
   GasT<R> gas;
   unsigned *status;
+  // boundary faces (FP64 ideal gas; bw == nullptr: none): face slots
+  // nf_int + b, lift weights bw[b][fp], outward normals bnrm[b][fp][dim],
+  // conditions; the primitive gradients at the boundary points go to bgrad
+  int nf_int;
+  const double *bw, *bnrm;
+  const int *bdr_bc;
+  const thx_bc *bcs;
+  const double *bc_data;
+  double *bgrad;  // [b][fp][dim][dim+2]
 };
 
 template <typename R, int DIM, int N>
@@ -714,6 +721,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
     const int fs = a.elem_face[te * NLF + lf];
     if (fs < 0) continue;
     const int f = fs >> 1, side = fs & 1;
+    if (a.bw && f >= a.nf_int) continue;  // boundary face: no neighbour
     const int eo = a.face_elem[2 * f + 1 - side];
     const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
     R ro[NEQ], qo[NEQ], so[NEQ];
@@ -775,6 +783,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
       const int fs = a.elem_face[e * 2 * DIM + lf];
       if (fs < 0) continue;
       const int f = fs >> 1, side = fs & 1;
+      if (a.bw && f >= a.nf_int) continue;  // boundary face: below
       const int fp = face_point<DIM, N>(dir, c);
       R so[NEQ];
 #pragma unroll
@@ -798,6 +807,46 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
         for (int k = 0; k < NEQ; ++k) g[cc][k] += acc[cc][k];
     }
   }
+  // boundary faces (include/NSOperator_impl.hpp:285-404,
+  // include/DGSEMIntegrator.hpp:1068-1094): w_b (exterior - interior entropy
+  // variables) n_c, the node's boundary faces summed then added
+  if constexpr (!IsF32<R>::value && !LTE) {
+    if (a.bw) {
+      R accb[DIM][NEQ];
+      bool anyb = false;
+#pragma unroll
+      for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) accb[cc][k] = R(0);
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir) {
+        const int me = c[dir];
+        if (me != 0 && me != N - 1) continue;
+        const int lf = 2 * dir + (me == N - 1 ? 1 : 0);
+        const int fs = a.elem_face[e * 2 * DIM + lf];
+        if (fs < 0 || (fs >> 1) < a.nf_int) continue;
+        const int b = (fs >> 1) - a.nf_int;
+        const long long bp = (long long)b * NFP + face_point<DIM, N>(dir, c);
+        R w[NEQ], fl[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) w[k] = sS[(el * NEQ + k) * ND + n];
+        bc_grad_flux<DIM>(a.gas, a.bcs[a.bdr_bc[b]], a.bc_data, w, fl);
+        const R scale = a.bw[bp];
+        const R *nr = a.bnrm + bp * DIM;
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k)
+#pragma unroll
+          for (int cc = 0; cc < DIM; ++cc) accb[cc][k] += scale * (fl[k] * nr[cc]);
+        anyb = true;
+      }
+      if (anyb) {
+#pragma unroll
+        for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+          for (int k = 0; k < NEQ; ++k) g[cc][k] += accb[cc][k];
+      }
+    }
+  }
   // entropy gradient -> primitive gradient, then the physical viscous flux
   // (include/NavierStokesFlux.hpp:160-290) that the face and volume kernels use
   R dp[DIM * NEQ];
@@ -818,6 +867,22 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
 #pragma unroll
     for (int k = 0; k < NV; ++k)
       a.vflux[((long long)d * NV + k) * L + (long long)e * ND + n] = vf[(1 + k) * DIM + d];
+  // primitive gradients at this node's boundary points, for the viscous
+  // boundary fluxes
+  if constexpr (!IsF32<R>::value && !LTE) {
+    if (a.bw) {
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir) {
+        const int me = c[dir];
+        if (me != 0 && me != N - 1) continue;
+        const int fs = a.elem_face[e * 2 * DIM + 2 * dir + (me == N - 1 ? 1 : 0)];
+        if (fs < 0 || (fs >> 1) < a.nf_int) continue;
+        const long long bp = (long long)((fs >> 1) - a.nf_int) * NFP + face_point<DIM, N>(dir, c);
+#pragma unroll
+        for (int i = 0; i < DIM * NEQ; ++i) a.bgrad[bp * DIM * NEQ + i] = dp[i];
+      }
+    }
+  }
 }
 
 template <typename R, int DIM, int N, bool LTE>

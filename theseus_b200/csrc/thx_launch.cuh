@@ -122,12 +122,12 @@ cudaError_t launch_face_batched(const FaceArgs<R> *args, const BatchWork *work, 
 
 using BndLaunch = cudaError_t (*)(const BndArgs &, cudaStream_t);
 
-template <int DIM, int SURF>
+template <int DIM, int SURF, bool NS>
 cudaError_t launch_bnd(const BndArgs &a, cudaStream_t s) {
   const int nfp = DIM == 2 ? a.N : a.N * a.N;
   const long long total = (long long)a.nbf * nfp;
   if (total <= 0) return cudaSuccess;
-  bnd_face_kernel<DIM, SURF><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(a);
+  bnd_face_kernel<DIM, SURF, NS><<<(unsigned)((total + 127) / 128), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -165,7 +165,7 @@ template <typename R>
 struct FaceKernelsT {
   FaceLaunch<R> face[6][2];      // [surface flux][ns]
   FaceBatchLaunch<R> faceb[6][2];
-  BndLaunch bnd[6];              // boundary faces [surface flux] (FP64)
+  BndLaunch bnd[6][2];           // boundary faces [surface flux][ns] (FP64)
 };
 using OrderKernels0 = OrderKernelsT<double>;
 using OrderKernels1 = OrderKernelsT<float>;

@@ -125,6 +125,7 @@ struct thx_operator_s {
   int nbf = 0;
   int *bdr_elem = nullptr, *bdr_lface = nullptr, *bdr_bc = nullptr;
   double *bdr_nrm = nullptr, *bdr_w = nullptr, *bc_data = nullptr;
+  double *bgrad = nullptr;   // NS: primitive gradients at the boundary points
   thx_bc *bcs = nullptr;
   unsigned *status = nullptr;
   unsigned long long *stab = nullptr;
