@@ -37,10 +37,16 @@ inline void check(int status, const char *what) {
 }
 
 // Geometric factors in the thx_geometry layout, owned on the host.
+// Boundary faces (empty: periodic) follow the reference's boundary cache:
+// element and local face, outward normals, lift weights, the condition of
+// each face and the condition table with its packed payloads.
 struct Geometry {
   int dim = 0, order = 0, num_elements = 0, num_faces = 0;
   std::vector<double> jac, metric, face_normal, face_wminus, face_wplus, coords;
   std::vector<int32_t> face_elem, face_lface;
+  std::vector<int32_t> bdr_elem, bdr_lface, bdr_bc;
+  std::vector<double> bdr_normal, bdr_weight, bc_data;
+  std::vector<thx_bc> bcs;
 
   int nodes_per_element() const { int32_t n = 0; thx_sizes(dim, order, &n, nullptr, nullptr); return n; }
   int points_per_face() const { int32_t n = 0; thx_sizes(dim, order, nullptr, &n, nullptr); return n; }
@@ -55,6 +61,13 @@ struct Geometry {
     g.face_elem = face_elem.data(); g.face_lface = face_lface.data();
     g.face_normal = face_normal.data(); g.face_wminus = face_wminus.data();
     g.face_wplus = face_wplus.data();
+    g.num_bdr_faces = (int32_t)bdr_elem.size();
+    if (g.num_bdr_faces > 0) {
+      g.bdr_elem = bdr_elem.data(); g.bdr_lface = bdr_lface.data(); g.bdr_bc = bdr_bc.data();
+      g.bdr_normal = bdr_normal.data(); g.bdr_weight = bdr_weight.data();
+      g.num_bcs = (int32_t)bcs.size(); g.bcs = bcs.data();
+      g.bc_data_len = (int32_t)bc_data.size(); g.bc_data = bc_data.data();
+    }
     return g;
   }
 

@@ -1727,7 +1727,7 @@ int orc_rk3_steps(const thx_geometry *g, const thx_config *cfg, double *u, doubl
 }
 
 // Stability estimate (include/RHSOperator_impl.hpp:10-174,
-// include/StabilityEstimate.hpp:12-92); periodic meshes have no boundary term.
+// include/StabilityEstimate.hpp:12-92), with the boundary-point term.
 int orc_estimate_dt(const thx_geometry *g, const thx_config *cfg, const double *u, double cfl,
                     double *dt, double *rates) {
   Disc c;
@@ -1792,6 +1792,47 @@ int orc_estimate_dt(const thx_geometry *g, const thx_config *cfg, const double *
       const double wmx = std::max(std::fabs(g->face_wminus[(size_t)f * c.nfp + fp]),
                                   std::fabs(g->face_wplus[(size_t)f * c.nfp + fp]));
       sur = std::max(sur, ws * wmx * surf_scale);
+    }
+  }
+  // boundary points (include/RHSOperator_impl.hpp:176-268): the interior
+  // wave speed, for an exterior state also its speed and (viscous) its
+  // effective diffusivity times the trace's metric square sum
+  for (int b = 0; b < g->num_bdr_faces; ++b) {
+    const int e = g->bdr_elem[b], lf = g->bdr_lface[b];
+    const thx_bc &bc = g->bcs[g->bdr_bc[b]];
+    for (int fp = 0; fp < c.nfp; ++fp) {
+      const size_t nm = (size_t)e * nd + trace_node(c, lf, fp);
+      double q[MAXEQ] = {0};
+      for (int k = 0; k < neq; ++k) q[k] = u[k * L + nm];
+      const double *nr = g->bdr_normal + ((size_t)b * c.nfp + fp) * dim;
+      double n2 = 0.0, vn = 0.0;
+      for (int d = 0; d < dim; ++d) { n2 += nr[d] * nr[d]; vn += vel(q, d) * nr[d]; }
+      double ws = std::fabs(vn) + sound_speed(c.gas, q) * std::sqrt(n2);
+      if (bc.type == THX_BC_PRESCRIBED_STATE || bc.type == THX_BC_SUPERSONIC_INFLOW) {
+        const double *qe = g->bc_data + bc.data_index;
+        if (visc) {
+          const double ij = 1.0 / g->jac[nm];
+          double mss = 0.0;
+          for (int rd = 0; rd < dim; ++rd) {
+            double mn2 = 0.0;
+            for (int pd = 0; pd < dim; ++pd) {
+              const double v = g->metric[(nm * dim + rd) * dim + pd];
+              mn2 += v * v;
+            }
+            mss += mn2 * ij * ij;
+          }
+          const double rho = qe[0];
+          const double mu = viscosity(c.gas, qe);
+          const double lon = (2.0 - c.gas.mu_bulk) * mu;
+          const double md = std::max(mu, lon) / rho;
+          const double td = conductivity(c.gas, qe) * c.gas.gamma / (rho * c.gas.cp);
+          dif = std::max(dif, dif_scale * std::max(md, td) * mss);
+        }
+        double ve = 0.0;
+        for (int d = 0; d < dim; ++d) ve += vel(qe, d) * nr[d];
+        ws = std::max(ws, std::fabs(ve) + sound_speed(c.gas, qe) * std::sqrt(n2));
+      }
+      sur = std::max(sur, ws * std::fabs(g->bdr_weight[(size_t)b * c.nfp + fp]) * surf_scale);
     }
   }
   if (rates) { rates[0] = adv; rates[1] = sur; rates[2] = dif; }

@@ -209,8 +209,34 @@ def test_gpu_boundaries_unsupported_forms_are_refused(cuda):
     m = bmesh(2, 3, (3, 3), {"x-": "slip", "x+": "slip"})
     with pytest.raises(T.THXError, match="unsupported"):
         T.EulerOperator(m, numerical_flux="chandrashekar", surface_flux="roe", precision="fp32")
-    op = T.EulerOperator(m, numerical_flux="chandrashekar", surface_flux="roe")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flow", ["euler", "ns"])
+def test_gpu_stability_estimate_with_boundaries(cuda, flow):
+    """The boundary-point term of the stability estimate: interior wave
+    speed, exterior state's speed and diffusivity (include/RHSOperator_impl.hpp:176-268)."""
     import torch
-    u = torch.as_tensor(smooth_state(m, seed=0), device="cuda")
-    with pytest.raises(T.THXError, match="unsupported"):
-        op.estimate_dt(u, 0.5)
+    sides = {"x-": spec("exterior-state", 2), "x+": "supersonic-outflow",
+             "y-": spec("no-slip-isothermal", 2), "y+": spec("supersonic-inflow", 2)}
+    m = bmesh(2, 3, (4, 3), sides, seed=21)
+    u = smooth_state(m, seed=8)
+    kw = dict(numerical_flux="chandrashekar", surface_flux="roe")
+    phys = dict(mu=0.05, Pr=0.72) if flow == "ns" else {}
+    op = (T.NSOperator if flow == "ns" else T.EulerOperator)(m, **kw, **phys)
+    r = op.EstimateStability(torch.as_tensor(u, device="cuda"))
+    cfg = T.make_config(flow=flow, volume_flux="chandrashekar", surface_flux="roe", **phys)
+    _, ref = O.estimate_dt(oracle_mesh(m), cfg, u, 1.0)
+    np.testing.assert_allclose(r, ref, rtol=1e-13, atol=0)
+
+
+def test_oracle_stability_boundary_term_is_active():
+    """An exterior state faster than the interior raises the surface rate."""
+    sides = {"x-": ("exterior-state", 1.0, 5.0, 0.0, 30.0), "x+": "supersonic-outflow"}
+    m = bmesh(2, 3, (4, 3), sides, perturb=False)
+    u = smooth_state(m, seed=2)
+    cfg = T.make_config(flow="euler", volume_flux="chandrashekar", surface_flux="roe")
+    _, with_b = O.estimate_dt(oracle_mesh(m), cfg, u, 1.0)
+    mp = bmesh(2, 3, (4, 3), {}, periodic=(True, True), perturb=False)
+    _, periodic = O.estimate_dt(oracle_mesh(mp), cfg, u, 1.0)
+    assert with_b[1] > periodic[1]

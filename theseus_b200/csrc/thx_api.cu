@@ -937,7 +937,6 @@ int thx_integral_measures(thx_handle h, const double *u, double *out) {
 int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, double *rates_out) {
   if (!h || !u || !dt_out) return THX_ERR_INVALID_ARGUMENT;
   if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
-  if (h->nbf > 0) return THX_ERR_UNSUPPORTED;  // the boundary-face rate term is not built
   DeviceGuard dg(h->device);
   if (!dg.ok) return THX_ERR_CUDA;
   StabArgs a;
@@ -951,8 +950,11 @@ int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, d
   a.adv_scale = h->adv_scale; a.dif_scale = h->dif_scale; a.surf_scale = h->surf_scale;
   a.viscous = h->ns ? 1 : 0;
   a.out = h->stab;
+  a.nbf = h->nbf;
+  a.bdr_elem = h->bdr_elem; a.bdr_lface = h->bdr_lface; a.bdr_bc = h->bdr_bc;
+  a.bnrm = h->bdr_nrm; a.bw = h->bdr_w; a.bcs = h->bcs; a.bc_data = h->bc_data;
   if (cudaMemset(h->stab, 0, sizeof(unsigned long long) * 3) != cudaSuccess) return THX_ERR_CUDA;
-  const long long work = h->L + (long long)h->nf * h->nfp;
+  const long long work = h->L + (long long)(h->nf + h->nbf) * h->nfp;
   const int grid = (int)std::min<long long>((work + 255) / 256, 148LL * 8);
   if (h->dim == 2) stability_kernel<2><<<grid, 256>>>(a);
   else stability_kernel<3><<<grid, 256>>>(a);

@@ -1084,6 +1084,12 @@ struct StabArgs {
   double adv_scale, dif_scale, surf_scale;
   int viscous;
   unsigned long long *out;  // [3] as ordered bit patterns of non-negative doubles
+  // boundary points
+  int nbf;
+  const int *bdr_elem, *bdr_lface, *bdr_bc;
+  const double *bnrm, *bw;
+  const thx_bc *bcs;
+  const double *bc_data;
 };
 
 template <int DIM>
@@ -1094,9 +1100,11 @@ __global__ void stability_kernel(const StabArgs a) {
   const int nfp = DIM == 2 ? N : N * N;
   const long long L = (long long)a.ne * nd;
   const long long nface_pts = (long long)a.nf * nfp;
+  const long long nbnd_pts = (long long)a.nbf * nfp;
   double adv = 0.0, dif = 0.0, sur = 0.0;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < L + nface_pts; t += stride) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < L + nface_pts + nbnd_pts;
+       t += stride) {
     if (t < L) {
       const long long e = t / nd, n = t % nd;
       double q[NEQ];
@@ -1126,6 +1134,51 @@ __global__ void stability_kernel(const StabArgs a) {
         const double td = (mu * a.gas.cp * a.gas.Pr_inv) * a.gas.gamma / (q[0] * a.gas.cp);
         dif = fmax(dif, a.dif_scale * fmax(md, td) * mss);
       }
+    } else if (t >= L + nface_pts) {
+      // boundary point (include/RHSOperator_impl.hpp:176-268)
+      const long long bpt = t - L - nface_pts;
+      const int b = (int)(bpt / nfp), fp = (int)(bpt % nfp);
+      const long long e = a.bdr_elem[b];
+      const long long node = trace_node<DIM>(N, a.bdr_lface[b], fp);
+      double q[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + e * nd + node];
+      const double *nr = a.bnrm + bpt * DIM;
+      double n2 = 0.0, vn = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        n2 += nr[d] * nr[d];
+        vn += (q[1 + d] / q[0]) * nr[d];
+      }
+      double ws = fabs(vn) + sound_speed<double, DIM>(a.gas, q) * sqrt(n2);
+      const thx_bc bc = a.bcs[a.bdr_bc[b]];
+      if (bc.type == THX_BC_PRESCRIBED_STATE || bc.type == THX_BC_SUPERSONIC_INFLOW) {
+        double qe[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) qe[k] = a.bc_data[bc.data_index + k];
+        if (a.viscous) {
+          const double ij = 1.0 / a.jac[e * a.jac_es + node * a.jac_ns];
+          const double *M = a.met + e * a.met_es + node * a.met_ns;
+          double mss = 0.0;
+#pragma unroll
+          for (int rd = 0; rd < DIM; ++rd) {
+            double mn2 = 0.0;
+#pragma unroll
+            for (int pd = 0; pd < DIM; ++pd) mn2 += M[rd * DIM + pd] * M[rd * DIM + pd];
+            mss += mn2 * ij * ij;
+          }
+          const double mu = viscosity<double, DIM>(a.gas, qe);
+          const double lon = (2.0 - a.gas.mu_bulk) * mu;
+          const double md = fmax(mu, lon) / qe[0];
+          const double td = (mu * a.gas.cp * a.gas.Pr_inv) * a.gas.gamma / (qe[0] * a.gas.cp);
+          dif = fmax(dif, a.dif_scale * fmax(md, td) * mss);
+        }
+        double ve = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ve += (qe[1 + d] / qe[0]) * nr[d];
+        ws = fmax(ws, fabs(ve) + sound_speed<double, DIM>(a.gas, qe) * sqrt(n2));
+      }
+      sur = fmax(sur, ws * fabs(a.bw[bpt]) * a.surf_scale);
     } else {
       const long long fpt = t - L;
       const int f = (int)(fpt / nfp), fp = (int)(fpt % nfp);
