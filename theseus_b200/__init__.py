@@ -56,6 +56,8 @@ def library():
         lib.thx_destroy.argtypes = [C.c_void_p]
         lib.thx_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.thx_rk3_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        lib.thx_rk3_steps_cfl.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
+                                          C.c_void_p]
         lib.thx_blending_coefficients.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.thx_estimate_dt.argtypes = [C.c_void_p, C.c_void_p, C.c_double, _D, _D]
         lib.thx_read_status.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]
@@ -326,6 +328,18 @@ class RHSOperator:
         _check(library().thx_rk3_steps(self._h, C.c_void_p(u.data_ptr()), float(dt), int(nsteps),
                                        _stream_ptr(stream)), "thx_rk3_steps")
         return u
+
+    def rk3_steps_cfl(self, u, cfl, nsteps, stream=None):
+        """nsteps SSP-RK3 steps with dt = cfl / TotalRate of each step's
+        initial state, computed on the device (no host round trip per step).
+        Returns the device tensor of the nsteps time steps taken."""
+        import torch
+        self._check_state(u, torch.float64)
+        dts = torch.zeros(max(1, int(nsteps)), dtype=torch.float64, device=u.device)
+        _check(library().thx_rk3_steps_cfl(self._h, C.c_void_p(u.data_ptr()), float(cfl), int(nsteps),
+                                           C.c_void_p(dts.data_ptr()), _stream_ptr(stream)),
+               "thx_rk3_steps_cfl")
+        return dts[:int(nsteps)]
 
     def blending_coefficients(self, stream=None):
         import torch

@@ -446,6 +446,7 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   }
   if ((st = dev_alloc(&h->status, 1, A))) return st;
   if ((st = dev_alloc(&h->stab, 3, A))) return st;
+  if ((st = dev_alloc(&h->dtd, 1, A))) return st;
   if ((st = dev_zero(h->status, sizeof(unsigned)))) return st;
   if ((st = dev_alloc(&h->alpha, h->ne, A))) return st;
   if ((st = dev_alloc(&h->eta, h->ne, A))) return st;
@@ -623,7 +624,8 @@ namespace {
 // volume+lift.  stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
 template <typename R>
 int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
-            double *um, double *y, float *yf, cudaEvent_t *ev = nullptr, double *du64 = nullptr) {
+            double *um, double *y, float *yf, cudaEvent_t *ev = nullptr, double *du64 = nullptr,
+            const double *dt_dev = nullptr) {
   R *tag = nullptr;
   if (ev) cudaEventRecord(ev[0], s);
   GradArgs<R> ga;
@@ -631,6 +633,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   VolArgs<R> va;
   op_args<R>(h, u, du, stage, dt, um, y, yf, ga, fa, va);
   va.du64 = du64;
+  va.dt_dev = dt_dev;
   if constexpr (!IsF32<R>::value) {
     if (h->lte) {
       cudaError_t te = h->dim == 2
@@ -715,6 +718,37 @@ void op_free(thx_operator_s *h) { free_all(h); }
 
 int op_to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
   return to_working_copy(h, u, s);
+}
+
+}  // namespace thx
+
+
+namespace thx {
+
+// Stability rates of state u into h->stab (ordered bit patterns of the
+// advective, surface and diffusive rates), stream-ordered
+// (include/RHSOperator_impl.hpp:10-270).
+int stability_rates(thx_operator_s *h, const double *u, cudaStream_t s) {
+  StabArgs a;
+  a.u = u; a.ne = h->ne; a.N = h->N;
+  a.jac = h->jac64; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
+  a.met = h->met64; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
+  a.face_elem = h->face_elem; a.face_lface = h->face_lface; a.nf = h->nf;
+  a.normal = h->nrm64; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
+  a.wm = h->wm64; a.wp = h->wp64; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
+  a.gas = h->g64;
+  a.adv_scale = h->adv_scale; a.dif_scale = h->dif_scale; a.surf_scale = h->surf_scale;
+  a.viscous = h->ns ? 1 : 0;
+  a.out = h->stab;
+  a.nbf = h->nbf;
+  a.bdr_elem = h->bdr_elem; a.bdr_lface = h->bdr_lface; a.bdr_bc = h->bdr_bc;
+  a.bnrm = h->bdr_nrm; a.bw = h->bdr_w; a.bcs = h->bcs; a.bc_data = h->bc_data;
+  if (cudaMemsetAsync(h->stab, 0, sizeof(unsigned long long) * 3, s) != cudaSuccess) return THX_ERR_CUDA;
+  const long long work = h->L + (long long)(h->nf + h->nbf) * h->nfp;
+  const int grid = (int)std::min<long long>((work + 255) / 256, 148LL * 8);
+  if (h->dim == 2) stability_kernel<2><<<grid, 256, 0, s>>>(a);
+  else stability_kernel<3><<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
 }
 
 }  // namespace thx
@@ -889,6 +923,37 @@ int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream) 
   return THX_OK;
 }
 
+int thx_rk3_steps_cfl(thx_handle h, double *u, double cfl, int nsteps, double *dt_history,
+                      void *stream) {
+  if (!h || !u || nsteps < 0 || !(cfl > 0.0)) return THX_ERR_INVALID_ARGUMENT;
+  if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = h->L * h->neq;
+  int st;
+  if (!h->y && (st = dev_alloc(&h->y, (size_t)n, h->allocs))) return st;
+  if (h->mixed && (st = to_working_copy(h, u, s))) return st;
+  for (int step = 0; step < nsteps; ++step) {
+    // dt from the stability rates of the step's initial state, on the device
+    if ((st = stability_rates(h, u, s))) return st;
+    cfl_dt_kernel<<<1, 1, 0, s>>>(h->stab, cfl, h->dtd, dt_history ? dt_history + step : nullptr,
+                                  h->status);
+    if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
+    if (h->mixed) {
+      for (int stage = 1; stage <= 3; ++stage)
+        if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, 0.0, u, h->y, h->yf, nullptr, nullptr,
+                                 h->dtd)))
+          return st;
+    } else {
+      if ((st = run_rhs<double>(h, u, nullptr, s, 1, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 2, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 3, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+    }
+  }
+  return THX_OK;
+}
+
 int thx_blending_coefficients(thx_handle h, double *alpha_dev, double *eta_dev, void *stream) {
   if (!h) return THX_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(h->device);
@@ -939,26 +1004,8 @@ int thx_estimate_dt(thx_handle h, const double *u, double cfl, double *dt_out, d
   if (h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
   DeviceGuard dg(h->device);
   if (!dg.ok) return THX_ERR_CUDA;
-  StabArgs a;
-  a.u = u; a.ne = h->ne; a.N = h->N;
-  a.jac = h->jac64; a.jac_es = h->lay.jac_es; a.jac_ns = h->lay.jac_ns;
-  a.met = h->met64; a.met_es = h->lay.met_es; a.met_ns = h->lay.met_ns;
-  a.face_elem = h->face_elem; a.face_lface = h->face_lface; a.nf = h->nf;
-  a.normal = h->nrm64; a.n_fs = h->lay.n_fs; a.n_ps = h->lay.n_ps;
-  a.wm = h->wm64; a.wp = h->wp64; a.w_fs = h->lay.w_fs; a.w_ps = h->lay.w_ps;
-  a.gas = h->g64;
-  a.adv_scale = h->adv_scale; a.dif_scale = h->dif_scale; a.surf_scale = h->surf_scale;
-  a.viscous = h->ns ? 1 : 0;
-  a.out = h->stab;
-  a.nbf = h->nbf;
-  a.bdr_elem = h->bdr_elem; a.bdr_lface = h->bdr_lface; a.bdr_bc = h->bdr_bc;
-  a.bnrm = h->bdr_nrm; a.bw = h->bdr_w; a.bcs = h->bcs; a.bc_data = h->bc_data;
-  if (cudaMemset(h->stab, 0, sizeof(unsigned long long) * 3) != cudaSuccess) return THX_ERR_CUDA;
-  const long long work = h->L + (long long)(h->nf + h->nbf) * h->nfp;
-  const int grid = (int)std::min<long long>((work + 255) / 256, 148LL * 8);
-  if (h->dim == 2) stability_kernel<2><<<grid, 256>>>(a);
-  else stability_kernel<3><<<grid, 256>>>(a);
-  if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
+  int st = thx::stability_rates(h, u, 0);
+  if (st) return st;
   unsigned long long r[3];
   if (cudaMemcpy(r, h->stab, sizeof(r), cudaMemcpyDeviceToHost) != cudaSuccess) return THX_ERR_CUDA;
   double rates[3];

@@ -139,6 +139,7 @@ struct VolArgs {
   // fused SSP-RK3 stage (stage==0: plain dudt)
   int stage;
   double dt;
+  const double *dt_dev;   // when set, the stage's dt is read here (device-side CFL step)
   double *um;             // FP64 master state (read every stage, written by stage 3)
   double *y;              // FP64 stage state (written by stages 1 and 2)
   float *yf;              // FP32 working copy of the next RHS input (mixed mode) or nullptr
@@ -438,7 +439,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     }
   } else {
     // fused SSP-RK3 stage in the arithmetic order of mfem::RK3SSPSolver::Step
-    const double dt = a.dt;
+    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
       const long long i = k * L + base;
@@ -1216,6 +1217,24 @@ __global__ void stability_kernel(const StabArgs a) {
   }
 }
 
+
+// dt = cfl / (max(advective, surface) + diffusive) from the stability
+// kernel's rates (src/Simulation.cpp:1150-1160), on the device, so that a
+// variable-dt time loop needs no host round trip; a non-positive total sets
+// the numerics flag and dt = 0.
+static __global__ void cfl_dt_kernel(const unsigned long long *rates, double cfl, double *dt, double *history,
+                              unsigned *status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double adv = __longlong_as_double((long long)rates[0]);
+  const double sur = __longlong_as_double((long long)rates[1]);
+  const double dif = __longlong_as_double((long long)rates[2]);
+  const double total = (adv > sur ? adv : sur) + dif;
+  double d = 0.0;
+  if (total > 0.0) d = cfl / total;
+  else atomicOr(status, STATUS_NONFINITE);
+  *dt = d;
+  if (history) *history = d;
+}
 
 // ---------------------------------------------------------------------------
 // Batched persistent forms: one launch serves every case of a batch group.

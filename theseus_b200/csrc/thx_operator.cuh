@@ -129,6 +129,7 @@ struct thx_operator_s {
   thx_bc *bcs = nullptr;
   unsigned *status = nullptr;
   unsigned long long *stab = nullptr;
+  double *dtd = nullptr;   // device-side CFL time step (thx_rk3_steps_cfl)
   double *y = nullptr;
   float *yf = nullptr;
   thx::Offsets off{};    // FP32 working-copy offsets (mixed mode)
