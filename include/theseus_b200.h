@@ -308,6 +308,60 @@ int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream);
 int thx_rk3_steps_cfl(thx_handle h, double *u, double cfl, int nsteps, double *dt_history,
                       void *stream);
 
+/* State of the reference's clocked time loop (src/Simulation.cpp:1150-1335
+ * with include/TimeStepControl.hpp and include/RunControl.hpp): the nominal
+ * step, the final time and the time-based output and checkpoint events the
+ * step is shortened to land on.  thx_time_loop_defaults fills the reference's
+ * runTime defaults. */
+typedef struct thx_time_loop {
+  double t;                 /* simulation time */
+  double dt;                /* nominal step (Simulation::dt); with cfl > 0 a value <= 0
+                               takes cfl / TotalRate of the current state first */
+  double t_final;           /* runTime.final_time */
+  double max_dt_growth;     /* runTime.max_dt_growth (1.2) */
+  double next_output;       /* next_save_t; INFINITY: no output events */
+  double output_dt;         /* runTime.initial_save_dt (0.01) */
+  double refined_output_dt; /* runTime.refined_save_dt (initial_save_dt) */
+  double refine_time;       /* runTime.refined_trigger (2.0) */
+  double next_checkpoint;   /* next_checkpoint_t; INFINITY: no checkpoint events */
+  double checkpoint_dt;     /* runTime.checkpoint_dt (0.01) */
+  double last_dt;           /* the step the last cycle took (dt_real) */
+  int64_t cycle;            /* ti */
+  int64_t max_cycles;       /* runTime.nsteps_max; <= 0: no limit */
+  int64_t output_cycles;    /* runTime.vis_steps (100) */
+  int64_t outputs;          /* output events so far */
+  int64_t checkpoints;      /* checkpoint events so far */
+  int32_t done;             /* the loop has ended; further cycles leave the state alone */
+  int32_t reserved;
+} thx_time_loop;
+
+void thx_time_loop_defaults(thx_time_loop *loop);
+/* TimeEventReached (include/TimeStepControl.hpp:21-25). */
+int thx_time_event_reached(double t, double event_time);
+/* LimitTimeStepToEvents over n event times (include/TimeStepControl.hpp:42-49). */
+double thx_limit_time_step_to_events(double step, double t, const double *events, int n);
+/* StepLimitReached (include/RunControl.hpp:11-14). */
+int thx_step_limit_reached(int64_t cycle, int64_t max_cycles);
+/* One cycle of the loop's bookkeeping on a HOST record, the code the device
+ * loop runs: begin returns the step to take (0 once done); end advances the
+ * time and cycle, updates the nominal step from total_rate when cfl > 0
+ * (total_rate = max(advective, surface) + diffusive rate of the new state),
+ * decides done and counts the output and checkpoint events. */
+double thx_time_loop_begin(thx_time_loop *loop);
+void thx_time_loop_end(thx_time_loop *loop, double dt_taken, double total_rate, double cfl);
+
+/* ncycles cycles of the reference's clocked SSP-RK3 loop on a device FP64
+ * state u, in place: each cycle takes the nominal step shortened to the next
+ * event (final time, output, checkpoint), then, with cfl > 0, sets the next
+ * nominal step to min(cfl / TotalRate, max_dt_growth * dt) from the new
+ * state's stability rates (cfl <= 0: fixed step).  loop points to a
+ * thx_time_loop in DEVICE memory, read and advanced on the device; once it is
+ * done the remaining cycles leave u unchanged.  Nothing waits for the host,
+ * so the call can be captured in a CUDA graph.  dt_history (device, may be
+ * NULL) receives each cycle's step. */
+int thx_rk3_time_loop(thx_handle h, double *u, double cfl, int ncycles, thx_time_loop *loop,
+                      double *dt_history, void *stream);
+
 /* Per-element blending coefficient alpha of the last RHS (device, double[E])
  * and the Persson smoothness eta (double[E]); either pointer may be NULL.
  * Mirrors ComputeBlendingCoefficient / CheckIndicatorSmoothness

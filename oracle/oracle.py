@@ -181,6 +181,68 @@ def estimate_dt(mesh, cfg, u, cfl):
     return dt.value, rates
 
 
+def time_event_tolerance(t):
+    """TimeEventTolerance (include/TimeStepControl.hpp:15-19)."""
+    return 16.0 * np.finfo(np.float64).eps * max(1.0, abs(t))
+
+
+def time_event_reached(t, event):
+    """TimeEventReached (include/TimeStepControl.hpp:21-25)."""
+    return t + time_event_tolerance(t) >= event
+
+
+def limit_time_step_to_events(step, t, events):
+    """LimitTimeStepToEvents / TimeToNextEvent (include/TimeStepControl.hpp:27-49)."""
+    r, tol = np.inf, time_event_tolerance(t)
+    for e in events:
+        d = e - t
+        if np.isfinite(e) and d > tol:
+            r = min(r, d)
+    return min(step, r)
+
+
+def time_loop_driver(u, step, total_rate, cfl, t_final, max_cycles, output_dt=0.01,
+                     refined_output_dt=None, refine_time=2.0, output_cycles=100, growth=1.2, dt=None):
+    """The reference's clocked time loop (src/Simulation.cpp:1150-1160 initial
+    dt = cfl / TotalRate; 1241-1304 per cycle: the nominal step shortened to
+    land on the final time and the next output time, one step, the new
+    nominal step min(cfl / TotalRate, growth * dt), done at
+    t >= t_final - 1e-8 dt or max_cycles; 1321-1331 output events advance the
+    next output time by initial_save_dt, refined_save_dt after refine_time).
+    step(u, h) advances u by h; total_rate(u) is TotalRate; cfl <= 0 keeps
+    the fixed step dt; output_dt None turns output off.  Returns (u, t,
+    [step per cycle], cycles, output events)."""
+    refined_output_dt = output_dt if refined_output_dt is None else refined_output_dt
+    t = 0.0
+    if cfl > 0 and not dt:
+        dt = cfl / total_rate(u)
+    next_out = t + output_dt if output_dt else np.inf
+    taken, cycle, outputs, done = [], 0, 0, False
+    while not done:
+        h = limit_time_step_to_events(dt, t, (t_final, next_out))
+        u = step(u, h)
+        t += h
+        cycle += 1
+        taken.append(h)
+        if cfl > 0:
+            dt = min(cfl / total_rate(u), growth * dt)
+        done = t >= t_final - 1e-8 * dt or (max_cycles > 0 and cycle >= max_cycles)
+        if np.isfinite(next_out) and (done or time_event_reached(t, next_out) or cycle % output_cycles == 0):
+            next_out += output_dt if t < refine_time else refined_output_dt
+            outputs += 1
+    return u, t, taken, cycle, outputs
+
+
+def time_loop(mesh, cfg, u, cfl, t_final, max_cycles, nthreads=1, **kw):
+    """time_loop_driver over the oracle's SSP-RK3 step and stability estimate."""
+    def total(v):
+        _, r = estimate_dt(mesh, cfg, v, 1.0)
+        return max(r[0], r[1]) + r[2]
+    u = np.array(u, dtype=np.float64, copy=True)
+    return time_loop_driver(u, lambda v, h: rk3_steps(mesh, cfg, v, h, 1, nthreads), total, cfl, t_final,
+                            max_cycles, **kw)
+
+
 def blending(mesh, cfg, u):
     u = np.ascontiguousarray(u, dtype=np.float64)
     a = np.zeros(mesh.num_elements)

@@ -341,6 +341,25 @@ class RHSOperator:
                "thx_rk3_steps_cfl")
         return dts[:int(nsteps)]
 
+    def run_time_loop(self, u, loop, ncycles, cfl=0.0, stream=None):
+        """ncycles cycles of the reference's clocked SSP-RK3 loop on u (FP64,
+        in place): `loop` is a TimeLoop (copied to the device, advanced there
+        and read back once at the end) or a device record from
+        TimeLoop.to_device (left on the device).  cfl > 0 makes the step
+        variable.  Returns the device tensor of the steps taken."""
+        import torch
+        from .timeloop import TimeLoop, _lib as _time_lib
+        self._check_state(u, torch.float64)
+        host = isinstance(loop, TimeLoop)
+        dev = loop.to_device(u.device) if host else loop
+        dts = torch.zeros(max(1, int(ncycles)), dtype=torch.float64, device=u.device)
+        _check(_time_lib().thx_rk3_time_loop(self._h, C.c_void_p(u.data_ptr()), float(cfl), int(ncycles),
+                                             C.c_void_p(dev.data_ptr()), C.c_void_p(dts.data_ptr()),
+                                             _stream_ptr(stream)), "thx_rk3_time_loop")
+        if host:
+            loop.load(dev)
+        return dts[:int(ncycles)]
+
     def blending_coefficients(self, stream=None):
         import torch
         a = torch.zeros(self.mesh.num_elements, dtype=torch.float64, device=self.device)

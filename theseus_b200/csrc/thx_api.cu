@@ -4,6 +4,7 @@
 // compute entry point returns THX_ERR_NO_DEVICE.
 #include "thx_operator.cuh"
 #include "thx_host.h"
+#include "thx_time.h"
 
 #include <algorithm>
 #include <cmath>
@@ -751,6 +752,38 @@ int stability_rates(thx_operator_s *h, const double *u, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
 }
 
+// The device side of the clocked time loop: one thread advances the
+// thx_time_loop record in device memory around each SSP-RK3 step.
+__device__ inline double total_rate_of(const unsigned long long *rates) {
+  const double adv = __longlong_as_double((long long)rates[0]);
+  const double sur = __longlong_as_double((long long)rates[1]);
+  const double dif = __longlong_as_double((long long)rates[2]);
+  return (adv > sur ? adv : sur) + dif;
+}
+
+// Initial nominal step of a variable-dt loop (src/Simulation.cpp:1150-1158).
+__global__ void time_loop_init_kernel(thx_time_loop *L, const unsigned long long *rates, double cfl,
+                                      unsigned *status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || L->done || L->dt > 0.0) return;
+  const double total = total_rate_of(rates);
+  if (total > 0.0) L->dt = cfl / total;
+  else atomicOr(status, STATUS_NONFINITE);
+}
+
+__global__ void time_loop_begin_kernel(thx_time_loop *L, double *dt, double *history) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double s = time_loop_begin(*L);
+  *dt = s;
+  if (history) *history = s;
+}
+
+__global__ void time_loop_end_kernel(thx_time_loop *L, const double *dt,
+                                     const unsigned long long *rates, double cfl, unsigned *status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double total = cfl > 0.0 ? total_rate_of(rates) : 0.0;
+  if (!time_loop_end(*L, *dt, total, cfl)) atomicOr(status, STATUS_NONFINITE);
+}
+
 }  // namespace thx
 
 extern "C" {
@@ -950,6 +983,73 @@ int thx_rk3_steps_cfl(thx_handle h, double *u, double cfl, int nsteps, double *d
       if ((st = run_rhs<double>(h, h->y, nullptr, s, 2, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
       if ((st = run_rhs<double>(h, h->y, nullptr, s, 3, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
     }
+  }
+  return THX_OK;
+}
+
+void thx_time_loop_defaults(thx_time_loop *loop) {
+  if (!loop) return;
+  std::memset(loop, 0, sizeof(*loop));
+  loop->t_final = INFINITY;
+  loop->max_dt_growth = 1.2;
+  loop->next_output = INFINITY;
+  loop->output_dt = 0.01;
+  loop->refined_output_dt = 0.01;
+  loop->refine_time = 2.0;
+  loop->next_checkpoint = INFINITY;
+  loop->checkpoint_dt = 0.01;
+  loop->max_cycles = -1;
+  loop->output_cycles = 100;
+}
+
+int thx_time_event_reached(double t, double event_time) { return thx::time_event_reached(t, event_time) ? 1 : 0; }
+
+double thx_limit_time_step_to_events(double step, double t, const double *events, int n) {
+  return thx::limit_step_to_events(step, t, events, events ? n : 0);
+}
+
+int thx_step_limit_reached(int64_t cycle, int64_t max_cycles) {
+  return thx::step_limit_reached(cycle, max_cycles) ? 1 : 0;
+}
+
+double thx_time_loop_begin(thx_time_loop *loop) { return loop ? thx::time_loop_begin(*loop) : 0.0; }
+
+void thx_time_loop_end(thx_time_loop *loop, double dt_taken, double total_rate, double cfl) {
+  if (loop) thx::time_loop_end(*loop, dt_taken, total_rate, cfl);
+}
+
+int thx_rk3_time_loop(thx_handle h, double *u, double cfl, int ncycles, thx_time_loop *loop,
+                      double *dt_history, void *stream) {
+  if (!h || !u || !loop || ncycles < 0) return THX_ERR_INVALID_ARGUMENT;
+  if (cfl > 0.0 && h->lte) return THX_ERR_UNSUPPORTED;  // ideal-gas rates only
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long n = h->L * h->neq;
+  int st;
+  if (!h->y && (st = dev_alloc(&h->y, (size_t)n, h->allocs))) return st;
+  if (h->mixed && (st = to_working_copy(h, u, s))) return st;
+  const bool variable = cfl > 0.0;
+  if (variable) {
+    if ((st = stability_rates(h, u, s))) return st;
+    time_loop_init_kernel<<<1, 1, 0, s>>>(loop, h->stab, cfl, h->status);
+  }
+  for (int c = 0; c < ncycles; ++c) {
+    time_loop_begin_kernel<<<1, 1, 0, s>>>(loop, h->dtd, dt_history ? dt_history + c : nullptr);
+    if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
+    if (h->mixed) {
+      for (int stage = 1; stage <= 3; ++stage)
+        if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, 0.0, u, h->y, h->yf, nullptr, nullptr,
+                                 h->dtd)))
+          return st;
+    } else {
+      if ((st = run_rhs<double>(h, u, nullptr, s, 1, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 2, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+      if ((st = run_rhs<double>(h, h->y, nullptr, s, 3, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
+    }
+    if (variable && (st = stability_rates(h, u, s))) return st;
+    time_loop_end_kernel<<<1, 1, 0, s>>>(loop, h->dtd, h->stab, cfl, h->status);
+    if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
   }
   return THX_OK;
 }

@@ -455,7 +455,10 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
       } else {
         y = a.y[i] + dt * kk;
         y = (1.0 / 3.0) * a.um[i] + (2.0 / 3.0) * y;
-        a.um[i] = y;
+        // a device-side step of 0 (a finished time loop, or no valid rate)
+        // leaves the state exactly as it was
+        if (a.dt_dev && dt == 0.0) y = a.um[i];
+        else a.um[i] = y;
       }
       if (a.yf) a.yf[i] = (float)(y - a.off[k]);
     }

@@ -82,8 +82,6 @@ def quad_mesh(path, order, boundary=None, coords=True):
 
 def quad_mesh_from(parsed, order, boundary=None, coords=True):
     """quad_mesh from read_gmsh's (nodes, quads, lines, periodic)."""
-    from . import Mesh, lgl, sizes
-    from ._abi import BC_TYPES, Boundary
     nodes, quads, lines, periodic = parsed
 
     def canon(v):
@@ -93,14 +91,30 @@ def quad_mesh_from(parsed, order, boundary=None, coords=True):
             v = periodic[v]
         return v
 
+    corners = np.array([[nodes[v] for v in vs] for _, *vs in quads], dtype=np.float64).reshape(-1, 4, 2)
+    vids = np.array([vs for _, *vs in quads], np.int64).reshape(-1, 4)
+    blines = {(min(p, q), max(p, q)): name for name, p, q in lines}
+    return quad_cells_mesh(corners, vids, order, blines, boundary, coords, canon)
+
+
+def quad_cells_mesh(corners, vids, order, blines=None, boundary=None, coords=True, canon=None):
+    """Geometry of straight-sided quadrilaterals: corners[e] are element e's
+    four vertex positions in cyclic order, vids[e] their vertex ids (shared
+    ids make a face interior; canon maps an id to its periodic
+    representative), blines maps a sorted vertex-id pair of a boundary edge to
+    the name of its condition in `boundary`."""
+    from . import Mesh, lgl, sizes
+    from ._abi import BC_TYPES, Boundary
+    canon = canon or (lambda v: v)
+    blines = blines or {}
     N = order + 1
     x, w = lgl(N)
-    ne = len(quads)
+    ne = len(corners)
     nd, nfp, _ = sizes(2, order)
     V = np.zeros((ne, 4, 2))
     vid = np.zeros((ne, 4), np.int64)
-    for e, (_, *vs) in enumerate(quads):
-        P = np.array([nodes[v] for v in vs])
+    for e in range(ne):
+        P, vs = corners[e], vids[e]
         # orient along the axes: v0 lower-left, v1 lower-right, v2 upper-right, v3 upper-left
         c = P.mean(axis=0)
         ang = np.arctan2(P[:, 1] - c[1], P[:, 0] - c[0])
@@ -128,9 +142,6 @@ def quad_mesh_from(parsed, order, boundary=None, coords=True):
         for lf, (p, q) in fv.items():
             k = (min(canon(vid[e, p]), canon(vid[e, q])), max(canon(vid[e, p]), canon(vid[e, q])))
             key.setdefault(k, []).append((e, lf))
-    bline = {}
-    for name, p, q in lines:
-        bline[(min(p, q), max(p, q))] = name
     faces, bfaces = [], []
     for k, users in key.items():
         if len(users) == 2:
@@ -144,7 +155,7 @@ def quad_mesh_from(parsed, order, boundary=None, coords=True):
             e, lf = users[0]
             p, q = fv[lf]
             raw = (min(vid[e, p], vid[e, q]), max(vid[e, p], vid[e, q]))
-            bfaces.append((lf // 2, e, lf, bline.get(raw, "")))
+            bfaces.append((lf // 2, e, lf, blines.get(raw, "")))
         else:
             raise ValueError("non-manifold face")
     faces.sort()
