@@ -73,16 +73,62 @@ def read_gmsh(path):
     return nodes, quads, lines, periodic
 
 
-def quad_mesh(path, order, boundary=None, coords=True):
-    """Geometry of a Gmsh quadrilateral mesh at polynomial order `order`.
+def quad_mesh(path, order, boundary=None, coords=True, refinements=0):
+    """Geometry of a Gmsh quadrilateral mesh at polynomial order `order`,
+    after `refinements` uniform refinements (the reference's ser_ref_levels).
     boundary maps a physical line name to a condition (as in box()); lines
     identified by $Periodic are periodic.  Returns a theseus_b200.Mesh."""
-    return quad_mesh_from(read_gmsh(path), order, boundary, coords)
+    return quad_mesh_from(read_gmsh(path), order, boundary, coords, refinements)
 
 
-def quad_mesh_from(parsed, order, boundary=None, coords=True):
+def refine(nodes, quads, lines):
+    """One uniform refinement of a first-order quadrilateral mesh without
+    high-order nodes, as mfem::Mesh::UniformRefinement makes it: new vertices
+    are averages of the old ones (mfem::Mesh::AverageVertices: the sum in
+    the listed order, times 1/n), an edge's midpoint from its two ends, an
+    element's centre from its four vertices in the element's order; each
+    quadrilateral splits into four, each boundary line into two."""
+    nodes = dict(nodes)
+    nxt = max(nodes) + 1
+    mids = {}
+
+    def average(vs):
+        n = len(vs)
+        x, y = nodes[vs[0]]
+        for v in vs[1:]:
+            x, y = x + nodes[v][0], y + nodes[v][1]
+        return (x * (1.0 / n), y * (1.0 / n))
+
+    def mid(a, b):
+        nonlocal nxt
+        k = (min(a, b), max(a, b))
+        if k not in mids:
+            nodes[nxt] = average([a, b])
+            mids[k] = nxt
+            nxt += 1
+        return mids[k]
+
+    out = []
+    for tag, v0, v1, v2, v3 in quads:
+        c = nxt
+        nodes[c] = average([v0, v1, v2, v3])
+        nxt += 1
+        m01, m12, m23, m30 = mid(v0, v1), mid(v1, v2), mid(v2, v3), mid(v3, v0)
+        out += [(tag, v0, m01, c, m30), (tag, m01, v1, m12, c), (tag, c, m12, v2, m23), (tag, m30, c, m23, v3)]
+    new_lines = []
+    for name, a, b in lines:
+        m = mids[(min(a, b), max(a, b))]
+        new_lines += [(name, a, m), (name, m, b)]
+    return nodes, out, new_lines
+
+
+def quad_mesh_from(parsed, order, boundary=None, coords=True, refinements=0):
     """quad_mesh from read_gmsh's (nodes, quads, lines, periodic)."""
     nodes, quads, lines, periodic = parsed
+    if refinements and periodic:
+        raise NotImplementedError("refinement of periodic Gmsh meshes")
+    for _ in range(refinements):
+        nodes, quads, lines = refine(nodes, quads, lines)
 
     def canon(v):
         seen = set()
