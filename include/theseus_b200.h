@@ -350,6 +350,36 @@ int thx_step_limit_reached(int64_t cycle, int64_t max_cycles);
 double thx_time_loop_begin(thx_time_loop *loop);
 void thx_time_loop_end(thx_time_loop *loop, double dt_taken, double total_rate, double cfl);
 
+/* Face table of conforming straight-sided cells (host; the face maps of
+ * include/dgsem_cache_utilities.hpp:516-639 for meshes whose cells are
+ * oriented along the mesh axes).  vertex_ids: int64[ne][2^dim], each cell's
+ * vertex ids in lexicographic order of its reference coordinates (x fastest);
+ * shared ids make a face interior (give periodic partners one id).  An
+ * interior face's minus side is the cell whose + face it is; faces are
+ * ordered by (direction, minus cell), boundary faces by (direction, cell,
+ * local face).  Capacities: face arrays ne*dim entries (pairs), boundary
+ * arrays 2*dim*ne; any output pointer may be NULL to count only.
+ * THX_ERR_INVALID_ARGUMENT for faces that are not aligned or shared by more
+ * than two cells. */
+int thx_cell_faces(int dim, int ne, const int64_t *vertex_ids, int32_t *face_elem, int32_t *face_lface,
+                   int32_t *num_faces, int32_t *bdr_elem, int32_t *bdr_lface, int32_t *num_bdr_faces);
+/* Geometric factors of straight-sided (bi/trilinear) cells computed on the
+ * DEVICE (replaces SetupGeometricTerms / AssembleElementVolumeGeometricTerms /
+ * AssembleInteriorFaceGeometryTerms, include/dgsem_cache_utilities.hpp:83-215,
+ * 470-639): per LGL node the Jacobian determinant and the adjugate rows,
+ * per face point the minus cell's outward face-Jacobian-scaled normal and
+ * the lift weights 1/(w0 J) of both sides, per boundary face point the
+ * normal and weight; optionally the node coordinates [dim][ne][nodes].
+ * Every pointer is DEVICE memory: corners double[ne][2^dim][dim]
+ * (lexicographic vertices), the face tables of thx_cell_faces, the outputs in
+ * the thx_geometry layout.  Allocates nothing and waits for nothing
+ * (stream-ordered). */
+int thx_cell_geometry(int dim, int order, int ne, const double *corners, int nf, const int32_t *face_elem,
+                      const int32_t *face_lface, int nbf, const int32_t *bdr_elem, const int32_t *bdr_lface,
+                      double *jac, double *metric, double *face_normal, double *face_wminus,
+                      double *face_wplus, double *bdr_normal, double *bdr_weight, double *node_coords,
+                      void *stream);
+
 /* ncycles cycles of the reference's clocked SSP-RK3 loop on a device FP64
  * state u, in place: each cycle takes the nominal step shortened to the next
  * event (final time, output, checkpoint), then, with cfl > 0, sets the next

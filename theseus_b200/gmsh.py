@@ -73,12 +73,12 @@ def read_gmsh(path):
     return nodes, quads, lines, periodic
 
 
-def quad_mesh(path, order, boundary=None, coords=True, refinements=0):
+def quad_mesh(path, order, boundary=None, coords=True, refinements=0, device=None):
     """Geometry of a Gmsh quadrilateral mesh at polynomial order `order`,
     after `refinements` uniform refinements (the reference's ser_ref_levels).
     boundary maps a physical line name to a condition (as in box()); lines
     identified by $Periodic are periodic.  Returns a theseus_b200.Mesh."""
-    return quad_mesh_from(read_gmsh(path), order, boundary, coords, refinements)
+    return quad_mesh_from(read_gmsh(path), order, boundary, coords, refinements, device)
 
 
 def refine(nodes, quads, lines):
@@ -122,7 +122,7 @@ def refine(nodes, quads, lines):
     return nodes, out, new_lines
 
 
-def quad_mesh_from(parsed, order, boundary=None, coords=True, refinements=0):
+def quad_mesh_from(parsed, order, boundary=None, coords=True, refinements=0, device=None):
     """quad_mesh from read_gmsh's (nodes, quads, lines, periodic)."""
     nodes, quads, lines, periodic = parsed
     if refinements and periodic:
@@ -140,15 +140,17 @@ def quad_mesh_from(parsed, order, boundary=None, coords=True, refinements=0):
     corners = np.array([[nodes[v] for v in vs] for _, *vs in quads], dtype=np.float64).reshape(-1, 4, 2)
     vids = np.array([vs for _, *vs in quads], np.int64).reshape(-1, 4)
     blines = {(min(p, q), max(p, q)): name for name, p, q in lines}
-    return quad_cells_mesh(corners, vids, order, blines, boundary, coords, canon)
+    return quad_cells_mesh(corners, vids, order, blines, boundary, coords, canon, device)
 
 
-def quad_cells_mesh(corners, vids, order, blines=None, boundary=None, coords=True, canon=None):
+def quad_cells_mesh(corners, vids, order, blines=None, boundary=None, coords=True, canon=None, device=None):
     """Geometry of straight-sided quadrilaterals: corners[e] are element e's
     four vertex positions in cyclic order, vids[e] their vertex ids (shared
     ids make a face interior; canon maps an id to its periodic
     representative), blines maps a sorted vertex-id pair of a boundary edge to
-    the name of its condition in `boundary`."""
+    the name of its condition in `boundary`.  With `device` (a CUDA device)
+    the face table comes from the library and the geometric factors are
+    computed on that GPU (theseus_b200.cells); the result is the same."""
     from . import Mesh, lgl, sizes
     from ._abi import BC_TYPES, Boundary
     canon = canon or (lambda v: v)
@@ -169,6 +171,12 @@ def quad_cells_mesh(corners, vids, order, blines=None, boundary=None, coords=Tru
         order_ = np.roll(order_, -k0)
         V[e] = P[order_]
         vid[e] = [vs[j] for j in order_]
+    if device is not None:
+        from .cells import cell_mesh
+        lex = [0, 1, 3, 2]                           # cyclic (ll, lr, ur, ul) -> lexicographic
+        ids = np.array([[canon(int(v)) for v in row] for row in vid[:, lex]], np.int64)
+        bfaces = {tuple(sorted((canon(int(p)), canon(int(q))))): n for (p, q), n in blines.items()}
+        return cell_mesh(2, order, V[:, lex], ids, bfaces, boundary, coords, device)
     # bilinear map at the LGL nodes (node = i + N j, i along x)
     xi, eta = np.meshgrid(x, x, indexing="xy")       # [j][i]
     xi, eta = xi.ravel(), eta.ravel()

@@ -129,14 +129,15 @@ def refine(elems, bdr, nv, dofs):
     return new_e, new_b, nv, np.array(new_d)
 
 
-def mfem_quad_mesh(path, order, refinements=0, boundary=None, coords=True):
+def mfem_quad_mesh(path, order, refinements=0, boundary=None, coords=True, device=None):
     """Geometry of an MFEM quadrilateral mesh after `refinements` uniform
     refinements (the reference's ser_ref_levels), at polynomial order
-    `order`.  boundary maps a boundary attribute to a condition (as in box())."""
-    return mfem_quad_mesh_from(read_mfem_mesh(path), order, refinements, boundary, coords)
+    `order`.  boundary maps a boundary attribute to a condition (as in box());
+    `device` computes the geometric factors on that GPU."""
+    return mfem_quad_mesh_from(read_mfem_mesh(path), order, refinements, boundary, coords, device)
 
 
-def mfem_quad_mesh_from(parsed, order, refinements=0, boundary=None, coords=True):
+def mfem_quad_mesh_from(parsed, order, refinements=0, boundary=None, coords=True, device=None):
     """mfem_quad_mesh from read_mfem_mesh's result."""
     _, elems, bdr, nv, dofs = parsed
     for _ in range(refinements):
@@ -146,4 +147,4 @@ def mfem_quad_mesh_from(parsed, order, refinements=0, boundary=None, coords=True
     blines = {(min(a, b), max(a, b)): str(attr) for attr, _, a, b in bdr}
     if boundary is not None:
         boundary = {str(k): v for k, v in boundary.items()}
-    return quad_cells_mesh(corners, vids, order, blines, boundary, coords)
+    return quad_cells_mesh(corners, vids, order, blines, boundary, coords, device=device)
