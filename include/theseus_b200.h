@@ -354,7 +354,9 @@ void thx_time_loop_end(thx_time_loop *loop, double dt_taken, double total_rate, 
  * include/dgsem_cache_utilities.hpp:516-639 for meshes whose cells are
  * oriented along the mesh axes).  vertex_ids: int64[ne][2^dim], each cell's
  * vertex ids in lexicographic order of its reference coordinates (x fastest);
- * shared ids make a face interior (give periodic partners one id).  An
+ * shared ids make a face interior (give periodic partners one id; faces are
+ * told apart by their vertex ids, so a periodic direction needs at least
+ * three cells).  An
  * interior face's minus side is the cell whose + face it is; faces are
  * ordered by (direction, minus cell), boundary faces by (direction, cell,
  * local face).  Capacities: face arrays ne*dim entries (pairs), boundary

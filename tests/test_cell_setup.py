@@ -78,10 +78,13 @@ def test_face_table_rejects_misaligned_and_nonmanifold_cells():
     three = np.concatenate([ids, ids[:1]])
     with pytest.raises(T.THXError):
         cell_faces(2, three)
+    _, two = box_cells(3, (3, 3, 2), [0.0] * 3, [1.0] * 3)   # two cells across a periodic direction
+    with pytest.raises(T.THXError):
+        cell_faces(3, two)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dim,n", [(2, (4, 3)), (3, (3, 4, 2))])
+@pytest.mark.parametrize("dim,n", [(2, (4, 3)), (3, (3, 4, 3))])
 def test_device_geometry_of_a_box(cuda, dim, n):
     lo, hi = [-1.0, 0.0, 0.5][:dim], [1.0, 3.0, 2.0][:dim]
     ref = T.periodic_box(dim, 3, n, lo, hi)
