@@ -250,20 +250,18 @@ def run_ours(args):
     nodes = m.num_nodes
     value = world * nodes * args.steps / (ms * 1e-3)
 
-    # end to end through the C ABI with host buffers (pinned), copies timed
-    hu = torch.as_tensor(u).to(op.dtype).pin_memory()
-    hdu = torch.empty_like(hu).pin_memory()
-    for _ in range(2):
-        ud.copy_(hu, non_blocking=True)
-        op.Mult(ud, du)
-        hdu.copy_(du, non_blocking=True)
+    # end to end through the C ABI with host buffers (thx_rhs_host: each
+    # step's FP64 state copied in from pinned host memory and its rate copied
+    # back, the copies of neighbouring steps overlapping the kernels), timed
+    # on the device from before the first copy-in to after the last copy-out
+    hu = [torch.as_tensor(u, dtype=torch.float64).pin_memory() for _ in range(2)]
+    hdu = [torch.empty_like(hu[0]).pin_memory() for _ in range(2)]
+    op.mult_host([hu[i % 2] for i in range(3)], [hdu[i % 2] for i in range(3)])
+    torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        ud.copy_(hu, non_blocking=True)
-        op.Mult(ud, du)
-        hdu.copy_(du, non_blocking=True)
+    op.mult_host([hu[i % 2] for i in range(args.steps)], [hdu[i % 2] for i in range(args.steps)])
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -272,8 +270,8 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e = {"value": world * nodes * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
-           "h2d_bytes_per_step": hu.numel() * hu.element_size(),
-           "d2h_bytes_per_step": hdu.numel() * hdu.element_size()}
+           "h2d_bytes_per_step": hu[0].numel() * hu[0].element_size(),
+           "d2h_bytes_per_step": hdu[0].numel() * hdu[0].element_size(), "overlap": "copy-in/compute/copy-out"}
 
     # per-kernel device times for the roofline (after the timed region)
     ud.copy_(torch.as_tensor(u).to(op.dtype))

@@ -294,6 +294,16 @@ int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream);
 int thx_rhs_euler_noalloc(const thx_geometry *geom_dev, const thx_config *cfg,
                           const double *u, double *dudt, void *stream);
 
+/* Right-hand sides of n states held in HOST memory: dudt_host[i] = L(u_host[i])
+ * (FP64 L-vectors; in FP32-mixed mode each state is evaluated as thx_rhs does).
+ * The library copies state i+1 in and rate i-1 out while it evaluates state
+ * i (two device buffers, a copy-in and a copy-out stream); with page-locked
+ * host buffers the transfers in both directions overlap the kernels.  The
+ * calls are stream-ordered on `stream`: work queued there before the call
+ * runs first, and work queued after it waits for the last copy-out.  Host
+ * buffers must stay valid until then. */
+int thx_rhs_host(thx_handle h, int n, const double *const *u_host, double *const *dudt_host, void *stream);
+
 /* nsteps SSP-RK3 steps (Shu-Osher form, as mfem::RK3SSPSolver::Step driven at
  * src/Simulation.cpp:1255) on a device FP64 state u, in place, with fixed dt.
  * In FP32-mixed mode the FP64 master state is accumulated in double and each

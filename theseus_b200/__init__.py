@@ -341,6 +341,27 @@ class RHSOperator:
                "thx_rk3_steps_cfl")
         return dts[:int(nsteps)]
 
+    def mult_host(self, states, rates, stream=None):
+        """rates[i] = L(states[i]) for FP64 host tensors (thx_rhs_host): the
+        transfers of neighbouring states overlap the evaluation when the host
+        tensors are pinned.  Stream-ordered: synchronise before reading rates."""
+        import torch
+        n = len(states)
+        if len(rates) != n:
+            raise ValueError("states and rates differ in length")
+        size = self.mesh.neq * self.mesh.num_nodes
+        for t in list(states) + list(rates):
+            if t.device.type != "cpu" or t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != size:
+                raise ValueError("host states and rates must be contiguous float64 CPU tensors of the mesh's size")
+        ins = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in states])
+        outs = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in rates])
+        lib = library()
+        if not getattr(lib, "_rhs_host_bound", False):
+            lib.thx_rhs_host.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+            lib._rhs_host_bound = True
+        _check(lib.thx_rhs_host(self._h, n, ins, outs, _stream_ptr(stream)), "thx_rhs_host")
+        return rates
+
     def run_time_loop(self, u, loop, ncycles, cfl=0.0, stream=None):
         """ncycles cycles of the reference's clocked SSP-RK3 loop on u (FP64,
         in place): `loop` is a TimeLoop (copied to the device, advanced there

@@ -229,6 +229,12 @@ void pick_face_kernels(thx_operator_s *h) {
 }
 
 void free_all(thx_operator_s *h) {
+  if (h->hp_in) cudaStreamSynchronize(h->hp_in);
+  if (h->hp_out) cudaStreamSynchronize(h->hp_out);
+  for (cudaEvent_t &e : h->hp_ev)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
+  if (h->hp_in) { cudaStreamDestroy(h->hp_in); h->hp_in = nullptr; }
+  if (h->hp_out) { cudaStreamDestroy(h->hp_out); h->hp_out = nullptr; }
   for (void *p : h->allocs) {
     if (h->pool) cudaFreeAsync(p, h->setup_stream);
     else cudaFree(p);
@@ -932,6 +938,51 @@ int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (h->mixed) return rhs_mixed(h, (const double *)u, (double *)dudt, s, nullptr);
   return run_rhs<double>(h, (const double *)u, (double *)dudt, s, 0, 0.0, nullptr, nullptr, nullptr);
+}
+
+int thx_rhs_host(thx_handle h, int n, const double *const *u_host, double *const *dudt_host, void *stream) {
+  if (!h || n < 0 || (n > 0 && (!u_host || !dudt_host))) return THX_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < n; ++i)
+    if (!u_host[i] || !dudt_host[i]) return THX_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  if (!dg.ok) return THX_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t count = (size_t)h->L * h->neq, bytes = sizeof(double) * count;
+  int st;
+  for (int b = 0; b < 2; ++b) {
+    if (!h->hp_u[b] && (st = dev_alloc(&h->hp_u[b], count, h->allocs))) return st;
+    if (!h->hp_du[b] && (st = dev_alloc(&h->hp_du[b], count, h->allocs))) return st;
+  }
+  if (!h->hp_in) {
+    THX_CU(cudaStreamCreateWithFlags(&h->hp_in, cudaStreamNonBlocking));
+    THX_CU(cudaStreamCreateWithFlags(&h->hp_out, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : h->hp_ev) THX_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  cudaEvent_t start = h->hp_ev[0], *in = h->hp_ev + 1, *done = h->hp_ev + 3, *out = h->hp_ev + 5;
+  // nothing starts before the work already queued on the caller's stream
+  THX_CU(cudaEventRecord(start, s));
+  THX_CU(cudaStreamWaitEvent(h->hp_in, start, 0));
+  THX_CU(cudaStreamWaitEvent(h->hp_out, start, 0));
+  for (int i = 0; i < n; ++i) {
+    const int b = i & 1;
+    // copy in once the right-hand side two states back has read this buffer
+    if (i >= 2) THX_CU(cudaStreamWaitEvent(h->hp_in, done[b], 0));
+    THX_CU(cudaMemcpyAsync(h->hp_u[b], u_host[i], bytes, cudaMemcpyHostToDevice, h->hp_in));
+    THX_CU(cudaEventRecord(in[b], h->hp_in));
+    THX_CU(cudaStreamWaitEvent(s, in[b], 0));
+    // overwrite the rate buffer once its previous copy-out is done
+    if (i >= 2) THX_CU(cudaStreamWaitEvent(s, out[b], 0));
+    if ((st = h->mixed ? rhs_mixed(h, h->hp_u[b], h->hp_du[b], s, nullptr)
+                       : run_rhs<double>(h, h->hp_u[b], h->hp_du[b], s, 0, 0.0, nullptr, nullptr, nullptr)))
+      return st;
+    THX_CU(cudaEventRecord(done[b], s));
+    THX_CU(cudaStreamWaitEvent(h->hp_out, done[b], 0));
+    THX_CU(cudaMemcpyAsync(dudt_host[i], h->hp_du[b], bytes, cudaMemcpyDeviceToHost, h->hp_out));
+    THX_CU(cudaEventRecord(out[b], h->hp_out));
+  }
+  // the caller's stream resumes after the last copy-out
+  for (int b = 0; b < 2 && b < n; ++b) THX_CU(cudaStreamWaitEvent(s, out[(n - 1 - b) & 1], 0));
+  return THX_OK;
 }
 
 int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream) {

@@ -156,6 +156,11 @@ struct thx_operator_s {
   cudaMemPool_t pool = nullptr;
   cudaStream_t setup_stream = nullptr;
   thx::HostRing *ring = nullptr;  // pinned staging of uploads (may be null)
+  // host-buffer pipeline (thx_rhs_host): two device state/rate buffers, a
+  // copy-in and a copy-out stream and their events
+  double *hp_u[2] = {nullptr, nullptr}, *hp_du[2] = {nullptr, nullptr};
+  cudaStream_t hp_in = nullptr, hp_out = nullptr;
+  cudaEvent_t hp_ev[7] = {};  // start, in[2], rhs[2], out[2]
   std::string desc;
 };
 
