@@ -147,6 +147,20 @@ class RHSOperator {
   void RK3Steps(double *u_dev, double dt, int nsteps, void *stream = nullptr) const {
     check(thx_rk3_steps(h_.get(), u_dev, dt, nsteps, stream), "thx_rk3_steps");
   }
+  // ncycles of the reference's clocked loop (src/Simulation.cpp:1150-1335) on
+  // the FP64 state; loop_dev is a thx_time_loop in device memory (fill it
+  // on the host with TimeLoopDefaults and copy it over); cfl > 0: variable dt.
+  void RunTimeLoop(double *u_dev, double cfl, int ncycles, thx_time_loop *loop_dev,
+                   double *dt_history_dev = nullptr, void *stream = nullptr) const {
+    check(thx_rk3_time_loop(h_.get(), u_dev, cfl, ncycles, loop_dev, dt_history_dev, stream),
+          "thx_rk3_time_loop");
+  }
+  // dudt_host[i] = L(u_host[i]) for FP64 host L-vectors; the transfers of
+  // neighbouring states overlap the kernels (page-locked buffers).  Ordered on
+  // `stream`: synchronise it before reading the rates.
+  void MultHost(int n, const double *const *u_host, double *const *dudt_host, void *stream = nullptr) const {
+    check(thx_rhs_host(h_.get(), n, u_host, dudt_host, stream), "thx_rhs_host");
+  }
   StabilityEstimate EstimateStability(const double *u_dev) const {
     double dt = 0.0, r[3] = {0, 0, 0};
     check(thx_estimate_dt(h_.get(), u_dev, 1.0, &dt, r), "thx_estimate_dt");
@@ -181,6 +195,22 @@ class RHSOperator {
   long long height_;
   std::unique_ptr<thx_operator_s, Deleter> h_;
 };
+
+// The reference's runTime defaults for the time loop, with the given final
+// time, fixed or first step (<= 0 with cfl > 0: from the stability
+// estimate), cycle limit (<= 0: none) and output interval (<= 0: no output).
+inline thx_time_loop TimeLoopDefaults(double t_final, double dt, long long max_cycles, double output_dt) {
+  thx_time_loop L;
+  thx_time_loop_defaults(&L);
+  L.t_final = t_final;
+  L.dt = dt;
+  L.max_cycles = max_cycles;
+  if (output_dt > 0.0) {
+    L.output_dt = L.refined_output_dt = output_dt;
+    L.next_output = L.t + output_dt;
+  }
+  return L;
+}
 
 // Default physics (the reference's runtime JSON defaults).
 inline thx_config DefaultPhysics() {

@@ -1,7 +1,9 @@
 // C++ caller of the library through include/theseus_b200/RHSOperator.hpp:
 // Navier-Stokes Taylor-Green vortex (3^3 hexes, p=4, Ranocha volume / HLL
-// surface flux), one Mult on device memory.  Writes u and dudt (doubles,
-// byNODES) to the file named by argv[1].  Exit code 3 reports an operator
+// surface flux), one Mult on device memory (checked against the same rate
+// through host buffers, exit code 6, and followed by a three-cycle clocked
+// time loop, exit code 7).  Writes u and dudt (doubles, byNODES) to the file
+// named by argv[1].  Exit code 3 reports an operator
 // error (for example "no CUDA device") on stderr.
 #include "theseus_b200/RHSOperator.hpp"
 
@@ -40,6 +42,21 @@ int main(int argc, char **argv) {
     cudaMemcpy(ud, u.data(), sizeof(double) * u.size(), cudaMemcpyHostToDevice);
     op.Mult(ud, dd);
     cudaMemcpy(du.data(), dd, sizeof(double) * du.size(), cudaMemcpyDeviceToHost);
+    // the same rate through host buffers, twice in one call
+    std::vector<double> h0(du.size()), h1(du.size());
+    const double *ins[2] = {u.data(), u.data()};
+    double *outs[2] = {h0.data(), h1.data()};
+    op.MultHost(2, ins, outs);
+    cudaDeviceSynchronize();
+    if (h0 != du || h1 != du) return 6;
+    // three fixed steps of the clocked loop, then a finished loop leaves u alone
+    thx_time_loop loop = theseus_b200::TimeLoopDefaults(1.0, 1e-3, 3, -1.0), *loop_dev = nullptr;
+    if (cudaMalloc(&loop_dev, sizeof(loop)) != cudaSuccess) return 4;
+    cudaMemcpy(loop_dev, &loop, sizeof(loop), cudaMemcpyHostToDevice);
+    op.RunTimeLoop(ud, 0.0, 5, loop_dev);
+    cudaMemcpy(&loop, loop_dev, sizeof(loop), cudaMemcpyDeviceToHost);
+    cudaFree(loop_dev);
+    if (loop.cycle != 3 || !loop.done || std::fabs(loop.t - 3e-3) > 1e-15) return 7;
     cudaFree(ud);
     cudaFree(dd);
     std::printf("%s\n", op.Describe().c_str());
