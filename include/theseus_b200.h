@@ -385,7 +385,8 @@ int thx_cell_faces(int dim, int ne, const int64_t *vertex_ids, int32_t *face_ele
  * Every pointer is DEVICE memory: corners double[ne][2^dim][dim]
  * (lexicographic vertices), the face tables of thx_cell_faces, the outputs in
  * the thx_geometry layout.  Allocates nothing and waits for nothing
- * (stream-ordered). */
+ * (stream-ordered).  A face entry naming no cell or local face of the mesh
+ * yields NaN normals and weights for that face. */
 int thx_cell_geometry(int dim, int order, int ne, const double *corners, int nf, const int32_t *face_elem,
                       const int32_t *face_lface, int nbf, const int32_t *bdr_elem, const int32_t *bdr_lface,
                       double *jac, double *metric, double *face_normal, double *face_wminus,

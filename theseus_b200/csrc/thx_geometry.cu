@@ -106,8 +106,10 @@ __global__ void cell_volume_kernel(int ne, int N, LglNodes r, const double *__re
 // One thread per (face, face point): the minus element's adjugate row of the
 // face direction at the trace node (outward: negated on a - face) and the
 // lift weights of both sides; boundary faces (minus side only) after them.
+// Face entries that name no element or local face of the mesh get NaN
+// outputs instead of a read outside the arrays.
 template <int DIM>
-__global__ void cell_face_kernel(int N, LglNodes r, const double *__restrict__ jac,
+__global__ void cell_face_kernel(int ne, int N, LglNodes r, const double *__restrict__ jac,
                                  const double *__restrict__ metric, int nf, const int32_t *__restrict__ fe,
                                  const int32_t *__restrict__ fl, double *__restrict__ normal,
                                  double *__restrict__ wm, double *__restrict__ wp, int nbf,
@@ -122,16 +124,24 @@ __global__ void cell_face_kernel(int N, LglNodes r, const double *__restrict__ j
   const long long s = bdr ? t - nint : t;
   const int f = (int)(s / nfp), fp = (int)(s % nfp);
   const int e = bdr ? be[f] : fe[2 * f], lf = bdr ? bl[f] : fl[2 * f];
+  double *out = (bdr ? bnormal : normal) + s * DIM;
+  const int ep = bdr ? 0 : fe[2 * f + 1], lp = bdr ? 0 : fl[2 * f + 1];
+  if (e < 0 || e >= ne || lf < 0 || lf >= 2 * DIM || ep < 0 || ep >= ne || lp < 0 || lp >= 2 * DIM) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int d = 0; d < DIM; ++d) out[d] = nan;
+    if (bdr) bw[s] = nan;
+    else wm[s] = wp[s] = nan;
+    return;
+  }
   const long long node = (long long)e * nd + cell_trace_node(DIM, N, lf, fp);
   const double *row = metric + (node * DIM + (lf >> 1)) * DIM;
-  double *out = (bdr ? bnormal : normal) + s * DIM;
   for (int d = 0; d < DIM; ++d) out[d] = (lf & 1) ? row[d] : 0.0 - row[d];
   const double w = 1.0 / (r.w0 * jac[node]);
   if (bdr) {
     bw[s] = w;
   } else {
     wm[s] = w;
-    const long long np_ = (long long)fe[2 * f + 1] * nd + cell_trace_node(DIM, N, fl[2 * f + 1], fp);
+    const long long np_ = (long long)ep * nd + cell_trace_node(DIM, N, lp, fp);
     wp[s] = 1.0 / (r.w0 * jac[np_]);
   }
 }
@@ -218,11 +228,11 @@ int thx_cell_geometry(int dim, int order, int ne, const double *corners, int nf,
   if (nfw > 0) {
     const int fgrid = (int)((nfw + 255) / 256);
     if (dim == 2)
-      cell_face_kernel<2><<<fgrid, 256, 0, s>>>(N, r, jac, metric, nf, face_elem, face_lface, face_normal,
+      cell_face_kernel<2><<<fgrid, 256, 0, s>>>(ne, N, r, jac, metric, nf, face_elem, face_lface, face_normal,
                                                 face_wminus, face_wplus, nbf, bdr_elem, bdr_lface, bdr_normal,
                                                 bdr_weight);
     else
-      cell_face_kernel<3><<<fgrid, 256, 0, s>>>(N, r, jac, metric, nf, face_elem, face_lface, face_normal,
+      cell_face_kernel<3><<<fgrid, 256, 0, s>>>(ne, N, r, jac, metric, nf, face_elem, face_lface, face_normal,
                                                 face_wminus, face_wplus, nbf, bdr_elem, bdr_lface, bdr_normal,
                                                 bdr_weight);
     if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
