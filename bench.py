@@ -201,6 +201,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms, dist=None, device=None):
+    """The slowest rank's time: every rank contributes its own device-timed
+    milliseconds (nccl: a CUDA tensor; gloo: a CPU tensor)."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, steps, ms):
+    """Whole-job throughput of `world` independent replicas, each processing
+    units_per_rank units per step, timed as the slowest rank's ms."""
+    return world * units_per_rank * steps / (ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     import theseus_b200 as T
@@ -243,12 +260,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     barrier()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     nodes = m.num_nodes
-    value = world * nodes * args.steps / (ms * 1e-3)
+    value = replica_throughput(world, nodes, args.steps, ms)
 
     # end to end through the C ABI with host buffers (thx_rhs_host: each
     # step's FP64 state copied in from pinned host memory and its rate copied
@@ -264,12 +278,8 @@ def run_ours(args):
     op.mult_host([hu[i % 2] for i in range(args.steps)], [hdu[i % 2] for i in range(args.steps)])
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * nodes * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    e2e = {"value": replica_throughput(world, nodes, args.steps, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": hu[0].numel() * hu[0].element_size(),
            "d2h_bytes_per_step": hdu[0].numel() * hdu[0].element_size(), "overlap": "copy-in/compute/copy-out"}
 
