@@ -650,6 +650,68 @@ def run_sedov(args):
     print(json.dumps(line), flush=True)
 
 
+def run_setup(args):
+    """Mesh set-up on the device: a 64^3 hexahedral box at p=3 (262,144 cells,
+    16.8 M nodes) from its cells -- the face table built by the library on
+    the host (thx_cell_faces), the geometric factors (Jacobian, adjugate
+    metric, node coordinates, face normals and lift weights) computed by the
+    device kernels (thx_cell_geometry) -- against the library's host box
+    builder (thx_box_geometry) for the same mesh, with the largest relative
+    difference of the factors."""
+    import torch
+    import theseus_b200 as T
+    from theseus_b200.cells import cell_faces, cell_geometry
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, order, dim = args.setup_n, 3, 3
+    h = 1.0 / n
+    ijk = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)[:, ::-1]
+    off = np.array([[(v >> d) & 1 for d in range(3)] for v in range(8)])
+    cell = ijk[:, None, :] + off[None, :, :]                      # (ne, 8, 3) lattice corners
+    corners = cell * h
+    ids = ((cell % n) * np.array([1, n, n * n])).sum(-1).astype(np.int64)
+    t0 = time.perf_counter()
+    fe, fl, be, bl = cell_faces(dim, ids)
+    faces_s = time.perf_counter() - t0
+    geo = cell_geometry(dim, order, corners, fe, fl, be, bl)     # warm-up (module load, allocation)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib = __import__("theseus_b200.cells", fromlist=["_lib"])._lib()
+    import ctypes as C
+    cd = torch.as_tensor(corners.astype(np.float64), device="cuda").contiguous()
+    fed, fld = (torch.as_tensor(x, device="cuda").contiguous() for x in (fe, fl))
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
+    a.record(stream)
+    for _ in range(args.steps):
+        lib.thx_cell_geometry(dim, order, len(ids), ptr(cd), len(fe), ptr(fed), ptr(fld), 0, None, None,
+                              ptr(geo["jac"]), ptr(geo["metric"]), ptr(geo["face_normal"]), ptr(geo["face_wminus"]),
+                              ptr(geo["face_wplus"]), None, None, ptr(geo["coords"]), C.c_void_p(stream.cuda_stream))
+    b.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = a.elapsed_time(b) / args.steps
+    t0 = time.perf_counter()
+    ref = T.periodic_box(dim, order, (n, n, n), [0.0] * 3, [1.0] * 3)
+    host_s = time.perf_counter() - t0
+    jac, met = geo["jac"].cpu().numpy(), geo["metric"].cpu().numpy()
+    diff = max(float(np.abs(jac - ref.jac).max() / np.abs(ref.jac).max()),
+               float(np.abs(met - ref.metric).max() / np.abs(ref.metric).max()))
+    nodes, nfp = len(ids) * (order + 1) ** 3, (order + 1) ** 2
+    written = nodes * 8 * (1 + 9 + 3) + len(fe) * nfp * 8 * (3 + 2)
+    read = len(ids) * 8 * 3 * 8 + len(fe) * 16 + len(fe) * nfp * (2 * 8 + 3 * 8)
+    gbs = (read + written) / (dev_ms * 1e-3) / 1e9
+    peak, src = peaks()
+    line = {"metric": "mesh set-up time (geometric factors on the device)", "value": dev_ms, "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"setup_box_{n}^3_p{order}", "cells": len(ids), "nodes": nodes,
+                       "faces": len(fe)},
+            "face_table_host_s": faces_s, "host_box_builder_s": host_s,
+            "speedup_vs_host_builder": host_s / (dev_ms * 1e-3),
+            "max_rel_diff_vs_host_builder": diff,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_source": src, "algorithmic_bytes": read + written}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -661,12 +723,14 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
-    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving", "lte", "sedov"],
+    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving", "lte", "sedov", "setup"],
                     help="rhs: the headline RHS throughput; serving: the batched case stream; "
-                         "lte: the LTE-gas Taylor-Green vortex; sedov: the blended blast")
+                         "lte: the LTE-gas Taylor-Green vortex; sedov: the blended blast; "
+                         "setup: mesh set-up on the device")
     ap.add_argument("--sedov-n", type=int, default=64, help="sedov: elements per direction")
     ap.add_argument("--sedov-steps", type=int, default=300, help="sedov: SSP-RK3 steps")
     ap.add_argument("--lte-n", type=int, default=24, help="lte: elements per direction")
+    ap.add_argument("--setup-n", type=int, default=64, help="setup: cells per direction")
     ap.add_argument("--cases", type=int, default=4096, help="serving: cases in the stream")
     ap.add_argument("--sample", type=int, default=256, help="serving: cases also run one at a time")
     ap.add_argument("--chunk", type=int, default=10, help="serving: SSP-RK3 steps per graph launch")
@@ -679,6 +743,8 @@ def main():
         run_lte(args)
     elif args.workload == "sedov":
         run_sedov(args)
+    elif args.workload == "setup":
+        run_setup(args)
     else:
         run_ours(args)
 
