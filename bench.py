@@ -676,8 +676,9 @@ def run_setup(args):
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    lib = __import__("theseus_b200.cells", fromlist=["_lib"])._lib()
     import ctypes as C
+    from theseus_b200.cells import _lib as cells_lib
+    lib = cells_lib()
     cd = torch.as_tensor(corners.astype(np.float64), device="cuda").contiguous()
     fed, fld = (torch.as_tensor(x, device="cuda").contiguous() for x in (fe, fl))
     ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None and t.numel() else None

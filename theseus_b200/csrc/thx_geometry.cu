@@ -18,7 +18,6 @@
 #include <algorithm>
 #include <array>
 #include <cuda_runtime.h>
-#include <map>
 #include <tuple>
 #include <vector>
 
@@ -155,32 +154,44 @@ int thx_cell_faces(int dim, int ne, const int64_t *vertex_ids, int32_t *face_ele
   if ((dim != 2 && dim != 3) || ne <= 0 || !vertex_ids || !num_faces || !num_bdr_faces)
     return THX_ERR_INVALID_ARGUMENT;
   const int nv = 1 << dim, nfv = 1 << (dim - 1);
-  using Key = std::array<int64_t, 4>;
-  std::map<Key, std::vector<std::pair<int, int>>> users;
+  // every local face keyed by its sorted vertex ids; equal keys end up
+  // adjacent after one sort
+  struct Side {
+    std::array<int64_t, 4> key;
+    int e, lf;
+  };
+  std::vector<Side> sides((size_t)ne * 2 * dim);
   for (int e = 0; e < ne; ++e)
     for (int lf = 0; lf < 2 * dim; ++lf) {
       const int dir = lf >> 1, side = lf & 1;
-      Key k{-1, -1, -1, -1};
+      Side &sd = sides[(size_t)e * 2 * dim + lf];
+      sd.key = {-1, -1, -1, -1};
+      sd.e = e;
+      sd.lf = lf;
       int m = 0;
       for (int v = 0; v < nv; ++v)
-        if (((v >> dir) & 1) == side) k[m++] = vertex_ids[(size_t)e * nv + v];
-      std::sort(k.begin(), k.begin() + nfv);
-      users[k].push_back({e, lf});
+        if (((v >> dir) & 1) == side) sd.key[m++] = vertex_ids[(size_t)e * nv + v];
+      std::sort(sd.key.begin(), sd.key.begin() + nfv);
     }
+  std::sort(sides.begin(), sides.end(), [](const Side &a, const Side &b) {
+    return a.key != b.key ? a.key < b.key : (a.e != b.e ? a.e < b.e : a.lf < b.lf);
+  });
   std::vector<std::tuple<int, int, int, int, int>> faces;
   std::vector<std::tuple<int, int, int>> bfaces;
-  for (auto &kv : users) {
-    auto &u = kv.second;
-    if (u.size() == 2) {
-      auto m = u[0], p = u[1];
+  for (size_t i = 0; i < sides.size();) {
+    size_t j = i + 1;
+    while (j < sides.size() && sides[j].key == sides[i].key) ++j;
+    if (j - i == 2) {
+      std::pair<int, int> m{sides[i].e, sides[i].lf}, p{sides[i + 1].e, sides[i + 1].lf};
       if ((m.second & 1) == 0) std::swap(m, p);  // minus side: the element whose + face it is
       if (p.second != m.second - 1) return THX_ERR_INVALID_ARGUMENT;  // faces not aligned
       faces.emplace_back(m.second >> 1, m.first, m.second, p.first, p.second);
-    } else if (u.size() == 1) {
-      bfaces.emplace_back(u[0].second >> 1, u[0].first, u[0].second);
+    } else if (j - i == 1) {
+      bfaces.emplace_back(sides[i].lf >> 1, sides[i].e, sides[i].lf);
     } else {
       return THX_ERR_INVALID_ARGUMENT;  // non-manifold face
     }
+    i = j;
   }
   std::sort(faces.begin(), faces.end());
   std::sort(bfaces.begin(), bfaces.end());
