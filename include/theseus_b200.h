@@ -309,11 +309,11 @@ int thx_rhs_host(thx_handle h, int n, const double *const *u_host, double *const
  * In FP32-mixed mode the FP64 master state is accumulated in double and each
  * RHS is evaluated on a float working copy. */
 int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream);
-/* nsteps SSP-RK3 steps with the variable time step of the reference's
- * variable_dt runs, dt = cfl / (max(advective, surface) + diffusive rate) of
- * each step's initial state (src/Simulation.cpp:1150-1160), computed on the
- * device: the loop never waits for the host, so it can be captured in a CUDA
- * graph.  dt_history (device, may be NULL) receives each step's dt.  A
+/* nsteps SSP-RK3 steps with dt = cfl / (max(advective, surface) + diffusive
+ * rate) of each step's initial state (src/Simulation.cpp:1150-1160), computed
+ * on the device: the loop never waits for the host, so it can be captured in
+ * a CUDA graph.  Unlike the reference's loop it applies no growth limit and
+ * lands on no events; thx_rk3_time_loop runs that loop.  dt_history (device, may be NULL) receives each step's dt.  A
  * non-positive rate sets the numerics status flag and dt = 0. */
 int thx_rk3_steps_cfl(thx_handle h, double *u, double cfl, int nsteps, double *dt_history,
                       void *stream);
