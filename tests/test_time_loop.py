@@ -46,10 +46,18 @@ def test_defaults_are_the_reference_runtime_defaults():
     assert math.isinf(L.next_output) and math.isinf(L.next_checkpoint) and math.isinf(L.t_final)
 
 
+def test_record_fields_are_set_on_the_record():
+    L = TimeLoop(t_final=1.0)
+    L.dt = 0.25
+    L.max_cycles = 3
+    assert L.c.dt == 0.25 and L.c.max_cycles == 3 and "dt" not in L.__dict__
+    assert [L.begin() for _ in range(1)] == [0.25]
+
+
 def host_driver(loop, rates, cfl, step_state=0.0):
     """Drive the library's host bookkeeping with scripted total rates."""
     if cfl > 0 and loop.dt <= 0:
-        loop.c.dt = cfl / rates(0)
+        loop.dt = cfl / rates(0)
     taken = []
     while not loop.done:
         h = loop.begin()
@@ -130,7 +138,7 @@ def test_device_loop_equals_host_driven_loop(cuda, flow, cfl):
     host = TimeLoop(**kw)
     if cfl > 0:
         r = op.EstimateStability(b)
-        host.c.dt = cfl / (max(r[0], r[1]) + r[2])
+        host.dt = cfl / (max(r[0], r[1]) + r[2])
     taken = []
     while not host.done:
         h = host.begin()

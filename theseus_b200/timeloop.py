@@ -92,6 +92,12 @@ class TimeLoop:
             return getattr(c, name)
         raise AttributeError(name)
 
+    def __setattr__(self, name, value):
+        if name != "c" and name in dict(TimeLoopC._fields_):
+            setattr(self.c, name, value)       # a record field, not a Python attribute
+        else:
+            object.__setattr__(self, name, value)
+
     def begin(self):
         """The step of the next cycle (0 once done), on the host record."""
         return _lib().thx_time_loop_begin(C.byref(self.c))
