@@ -46,6 +46,26 @@ def test_defaults_are_the_reference_runtime_defaults():
     assert math.isinf(L.next_output) and math.isinf(L.next_checkpoint) and math.isinf(L.t_final)
 
 
+def test_record_layout_matches_the_c_header(tmp_path):
+    """The ctypes record and the C struct agree in size and field offsets."""
+    import ctypes
+    import os
+    import subprocess
+    from theseus_b200.timeloop import TimeLoopC
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    names = [n for n, _ in TimeLoopC._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "theseus_b200.h"\nint main(void) {\n'
+                   '  printf("%zu", sizeof(thx_time_loop));\n' +
+                   "".join(f'  printf(" %zu", offsetof(thx_time_loop, {n}));\n' for n in names) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(TimeLoopC)
+    assert got[1:] == [getattr(TimeLoopC, n).offset for n in names]
+
+
 def test_record_fields_are_set_on_the_record():
     L = TimeLoop(t_final=1.0)
     L.dt = 0.25
