@@ -6,9 +6,14 @@ whole mesh (RHSOperator::Mult).  DOF = solution nodes (E*N^d).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Prints one JSON line (rank 0).  --impl reference times the CPU implementation
-of the path (the FP64 oracle restatement of the reference's RHS, all host
-threads) on a bounded sample of the same workload.
+Prints one JSON line (rank 0): the headline FP64 figure, its end-to-end
+figure through the C ABI with host buffers, the dominant kernel's roofline,
+the FP32-mixed companion, the reference's CPU right-hand side on the same
+workload, and (one GPU) compact results of the other configurations -- the
+2-D isentropic vortex, the Sedov blast, the LTE Taylor-Green vortex and the
+batched serving stream.  --impl reference times the reference's CPU
+right-hand side (its own header kernels compiled here, all host threads) on
+the full workload, one right-hand side per step.
 """
 import argparse
 import json
@@ -112,6 +117,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def fp64_peak_tflops():
+    """FP64 FMA throughput of this GPU (thx_measure_fp64_fma_peak: independent
+    FMA chains on every SM, best of five CUDA-event-timed launches)."""
+    import ctypes as C
+    import torch
+    import theseus_b200 as T
+    lib = T.library()
+    lib.thx_measure_fp64_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.c_void_p]
+    v = C.c_double()
+    st = lib.thx_measure_fp64_fma_peak(2048, 5, C.byref(v), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return v.value / 1e12 if st == 0 else None
+
+
 def bytes_per_phase(m, elem_size=8):
     """Algorithmic HBM bytes of each kernel for one RHS (geometry stored once):
     gradient: read u, write the physical viscous flux (dim x (neq-1) per node);
@@ -128,75 +146,124 @@ def bytes_per_phase(m, elem_size=8):
     return {"blend": nodes * neq * s, "grad": grad, "face": face, "volume": vol}
 
 
+# Floating-point operations of one two-point volume flux as the kernels
+# evaluate it from per-node primitives (rho, v, p and one auxiliary), counted
+# from the source with +, -, x = 1, FMA = 2, divide / sqrt / log = 1; the log
+# mean (y - x)/log(y/x) with its branch variable u is 11.  D = dimension.
+#   Ranocha:       2 log means, p1 p2 / log mean, the kinetic-energy and
+#                  pressure-work terms: 34 + 16 D
+#   Chandrashekar: 2 log means, p_hat, h_hat: 33 + 15 D
+#   Pirozzoli:     arithmetic means only: 10 + 12 D
+PAIR_FLOPS = {"ranocha": lambda d: 34 + 16 * d, "chandrashekar": lambda d: 33 + 15 * d,
+              "pirozzoli": lambda d: 10 + 12 * d}
+
+
+def volume_flops(m, volume_flux, viscous):
+    """Algorithmic flops of the volume kernel for one RHS: every symmetric pair
+    once (PAIR_FLOPS) plus its D-hat-2 accumulation into both end nodes
+    (2 nodes x neq FMAs); for Navier-Stokes the contravariant viscous flux
+    (dim x dim metric products per flux row) and its D-hat divergence
+    (N terms per direction) per node.  Returns (flops, pairs)."""
+    dim, N, neq = m.dim, m.order + 1, m.neq
+    pairs = m.num_elements * dim * N ** (dim - 1) * (N * (N - 1) // 2)
+    per_pair = PAIR_FLOPS[volume_flux](dim) + 2 * 2 * neq
+    per_node = (2 * dim * dim * (neq - 1) + 2 * dim * N * (neq - 1)) if viscous else 0
+    return pairs * per_pair + m.num_nodes * per_node, pairs
+
+
+# DRAM bytes per node of one launch, from ncu captures of the same kernels
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / nodes of the
+# captured mesh; the captures and the meshes are listed beside the figures).
+# A kernel's traffic grows with its node count, so the bench scales these to
+# its own mesh.  Filled per (kernel, precision); absent: null.
+TRAFFIC_PER_NODE = {}
+
+
 def cpu_rhs_fn():
     """The CPU right-hand side that stands for the reference: the reference's
-    own point kernels compiled from its headers (oracle/_ref, OpenMP over
-    elements and faces) when that library was built, else the oracle's
-    restatement.  Returns (rhs(mesh, cfg, u), kind, threads)."""
+    own point kernels compiled from its headers, OpenMP over elements and
+    faces -- the -O3 -march=native build where this host can run it, else the
+    parity build (oracle/_ref) -- or, when neither was built, the oracle's
+    restatement.  Returns (rhs(mesh, cfg, u), kind, threads, build)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     threads = O.max_threads()
-    if os.path.exists(O.REF_PATH):
+    if O.ref_native() is not None:
+        return (lambda om, cfg, u: O.ref_rhs(om, cfg, u, native=True)), "reference", threads, \
+            "reference headers, g++ -O3 -march=native, OpenMP"
+    if O.ref_available():
         try:
             O.ref()
-            return (lambda om, cfg, u: O.ref_rhs(om, cfg, u)), "reference", threads
+            return (lambda om, cfg, u: O.ref_rhs(om, cfg, u)), "reference", threads, \
+                "reference headers, g++ -O2 -march=x86-64-v3 -ffp-contract=off, OpenMP"
         except OSError:
             pass
-    return (lambda om, cfg, u: O.rhs(om, cfg, u, nthreads=threads)), "port", threads
+    return (lambda om, cfg, u: O.rhs(om, cfg, u, nthreads=threads)), "port", threads, \
+        "oracle restatement, OpenMP"
 
 
-def cpu_case(sample_n):
+def cpu_case(n=None):
+    """The workload's mesh (the oracle's own box builder: nothing of the
+    product library is loaded), its configuration and its state."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    import theseus_b200 as T
-    m, u = build_case(sample_n)
-    om = O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
-                m.face_wminus, m.face_wplus)
-    cfg = T.make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
-                        surface_flux=WORKLOAD["surface_flux"], **physics())
-    return m, om, cfg, u
+    from theseus_b200 import cases
+    from theseus_b200._abi import make_config
+    n = n or WORKLOAD["mesh"]
+    om = O.box_mesh(3, WORKLOAD["order"], n, [0.0] * 3, [2 * np.pi] * 3)
+    u = cases.taylor_green(om.coords, mach=WORKLOAD["mach"], noise=WORKLOAD["noise"], seed=0)
+    cfg = make_config(flow="ns", volume_flux=WORKLOAD["volume_flux"],
+                      surface_flux=WORKLOAD["surface_flux"], **physics())
+    return om, cfg, u
 
 
-def cpu_reference(args, sample_n=(16, 16, 16), budget_s=20.0):
-    """The CPU reference on a bounded sample of the workload, all host threads."""
-    fn, kind, threads = cpu_rhs_fn()
-    m, om, cfg, u = cpu_case(sample_n)
-    fn(om, cfg, u)  # warm-up
+def cpu_reference(budget_s=15.0, max_evals=20, keep_rate=False):
+    """The CPU reference on the full workload, all host threads: one warm-up
+    right-hand side, then evaluations until budget_s has passed (at most
+    max_evals).  keep_rate: also return the last rate (for the parity check)."""
+    fn, kind, threads, build = cpu_rhs_fn()
+    om, cfg, u = cpu_case()
+    du = fn(om, cfg, u)  # warm-up
     t0 = time.perf_counter()
     evals = 0
     while True:
-        fn(om, cfg, u)
+        du = fn(om, cfg, u)
         evals += 1
-        if time.perf_counter() - t0 > budget_s or evals >= 200:
+        if time.perf_counter() - t0 > budget_s or evals >= max_evals:
             break
     dt = time.perf_counter() - t0
-    return {"value": m.num_nodes * evals / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"TGV {sample_n[0]}x{sample_n[1]}x{sample_n[2]} p=4 ({m.num_nodes} nodes), "
-                      f"{evals} RHS evaluations in {dt:.1f} s"}
+    nodes = om.num_elements * om.nd
+    out = {"value": nodes * evals / dt, "unit": UNIT, "cores": threads, "kind": kind,
+           "build": build,
+           "sample": f"the full workload (TGV {om.shape[0]}^3 p={om.order}, {nodes} nodes): "
+                     f"{evals} RHS evaluations in {dt:.1f} s"}
+    return (out, du, u) if keep_rate else out
 
 
 def run_reference(args):
+    """--impl reference: the reference's CPU right-hand side on this host's
+    cores, on the same workload (the full 32^3 mesh), each step one RHS."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    fn, kind, threads = cpu_rhs_fn()
-    sample = (16, 16, 16)
-    m, om, cfg, u = cpu_case(sample)
+    fn, kind, threads, build = cpu_rhs_fn()
+    om, cfg, u = cpu_case()
     for _ in range(args.warmup):
         fn(om, cfg, u)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         fn(om, cfg, u)
     dt = time.perf_counter() - t0
-    value = m.num_nodes * args.steps / dt
+    nodes = om.num_elements * om.nd
+    value = nodes * args.steps / dt
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": dict(WORKLOAD, sample=f"{sample[0]}^3 p=4 sub-mesh of the workload",
-                           parallelism="cpu threads"),
+            "config": dict(WORKLOAD, parallelism="cpu threads"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"TGV {sample[0]}^3 p=4 ({m.num_nodes} nodes) per step"},
+                             "build": build,
+                             "sample": f"the full workload ({nodes} nodes), one RHS per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -216,6 +283,31 @@ def replica_throughput(world, units_per_rank, steps, ms):
     """Whole-job throughput of `world` independent replicas, each processing
     units_per_rank units per step, timed as the slowest rank's ms."""
     return world * units_per_rank * steps / (ms * 1e-3)
+
+
+def timed_rk3(op, u0, dt, steps, stream, repeats=2):
+    """Device time (ms) of `steps` SSP-RK3 steps from u0, after a short warm-up
+    run; the median of `repeats` runs, each from the same initial state.
+    Returns (ms, final state of the last run)."""
+    import torch
+    y = u0.clone()
+    op.rk3_steps(y, dt, 3)  # warm-up: graphs, caches, clocks
+    times = []
+    for _ in range(repeats):
+        y.copy_(u0)
+        torch.cuda.synchronize()
+        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ta.record(stream)
+        op.rk3_steps(y, dt, steps)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        times.append(ta.elapsed_time(tb))
+    return float(statistics.median(times)), y
+
+
+def field_errors(got, ref, groups):
+    """Relative L2 per conserved field (rows grouped: density, momentum, energy)."""
+    return [float(((got[g] - ref[g]).pow(2).sum() / ref[g].pow(2).sum()).sqrt()) for g in groups]
 
 
 def run_ours(args):
@@ -283,27 +375,43 @@ def run_ours(args):
            "h2d_bytes_per_step": hu[0].numel() * hu[0].element_size(),
            "d2h_bytes_per_step": hdu[0].numel() * hdu[0].element_size(), "overlap": "copy-in/compute/copy-out"}
 
-    # per-kernel device times for the roofline (after the timed region)
+    # per-kernel device times (CUDA events on the launching stream, one event
+    # between consecutive kernels of a right-hand side) over as many
+    # right-hand sides as the timed region, after it
     ud.copy_(torch.as_tensor(u).to(op.dtype))
     phases = np.zeros(4)
-    nprof = max(3, min(args.steps, 10))
+    nprof = max(3, args.steps)
     for _ in range(nprof):
         phases += np.array(op.profile(ud, du))
     phases /= nprof
     names = ["blend", "grad", "face", "volume"]
-    algo = bytes_per_phase(m, 4 if prec == "fp32" else 8)
+    es = 4 if prec == "fp32" else 8
+    algo = bytes_per_phase(m, es)
+    peak_hbm, peak_kind = peaks()
+    fp64_tf = fp64_peak_tflops()
+    vflops, pairs = volume_flops(m, WORKLOAD["volume_flux"], True)
     dom = int(np.argmax(phases))
-    peak, peak_kind = peaks()
-    achieved = algo[names[dom]] / (phases[dom] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": names[dom] + "_kernel", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None,
-                "phase_ms": {k: float(v) for k, v in zip(names, phases)},
-                "algorithmic_bytes": {k: int(v) for k, v in algo.items()}}
-    # FP64 pipe view of the flux-differencing kernel: pairs x F_pair flops
-    N = m.order + 1
-    pairs = m.num_elements * 3 * N * N * (N * (N - 1) // 2)
-    roofline["volume_pair_evals_per_s"] = pairs / (phases[3] * 1e-3)
+    kname = names[dom] + "_kernel"
+    traffic = TRAFFIC_PER_NODE.get((kname, prec))
+    if names[dom] == "volume" and prec == "fp64" and fp64_tf:
+        # the pair phase is FP64 arithmetic: roofline against the FP64 FMA peak
+        achieved = vflops / (phases[dom] * 1e-3) / 1e12
+        roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": fp64_tf,
+                    "unit": "TFLOP/s", "frac": achieved / fp64_tf,
+                    "peak_source": "measured (thx_measure_fp64_fma_peak, this run)",
+                    "algorithmic_flops": vflops}
+    else:
+        achieved = algo[names[dom]] / (phases[dom] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak_hbm,
+                    "unit": "GB/s", "frac": achieved / peak_hbm, "peak_source": peak_kind}
+    roofline["traffic"] = traffic * nodes if traffic else None
+    roofline["phase_ms"] = {k: float(v) for k, v in zip(names, phases)}
+    roofline["algorithmic_bytes"] = {k: int(v) for k, v in algo.items()}
+    roofline["hbm_frac"] = {k: (algo[k] / (phases[i] * 1e-3) / 1e9) / peak_hbm
+                            for i, k in enumerate(names) if phases[i] > 0.01}
+    roofline["volume_fp64"] = {"pairs": pairs, "pair_flops": PAIR_FLOPS[WORKLOAD["volume_flux"]](3),
+                               "flops": vflops, "fp64_fma_peak_tflops": fp64_tf,
+                               "pair_evals_per_s": pairs / (phases[3] * 1e-3)}
 
     # FP32-mixed companion number and its error against FP64: RHS and the
     # final solution after a fixed-dt SSP-RK3 run from the same state
@@ -328,25 +436,13 @@ def run_ours(args):
         op.Mult(u64, du)
         ref = du.clone()
         err = ((d32 - ref).pow(2).sum(dim=(1, 2)) / ref.pow(2).sum(dim=(1, 2))).sqrt()
-        # trajectories: fixed dt from CFL 0.5 at t=0, rk_steps SSP-RK3 steps each
+        # trajectories: fixed dt from CFL 0.5 at t=0, rk_steps SSP-RK3 steps
+        # each, warmed up and timed twice (median)
         dt = op.estimate_dt(u64, 0.5)
-        ya, yb = u64.clone(), u64.clone()
-        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ta.record(stream)
-        op.rk3_steps(ya, dt, args.rk_steps)
-        tb.record(stream)
-        torch.cuda.synchronize()
-        ms_rk64 = ta.elapsed_time(tb)
-        ta.record(stream)
-        op32.rk3_steps(yb, dt, args.rk_steps)
-        tb.record(stream)
-        torch.cuda.synchronize()
-        ms_rk32 = ta.elapsed_time(tb)
+        ms_rk64, ya = timed_rk3(op, u64, dt, args.rk_steps, stream)
+        ms_rk32, yb = timed_rk3(op32, u64, dt, args.rk_steps, stream)
         serr = ((yb - ya).pow(2).sum(dim=(1, 2)) / ya.pow(2).sum(dim=(1, 2))).sqrt()
-        # per conserved field: density, the momentum vector, total energy
-        groups = [[0], [1, 2, 3], [4]]
-        ferr = [float(((yb[g] - ya[g]).pow(2).sum() / ya[g].pow(2).sum()).sqrt()) for g in groups]
-        # kinetic-energy integral (IntegralMeasures) after the run, both paths
+        ferr = field_errors(yb, ya, [[0], [1, 2, 3], [4]])
         ke0 = op.IntegralMeasures(u64)["ke"]
         ke64 = op.IntegralMeasures(ya)["ke"]
         ke32 = op.IntegralMeasures(yb)["ke"]
@@ -359,7 +455,7 @@ def run_ours(args):
             "speedup_vs_fp64": (ms / ms32) if ms32 > 0 else None,
             "rhs_rel_l2_vs_fp64": [float(x) for x in err.tolist()],
             "state_offset": off,
-            "rk3": {"steps": args.rk_steps, "dt": dt,
+            "rk3": {"steps": args.rk_steps, "dt": dt, "timing": "median of 2 runs after a 3-step warm-up",
                     "fp64_dof_rhs_per_s": 3 * nodes * args.rk_steps / (ms_rk64 * 1e-3),
                     "fp32_mixed_dof_rhs_per_s": 3 * nodes * args.rk_steps / (ms_rk32 * 1e-3),
                     "speedup": ms_rk64 / ms_rk32,
@@ -370,9 +466,9 @@ def run_ours(args):
                     "kinetic_energy": {"t0": ke0, "fp64": ke64, "fp32_mixed": ke32,
                                        "rel_diff": abs(ke32 - ke64) / abs(ke64)}},
             "phase_ms": {k: float(v) for k, v in zip(["blend", "grad", "face", "volume"], ph32)}}
-        del op32
+        del op32, ya, yb
 
-    launches = args.steps * (3 if True else 2)
+    launches = args.steps * 3  # gradient, face and volume kernels per right-hand side
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32-mixed",
@@ -384,13 +480,145 @@ def run_ours(args):
             "e2e": e2e, "roofline": roofline, "clocks": clk.summary(),
             "gpu_launches": launches}
     line.update(extra)
-    if rank == 0 and not args.skip_cpu:
-        line["cpu_baseline"] = cpu_reference(args)
+    if rank == 0 and not args.skip_cpu and world == 1:
+        # the reference's CPU right-hand side on the same (full) workload, and
+        # this run's GPU rate against it
+        cb, ref_du, _ = cpu_reference(keep_rate=True)
+        line["cpu_baseline"] = cb
+        ud.copy_(torch.as_tensor(u))
+        op.Mult(ud, du)
+        got = du.cpu().numpy()
+        rel = np.sqrt(((got - ref_du) ** 2).reshape(5, -1).sum(1) / (ref_du ** 2).reshape(5, -1).sum(1))
+        line["rhs_rel_l2_vs_cpu_reference_full_mesh"] = [float(x) for x in rel]
+    if world == 1 and not args.no_workloads:
+        del op, ud, du
+        torch.cuda.empty_cache()
+        line["workloads"] = other_workloads(args)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def other_workloads(args):
+    """Compact results of the other configurations (each also available in
+    full with --workload): the 2-D isentropic vortex, the Sedov blast, the LTE
+    Taylor-Green vortex and the batched serving stream."""
+    import torch
+    out = {}
+    for name, fn in (("vortex_2d", run_vortex), ("sedov", run_sedov), ("lte", run_lte),
+                     ("serving", run_serving)):
+        try:
+            full = fn(args)
+            out[name] = compact(name, full)
+        except Exception as exc:  # report, keep the headline line
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"[:400]}
+        torch.cuda.empty_cache()
+    return out
+
+
+def compact(name, d):
+    keep = {
+        "vortex_2d": ["value", "unit", "config", "rk3", "fp32_mixed", "rhs_rel_l2_vs_oracle",
+                      "final_rel_l2_vs_oracle", "entropy_residual", "cpu"],
+        "sedov": ["value", "unit", "config", "fp32_speedup", "final_solution_rel_l2_fp32_vs_fp64",
+                  "blending_agreement_t0", "rhs_rel_l2_vs_oracle_4cubed"],
+        "lte": ["value", "unit", "config", "newton_recoveries_per_s", "lteec_pairs_per_s",
+                "rhs_rel_l2_vs_oracle_3cubed", "rk3", "phase_ms"],
+        "serving": ["value", "unit", "latency_s", "makespan_s", "dof_rhs_per_s", "one_at_a_time_fp64",
+                    "speedup_vs_one_at_a_time", "final_solution_rel_l2_vs_fp64"],
+    }[name]
+    r = {k: d[k] for k in keep if k in d}
+    if name == "sedov":
+        for p in ("fp64", "fp32_mixed"):
+            q = d[p]
+            r[p] = {"dof_rhs_per_s": q["dof_rhs_per_s"], "blended_fraction": q["blended_fraction"],
+                    "rk3_dof_rhs_per_s": q["rk3"]["dof_rhs_per_s"], "status": q["status"]}
+    if name == "serving" and "final_solution_rel_l2_vs_fp64" in r:
+        r["final_solution_rel_l2_vs_fp64"] = {k: v for k, v in r["final_solution_rel_l2_vs_fp64"].items()
+                                              if k != "worst"}
+    return r
+
+
+def run_vortex(args):
+    """2-D Euler isentropic vortex: periodic [-5, 5]^2, 32 x 32 quads, p=3
+    (16,384 nodes, 4 conserved variables), Chandrashekar volume / Roe surface
+    flux, no blending, rho = 1, u = (1, 1), p = 1 with a vortex of strength 5 at
+    the origin, dt from CFL 0.5 at t = 0 (the oracle's estimate) held fixed,
+    100 SSP-RK3 steps in FP64 and FP32-mixed.  Reports RHS throughput, the
+    trajectories against the oracle's (all host threads), the entropy
+    residual of the first right-hand side on both sides, and the reference's
+    CPU right-hand side and the oracle's 100-step run timed on this host."""
+    import torch
+    import theseus_b200 as T
+    from theseus_b200 import cases
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    steps = 100
+    m = T.periodic_box(2, 3, (32, 32), [-5.0, -5.0], [5.0, 5.0])
+    u = cases.isentropic_vortex(m.coords, strength=5.0)
+    kw = dict(numerical_flux="chandrashekar", surface_flux="roe")
+    cfg = T.make_config(flow="euler", volume_flux="chandrashekar", surface_flux="roe")
+    om = O.Mesh(m.dim, m.order, m.jac, m.metric, m.face_elem, m.face_lface, m.face_normal,
+                m.face_wminus, m.face_wplus)
+    nth = O.max_threads()
+    dt, _ = O.estimate_dt(om, cfg, u, 0.5)
+    stream = torch.cuda.current_stream()
+    op = T.EulerOperator(m, **kw)
+    ud = torch.as_tensor(u, device="cuda").contiguous()
+    du = torch.empty_like(ud)
+    for _ in range(max(args.warmup, 3)):
+        op.Mult(ud, du)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        op.Mult(ud, du)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    gpu_du = du.cpu().numpy()
+    ms_rk, y = timed_rk3(op, ud, dt, steps, stream)
+    op32 = T.EulerOperator(m, precision="fp32", state_offset=[1.0, 1.0, 1.0, 3.5], **kw)
+    ms_rk32, y32 = timed_rk3(op32, ud, dt, steps, stream)
+    # oracle: first right-hand side, its entropy residual, the trajectory
+    ref_du = O.rhs(om, cfg, u, nthreads=nth)
+    t0 = time.perf_counter()
+    ref_y = O.rk3_steps(om, cfg, u, dt, steps, nthreads=nth)
+    port_s = time.perf_counter() - t0
+    yg = y.cpu().numpy()
+    rel = lambda g, r: [float(x) for x in np.sqrt(((g - r) ** 2).reshape(4, -1).sum(1) /
+                                                  (r ** 2).reshape(4, -1).sum(1))]
+    groups = [[0], [1, 2], [3]]
+    y32g = y32.cpu().numpy()
+    f32 = [float(np.sqrt(((y32g[g] - yg[g]) ** 2).sum() / (yg[g] ** 2).sum())) for g in groups]
+    # the reference's CPU right-hand side on the same case
+    fn, kind, threads, build = cpu_rhs_fn()
+    fn(om, cfg, u)
+    t0 = time.perf_counter()
+    n_cpu = 0
+    while time.perf_counter() - t0 < 2.0 and n_cpu < 200:
+        fn(om, cfg, u)
+        n_cpu += 1
+    cpu_s = (time.perf_counter() - t0) / n_cpu
+    return {"metric": "DOF*RHS/s (2-D Euler isentropic vortex)", "value": m.num_nodes / (ms * 1e-3),
+            "unit": "DOF*RHS/s", "n_gpus": 1, "ms_per_step": ms, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "euler2d_vortex_32^2_p3", "nodes": m.num_nodes, "strength": 5.0,
+                       "fluxes": {"volume": "chandrashekar", "surface": "roe"}, "blending": False,
+                       "cfl": 0.5, "dt": dt, "steps": steps},
+            "rk3": {"ms": ms_rk, "dof_rhs_per_s": 3 * steps * m.num_nodes / (ms_rk * 1e-3),
+                    "timing": "median of 2 runs after a 3-step warm-up"},
+            "fp32_mixed": {"rk3_ms": ms_rk32, "speedup": ms_rk / ms_rk32,
+                           "final_solution_rel_l2_vs_fp64": dict(zip(("density", "momentum", "energy"),
+                                                                     f32))},
+            "rhs_rel_l2_vs_oracle": rel(gpu_du, ref_du),
+            "final_rel_l2_vs_oracle": rel(yg, ref_y),
+            "entropy_residual": {"gpu": O.entropy_residual(om, cfg, u, gpu_du),
+                                 "oracle": O.entropy_residual(om, cfg, u, ref_du)},
+            "cpu": {"rhs_dof_rhs_per_s": m.num_nodes / cpu_s, "kind": kind, "build": build,
+                    "cores": threads, "oracle_100_steps_s": port_s, "oracle_threads": nth}}
 
 
 def run_serving(args):
@@ -475,7 +703,7 @@ def run_serving(args):
                                               "worst": [dict(p, err=e) for e, p in
                                                         sorted(worst, key=lambda x: -x[0])[:3]]},
             "engine": st, "host_seconds": host, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_lte(args):
@@ -532,13 +760,7 @@ def run_lte(args):
     # SSP-RK3 trajectory at a fixed dt (acoustic CFL ~0.3 on the LGL spacing)
     h = 2 * np.pi / n / 16.0
     dt = 0.3 * h / (300.0 + 1100.0)
-    y = ud.clone()
-    ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ta.record(stream)
-    op.rk3_steps(y, dt, args.rk_steps)
-    tb.record(stream)
-    torch.cuda.synchronize()
-    rk_ms = ta.elapsed_time(tb)
+    rk_ms, y = timed_rk3(op, ud, dt, args.rk_steps, stream)
     rk_status = op.read_status()
     line = {"metric": "DOF*RHS/s (LTE Helmholtz gas, LTEEC)", "value": m.num_nodes / (ms * 1e-3),
             "unit": "DOF*RHS/s", "n_gpus": 1, "ms_per_step": ms, "dtype": "f64", "data": "synthetic",
@@ -551,7 +773,7 @@ def run_lte(args):
             "rk3": {"steps": args.rk_steps, "dt": dt, "ms": rk_ms, "status": rk_status,
                     "dof_rhs_per_s": 3 * args.rk_steps * m.num_nodes / (rk_ms * 1e-3)},
             "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_sedov(args):
@@ -592,13 +814,7 @@ def run_sedov(args):
         ph = np.mean([op.profile(ud, du) for _ in range(3)], axis=0)
         alpha, _ = op.blending_coefficients()
         dt = op.estimate_dt(ud, 0.5) if prec == "fp64" else out["fp64"]["rk3"]["dt"]
-        y = ud.clone()
-        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ta.record(stream)
-        op.rk3_steps(y, dt, args.sedov_steps)
-        tb.record(stream)
-        torch.cuda.synchronize()
-        rk_ms = ta.elapsed_time(tb)
+        rk_ms, y = timed_rk3(op, ud, dt, args.sedov_steps, stream)
         out[prec] = {"dof_rhs_per_s": m.num_nodes / (ms * 1e-3), "ms_per_rhs": ms,
                      "phase_ms": {"indicator": ph[0], "face": ph[2], "volume+fv": ph[3]},
                      "blended_fraction": float((alpha > 0).float().mean().item()),
@@ -647,7 +863,7 @@ def run_sedov(args):
             "blending_agreement_t0": agreement,
             "rhs_rel_l2_vs_oracle_4cubed": [float(x) for x in rel],
             "rhs_vs_oracle_note": "absolute L2 for fields whose oracle rate is zero (mass at rest)"}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_setup(args):
@@ -710,7 +926,7 @@ def run_setup(args):
             "max_rel_diff_vs_host_builder": diff,
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                          "peak_source": src, "algorithmic_bytes": read + written}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -724,10 +940,14 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
-    ap.add_argument("--workload", default="rhs", choices=["rhs", "serving", "lte", "sedov", "setup"],
-                    help="rhs: the headline RHS throughput; serving: the batched case stream; "
-                         "lte: the LTE-gas Taylor-Green vortex; sedov: the blended blast; "
-                         "setup: mesh set-up on the device")
+    ap.add_argument("--workload", default="rhs",
+                    choices=["rhs", "serving", "lte", "sedov", "setup", "vortex"],
+                    help="rhs: the headline RHS throughput (with compact results of vortex, "
+                         "sedov, lte and serving unless --no-workloads); serving: the batched "
+                         "case stream; lte: the LTE-gas Taylor-Green vortex; sedov: the blended "
+                         "blast; setup: mesh set-up on the device; vortex: the 2-D isentropic vortex")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="rhs: skip the other configurations")
     ap.add_argument("--sedov-n", type=int, default=64, help="sedov: elements per direction")
     ap.add_argument("--sedov-steps", type=int, default=300, help="sedov: SSP-RK3 steps")
     ap.add_argument("--lte-n", type=int, default=24, help="lte: elements per direction")
@@ -738,16 +958,12 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "serving":
-        run_serving(args)
-    elif args.workload == "lte":
-        run_lte(args)
-    elif args.workload == "sedov":
-        run_sedov(args)
-    elif args.workload == "setup":
-        run_setup(args)
-    else:
+    elif args.workload == "rhs":
         run_ours(args)
+    else:
+        fn = {"serving": run_serving, "lte": run_lte, "sedov": run_sedov, "setup": run_setup,
+              "vortex": run_vortex}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
 
 
 if __name__ == "__main__":

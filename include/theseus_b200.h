@@ -286,13 +286,28 @@ int thx_rhs(thx_handle h, const void *u, void *dudt, void *stream);
  * handle: geom holds DEVICE pointers in the thx_geometry layout (full per-node
  * arrays), u and dudt are device FP64 L-vectors.  Euler flow, FP64, no
  * blending (else THX_ERR_UNSUPPORTED).  Its scratch (face fluxes, element-to-face
- * table, operators) is one static 8 MiB device array per GPU, kept until the
- * process exits: meshes needing more return THX_ERR_INVALID_ARGUMENT.  The
- * first call on a device looks the array up (make it before any stream
- * capture); every call rewrites what it reads, and calls that overlap on the
- * GPU race on the shared array. */
+ * table, checked copies of the face tables, operators) is one static 8 MiB
+ * device array per GPU, kept until the process exits: meshes needing more
+ * return THX_ERR_INVALID_ARGUMENT.  The first call on a device looks the array
+ * up (make it before any stream capture); every call rewrites what it reads,
+ * and calls that overlap on the GPU race on the shared array.
+ * status (may be NULL): a caller-owned word in device or page-locked host
+ * memory that receives, stream-ordered, this call's THX_STATUS_* bits --
+ * THX_STATUS_NONPOSITIVE for a non-positive density or pressure,
+ * THX_STATUS_LAUNCH when the volume kernel could not run,
+ * THX_STATUS_FACE_TABLE when a face_elem/face_lface entry is out of range
+ * (that face's fluxes are NaN and nothing outside the arrays is touched).
+ * Read it after the stream has synchronised. */
 int thx_rhs_euler_noalloc(const thx_geometry *geom_dev, const thx_config *cfg,
-                          const double *u, double *dudt, void *stream);
+                          const double *u, double *dudt, unsigned int *status, void *stream);
+
+/* FP64 fused-multiply-add throughput of the current device (no counterpart in
+ * the reference): eight independent FMA chains per thread on eight 256-thread
+ * CTAs per SM, `iters` rounds of 64 FMAs each, the best of `repeats` timed
+ * launches after one warm-up, CUDA events on `stream`.  *flops_per_s counts an
+ * FMA as two operations.  The denominator of the FP64-pipe roofline of the
+ * flux-differencing kernels. */
+int thx_measure_fp64_fma_peak(int iters, int repeats, double *flops_per_s, void *stream);
 
 /* Right-hand sides of n states held in HOST memory: dudt_host[i] = L(u_host[i])
  * (FP64 L-vectors; in FP32-mixed mode each state is evaluated as thx_rhs does).
@@ -433,6 +448,7 @@ int thx_integral_measures(thx_handle h, const double *u, double *out);
 #define THX_STATUS_NONFINITE 2u    /* non-finite value seen */
 #define THX_STATUS_LAUNCH 4u       /* a kernel got too little shared memory and did nothing */
 #define THX_STATUS_EOS 8u          /* LTE temperature recovery failed or left the table */
+#define THX_STATUS_FACE_TABLE 16u  /* a face table entry was out of range (thx_rhs_euler_noalloc) */
 int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
 
 /* ---- batch engine (no counterpart in the reference) -----------------------

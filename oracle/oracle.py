@@ -17,19 +17,22 @@ from theseus_b200._abi import Config, Geometry, make_config, FLOW_NAVIER_STOKES 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libthx_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libthx_ref.so")
+REF_NATIVE_PATH = os.path.join(HERE, "_ref", "libthx_ref_native.so")
+REF_NATIVE_FLAGS = os.path.join(HERE, "_ref", "native_cpu_flags.txt")
 
 _lib = None
 _ref = None
+_ref_native = None
 
 D = C.POINTER(C.c_double)
 I32 = C.POINTER(C.c_int32)
 
 
-def build(ref=False):
-    """Compile the oracle (and, if asked and the reference tree exists, _ref)."""
+def build(ref_include=None):
+    """Compile the oracle and, given the reference's include directory, _ref."""
     subprocess.check_call(["make", "-s", "-C", HERE])
-    if ref and os.path.isdir("/root/reference/include"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    if ref_include and os.path.isdir(ref_include):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={ref_include}"])
 
 
 def lib():
@@ -50,6 +53,31 @@ def ref():
     if _ref is None:
         _ref = C.CDLL(REF_PATH)
     return _ref
+
+
+def _cpu_flags():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_native():
+    """The -O3 -march=native build of the reference kernels (the timed CPU
+    baseline), or None when it was not built or this host lacks one of the
+    instruction-set flags of the host that built it."""
+    global _ref_native
+    if _ref_native is None:
+        if not (os.path.exists(REF_NATIVE_PATH) and os.path.exists(REF_NATIVE_FLAGS)):
+            return None
+        need = set(open(REF_NATIVE_FLAGS).read().split())
+        if not need or not need <= _cpu_flags():
+            return None
+        _ref_native = C.CDLL(REF_NATIVE_PATH)
+    return _ref_native
 
 
 def _dp(a):
@@ -317,8 +345,9 @@ def viscous_flux(cfg, dim, q, dprim, use_ref=False):
     return out.reshape(dim + 2, dim)
 
 
-def ref_rhs(mesh, cfg, u, alpha=None):
-    """Full RHS through the reference's own point kernels (oracle/_ref)."""
+def ref_rhs(mesh, cfg, u, alpha=None, native=False):
+    """Full RHS through the reference's own point kernels (oracle/_ref; with
+    native=True the -O3 -march=native build, which must be available)."""
     x, w, Dm, Dh, Dh2 = operators(mesh.order)
     u = np.ascontiguousarray(u, dtype=np.float64)
     du = np.zeros_like(u)
@@ -326,7 +355,8 @@ def ref_rhs(mesh, cfg, u, alpha=None):
     if alpha is not None:
         xi, eta, zeta = subcell_metrics(mesh, cfg)
         alpha = np.ascontiguousarray(alpha, np.float64)
-    _check(ref().ref_rhs(C.byref(mesh.struct()), C.byref(cfg), _dp(Dm), _dp(Dh), _dp(Dh2), _dp(w),
+    L = ref_native() if native else ref()
+    _check(L.ref_rhs(C.byref(mesh.struct()), C.byref(cfg), _dp(Dm), _dp(Dh), _dp(Dh2), _dp(w),
                          _dp(alpha), _dp(xi), _dp(eta), _dp(zeta), _dp(u), _dp(du)), "ref_rhs")
     return du
 

@@ -9,14 +9,16 @@ Each golden entry is one DG node of one visualisation subcell: keys are the
 subcell centre (x, y) and the node (x, y); fields are density, pressure and
 velocity there.  Every other entry is kept (the file stays small; every
 element and every node position is still represented).  Run from the
-repository root with the reference tree at REF (default /root/reference).
+repository root with the reference tree at REF.
 """
 import os
 import sys
 
 import numpy as np
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
+if not REF:
+    sys.exit("set REF to the root of the reference tree")
 SRC = os.path.join(REF, "TestCases", "GoldenData", "NumericalFluxes")
 OUT = os.path.dirname(os.path.abspath(__file__))
 

@@ -9,7 +9,7 @@ element blocks of (p+1)^2 points, with binary arrays written as base64 of a
 uint32 byte count followed by the data.  Stored per point: the element
 centre (mean of its block), the point, density, pressure, velocity and the
 blending coefficient.  Run from the repository root with the reference tree
-at REF (default /root/reference)."""
+at REF."""
 import base64
 import os
 import re
@@ -17,7 +17,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
+if not REF:
+    sys.exit("set REF to the root of the reference tree")
 SRC = os.path.join(REF, "TestCases", "GoldenData", "LidDrivenCavity", "Cycle004000")
 OUT = os.path.dirname(os.path.abspath(__file__))
 NODES = 16  # (p+1)^2 at p = 3

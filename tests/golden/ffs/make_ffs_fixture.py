@@ -9,7 +9,7 @@ vertex ids and named boundary lines, and for a subset of the golden's
 elements -- every element with a non-zero blending coefficient and every
 32nd other one, in the file's element order -- the points, element centres,
 density, pressure, velocity and blending coefficient.  Run from the
-repository root with the reference tree at REF (default /root/reference)."""
+repository root with the reference tree at REF."""
 import base64
 import io
 import os
@@ -19,7 +19,9 @@ import tarfile
 
 import numpy as np
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
+if not REF:
+    sys.exit("set REF to the root of the reference tree")
 OUT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(OUT, "..", "..", ".."))
 from theseus_b200.gmsh import read_gmsh  # noqa: E402

@@ -7,7 +7,7 @@ dt=1e-4, 100 steps, two ranks) and the mesh it ran on
 into tests/golden/tgv2d/tgv2d_p3_100.npz: the mesh as node coordinates, quad
 vertex ids and periodic node pairs, and per golden point the element centre,
 the point, density, pressure and velocity.  Run from the repository root with
-the reference tree at REF (default /root/reference)."""
+the reference tree at REF."""
 import base64
 import os
 import re
@@ -15,7 +15,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
+if not REF:
+    sys.exit("set REF to the root of the reference tree")
 OUT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(OUT, "..", "..", ".."))
 from theseus_b200.gmsh import read_gmsh  # noqa: E402

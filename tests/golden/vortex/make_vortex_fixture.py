@@ -7,8 +7,7 @@ ran on (3 x 3 periodic quads with first-order L2 nodes) into
 tests/golden/vortex/vortex_p3_500.npz: the mesh as element vertex ids, the
 vertex count and per-element corner coordinates, and per golden point the
 element centre, the point, density, pressure, velocity and blending
-coefficient.  Run from the repository root with the reference tree at REF
-(default /root/reference)."""
+coefficient.  Run from the repository root with the reference tree at REF."""
 import base64
 import os
 import re
@@ -16,7 +15,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF")
+if not REF:
+    sys.exit("set REF to the root of the reference tree")
 OUT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(OUT, "..", "..", ".."))
 from theseus_b200.mfem_mesh import read_mfem_mesh  # noqa: E402

@@ -213,3 +213,4 @@ STATUS_NONPOSITIVE = 1
 STATUS_NONFINITE = 2
 STATUS_LAUNCH = 4
 STATUS_EOS = 8
+STATUS_FACE_TABLE = 16

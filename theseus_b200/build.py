@@ -27,7 +27,7 @@ def units():
     u = [("thx_api.o", "thx_api.cu", []), ("thx_host.o", "thx_host.cpp", []),
          ("thx_lte_host.o", "thx_lte_host.cpp", []), ("thx_engine.o", "thx_engine.cu", []),
          ("thx_noalloc.o", "thx_noalloc.cu", []), ("thx_checkpoint.o", "thx_checkpoint.cpp", []),
-         ("thx_geometry.o", "thx_geometry.cu", [])]
+         ("thx_geometry.o", "thx_geometry.cu", []), ("thx_peak.o", "thx_peak.cu", [])]
     for dim in (2, 3):
         u.append((f"lte_face_{dim}.o", "thx_inst_lte.cu", [f"-DTHX_DIM={dim}"]))
         for n in ORDERS:

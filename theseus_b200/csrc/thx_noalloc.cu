@@ -13,6 +13,9 @@
 // The array is shared by all calls and keeps the previous call's contents, so
 // everything that must start from a known value is rewritten on every call.
 // Calls that overlap on the GPU (two streams, or two host threads) race on it.
+// Each call's status bits (non-positive state, a kernel that could not run, an
+// out-of-range face table entry) are copied, stream-ordered, to a word the
+// caller passes.
 #include "thx_launch.cuh"
 #include "thx_host.h"
 
@@ -61,18 +64,49 @@ __global__ void noalloc_fill_ops(const OpsParam p, double *dst) {
   for (int i = threadIdx.x; i < p.n; i += blockDim.x) dst[i] = p.v[i];
 }
 
-__global__ void noalloc_elem_face(int nf, int dim, const int *face_elem, const int *face_lface,
-                                  int *elem_face) {
+// Copies the face tables into the scratch array with every entry checked:
+// an entry whose element or local face is out of range is replaced by
+// (element 0, local face 0), which the face kernel can read without leaving
+// the state arrays, is left out of the element-to-face table, and sets
+// THX_STATUS_FACE_TABLE; noalloc_poison_bad_faces later gives such a face NaN fluxes.
+__global__ void noalloc_face_tables(int nf, int ne, int dim, const int *face_elem,
+                                    const int *face_lface, int *fe_ok, int *fl_ok, int *elem_face,
+                                    unsigned *status) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 2 * nf) return;
   const int f = t >> 1, s = t & 1;
-  elem_face[face_elem[t] * 2 * dim + face_lface[t]] = 2 * f + s;
+  const int e = face_elem[t], lf = face_lface[t];
+  if (e < 0 || e >= ne || lf < 0 || lf >= 2 * dim) {
+    fe_ok[t] = 0;
+    fl_ok[t] = 0;
+    atomicOr(status, THX_STATUS_FACE_TABLE);
+    return;
+  }
+  fe_ok[t] = e;
+  fl_ok[t] = lf;
+  elem_face[e * 2 * dim + lf] = 2 * f + s;
+}
+
+// NaN fluxes on every face with an out-of-range table entry (either side).
+__global__ void noalloc_poison_bad_faces(int nf, int ne, int dim, int nfp, int neq,
+                                         const int *face_elem, const int *face_lface,
+                                         double *fstar) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  bool bad = false;
+  for (int s = 0; s < 2; ++s) {
+    const int e = face_elem[2 * f + s], lf = face_lface[2 * f + s];
+    if (e < 0 || e >= ne || lf < 0 || lf >= 2 * dim) bad = true;
+  }
+  if (!bad) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  for (int i = 0; i < neq * nfp; ++i) fstar[(long long)f * neq * nfp + i] = nan;
 }
 
 }  // namespace
 
 extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cfg, const double *u,
-                                     double *dudt, void *stream) {
+                                     double *dudt, unsigned int *status_out, void *stream) {
   using namespace thx;
   if (!g || !cfg || !u || !dudt || !g->jac || !g->metric || !g->face_elem || !g->face_lface ||
       !g->face_normal || !g->face_wminus || !g->face_wplus)
@@ -90,12 +124,14 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   const int nd = dim == 2 ? N * N : N * N * N;
   const int nfp = dim == 2 ? N : N * N;
   const int neq = dim + 2, ne = g->num_elements, nf = g->num_faces;
-  // scratch layout: [ops][status][elem_face][face fluxes]
+  // scratch layout: [ops][status][elem_face][checked face tables][face fluxes]
   const size_t ops_bytes = round256(sizeof(double) * (2 * N * N + N));
   const size_t status_bytes = 256;
   const size_t ef_bytes = round256(sizeof(int) * (size_t)ne * 2 * dim);
+  const size_t ft_bytes = round256(sizeof(int) * (size_t)nf * 2);
   const size_t fs_bytes = round256(sizeof(double) * (size_t)nf * nfp * neq);
-  if (ops_bytes + status_bytes + ef_bytes + fs_bytes > kScratchBytes) return THX_ERR_INVALID_ARGUMENT;
+  if (ops_bytes + status_bytes + ef_bytes + 2 * ft_bytes + fs_bytes > kScratchBytes)
+    return THX_ERR_INVALID_ARGUMENT;
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return THX_ERR_NO_DEVICE; }
@@ -105,7 +141,9 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   double *ops = reinterpret_cast<double *>(base);
   unsigned *status = reinterpret_cast<unsigned *>(base + ops_bytes);
   int *elem_face = reinterpret_cast<int *>(base + ops_bytes + status_bytes);
-  double *fstar = reinterpret_cast<double *>(base + ops_bytes + status_bytes + ef_bytes);
+  int *fe_ok = reinterpret_cast<int *>(base + ops_bytes + status_bytes + ef_bytes);
+  int *fl_ok = reinterpret_cast<int *>(base + ops_bytes + status_bytes + ef_bytes + ft_bytes);
+  double *fstar = reinterpret_cast<double *>(base + ops_bytes + status_bytes + ef_bytes + 2 * ft_bytes);
   cudaStream_t s = (cudaStream_t)stream;
 
   // derivative operators (host arithmetic, passed by value)
@@ -123,7 +161,8 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   if (cudaMemsetAsync(status, 0, sizeof(unsigned), s) != cudaSuccess) return THX_ERR_CUDA;
   if (cudaMemsetAsync(elem_face, 0xff, sizeof(int) * (size_t)ne * 2 * dim, s) != cudaSuccess)
     return THX_ERR_CUDA;
-  noalloc_elem_face<<<(2 * nf + 255) / 256, 256, 0, s>>>(nf, dim, g->face_elem, g->face_lface, elem_face);
+  noalloc_face_tables<<<(2 * nf + 255) / 256, 256, 0, s>>>(nf, ne, dim, g->face_elem, g->face_lface,
+                                                           fe_ok, fl_ok, elem_face, status);
   if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
 
   // the same face and volume kernels as thx_rhs, on the full per-node layout
@@ -140,10 +179,13 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   FaceKernels0 fk = dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
   FaceArgs<double> fa;
   fa.u = u; fa.ne = ne; fa.nf = nf; fa.N = N;
-  fa.face_elem = g->face_elem; fa.face_lface = g->face_lface;
+  fa.face_elem = fe_ok; fa.face_lface = fl_ok;
   fa.normal = g->face_normal; fa.n_fs = nfp; fa.n_ps = 1;
   fa.vflux = nullptr; fa.fstar = fstar; fa.gas = gas;
   if (fk.face[cfg->surface_flux][0](fa, s) != cudaSuccess) return THX_ERR_CUDA;
+  noalloc_poison_bad_faces<<<(nf + 127) / 128, 128, 0, s>>>(nf, ne, dim, nfp, neq, g->face_elem,
+                                                             g->face_lface, fstar);
+  if (cudaGetLastError() != cudaSuccess) return THX_ERR_CUDA;
 
   const int vk = (cfg->volume_flux == THX_FLUX_CHANDRASHEKAR) ? VOL_CHANDRASHEKAR
                : (cfg->volume_flux == THX_FLUX_RANOCHA)     ? VOL_RANOCHA
@@ -168,5 +210,12 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
   va.fv_flux = cfg->fv_flux; va.gas = gas; va.ops = ops;
   va.stage = 0; va.status = status;
   if (vol(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
+  // the status word, stream-ordered, to the caller's device or page-locked
+  // host word
+  if (status_out &&
+      cudaMemcpyAsync(status_out, status, sizeof(unsigned), cudaMemcpyDefault, s) != cudaSuccess) {
+    cudaGetLastError();
+    return THX_ERR_CUDA;
+  }
   return THX_OK;
 }
