@@ -190,7 +190,7 @@ def cpu_rhs_fn():
     threads = O.max_threads()
     if O.ref_native() is not None:
         return (lambda om, cfg, u: O.ref_rhs(om, cfg, u, native=True)), "reference", threads, \
-            "reference headers, g++ -O3 -march=native, OpenMP"
+            f"reference headers, {O.ref_native.build}, OpenMP"
     if O.ref_available():
         try:
             O.ref()

@@ -19,6 +19,10 @@ LIB_PATH = os.path.join(HERE, "libthx_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libthx_ref.so")
 REF_NATIVE_PATH = os.path.join(HERE, "_ref", "libthx_ref_native.so")
 REF_NATIVE_FLAGS = os.path.join(HERE, "_ref", "native_cpu_flags.txt")
+REF_V4_PATH = os.path.join(HERE, "_ref", "libthx_ref_v4.so")
+# instruction-set flags that -march=x86-64-v4 assumes beyond v3 (AVX-512 F/BW/CD/DQ/VL)
+V4_FLAGS = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl", "avx2", "fma", "bmi1",
+            "bmi2", "movbe", "f16c"}
 
 _lib = None
 _ref = None
@@ -66,18 +70,25 @@ def _cpu_flags():
 
 
 def ref_native():
-    """The -O3 -march=native build of the reference kernels (the timed CPU
-    baseline), or None when it was not built or this host lacks one of the
-    instruction-set flags of the host that built it."""
+    """The optimised build of the reference kernels that this host can run
+    (the timed CPU baseline): -O3 -march=native when this host has every
+    instruction-set flag of the host that built it, else -O3 -march=x86-64-v4
+    on an AVX-512 host, else None.  Sets ref_native.build to its flags."""
     global _ref_native
     if _ref_native is None:
-        if not (os.path.exists(REF_NATIVE_PATH) and os.path.exists(REF_NATIVE_FLAGS)):
-            return None
-        need = set(open(REF_NATIVE_FLAGS).read().split())
-        if not need or not need <= _cpu_flags():
-            return None
-        _ref_native = C.CDLL(REF_NATIVE_PATH)
+        have = _cpu_flags()
+        if os.path.exists(REF_NATIVE_PATH) and os.path.exists(REF_NATIVE_FLAGS):
+            need = set(open(REF_NATIVE_FLAGS).read().split())
+            if need and need <= have:
+                _ref_native = C.CDLL(REF_NATIVE_PATH)
+                ref_native.build = "g++ -O3 -march=native (the build host's CPU)"
+        if _ref_native is None and os.path.exists(REF_V4_PATH) and V4_FLAGS <= have:
+            _ref_native = C.CDLL(REF_V4_PATH)
+            ref_native.build = "g++ -O3 -march=x86-64-v4"
     return _ref_native
+
+
+ref_native.build = None
 
 
 def _dp(a):

@@ -222,9 +222,11 @@ void pick_face_kernels(thx_operator_s *h) {
     FaceKernels0 k = h->dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
     h->face64 = k.face[s][ns];
     h->bnd64 = k.bnd[s][ns];
+    h->ent64 = k.entropy;
   } else {
     FaceKernels1 k = h->dim == 2 ? face_kernels_1_2() : face_kernels_1_3();
     h->face32 = k.face[s][ns];
+    h->ent32 = k.entropy;
   }
 }
 
@@ -401,6 +403,15 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   if ((st = upload(&h->face_elem, g->face_elem, (size_t)2 * h->nf, A))) return st;
   if ((st = upload(&h->face_lface, g->face_lface, (size_t)2 * h->nf, A))) return st;
   {
+    // face-kernel processing order: interior faces by minus-side element
+    // (stable), so that the CTAs in flight gather from a narrow element window
+    std::vector<int> order(h->nf);
+    for (int f = 0; f < h->nf; ++f) order[f] = f;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return g->face_elem[2 * x] < g->face_elem[2 * y]; });
+    if ((st = upload(&h->face_order, order.data(), order.size(), A))) return st;
+  }
+  {
     std::vector<int> ef((size_t)h->ne * 2 * dim, -1);
     for (int f = 0; f < h->nf; ++f)
       for (int s = 0; s < 2; ++s) {
@@ -450,6 +461,7 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if ((st = dev_alloc(&p, fsz, A))) return st;
     h->fstar = p;
     if (h->ns) { if ((st = dev_alloc(&p, (size_t)dim * (h->neq - 1) * h->L, A))) return st; h->vflux = p; }
+    if (h->ns && !h->lte) { if ((st = dev_alloc(&p, (size_t)h->neq * h->L, A))) return st; h->svars = p; }
   }
   if ((st = dev_alloc(&h->status, 1, A))) return st;
   if ((st = dev_alloc(&h->stab, 3, A))) return st;
@@ -551,6 +563,8 @@ Geo<float> geo(thx_operator_s *h, float *) {
 }
 VolLaunch<double> volk(thx_operator_s *h, double *) { return h->vol64; }
 VolLaunch<float> volk(thx_operator_s *h, float *) { return h->vol32; }
+EntropyLaunch<double> entk(thx_operator_s *h, double *) { return h->ent64; }
+EntropyLaunch<float> entk(thx_operator_s *h, float *) { return h->ent32; }
 GradLaunch<double> gradk(thx_operator_s *h, double *) { return h->grad64; }
 GradLaunch<float> gradk(thx_operator_s *h, float *) { return h->grad32; }
 BlendLaunch<double> blendk(thx_operator_s *h, double *) { return h->blend64; }
@@ -582,6 +596,7 @@ void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double 
   ga.normal = G.nrm; ga.n_fs = h->lay.n_fs; ga.n_ps = h->lay.n_ps;
   ga.wm = G.wm; ga.wp = G.wp; ga.w_fs = h->lay.w_fs; ga.w_ps = h->lay.w_ps;
   ga.D = G.D; ga.gas = g; ga.status = h->status;
+  ga.svars = reinterpret_cast<const R *>(h->svars);
   ga.nf_int = h->nf;
   if constexpr (IsF32<R>::value) {
     ga.bw = nullptr;
@@ -595,6 +610,7 @@ void op_args(thx_operator_s *h, const R *u, R *du, int stage, double dt, double 
   fa.face_elem = h->face_elem; fa.face_lface = h->face_lface;
   fa.normal = G.nrm; fa.n_fs = h->lay.n_fs; fa.n_ps = h->lay.n_ps;
   fa.vflux = vfl; fa.fstar = fst; fa.gas = g;
+  fa.order = h->face_order;
   va = VolArgs<R>{};
   va.u = u; va.du = du; va.ne = h->ne;
   va.jac = G.jac; va.jac_es = h->lay.jac_es; va.jac_ns = h->lay.jac_ns;
@@ -658,6 +674,11 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     if (blendk(h, tag)(b, s) != cudaSuccess) return THX_ERR_CUDA;
   }
   if (ev) cudaEventRecord(ev[1], s);
+  // FP64 Navier-Stokes (ideal gas): the entropy variables of every node
+  // first, read by the gradient kernel
+  if (h->svars &&
+      entk(h, tag)(u, h->L, gas(h, tag), reinterpret_cast<R *>(h->svars), s) != cudaSuccess)
+    return THX_ERR_CUDA;
   if (h->ns && gradk(h, tag)(ga, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[2], s);
   if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;

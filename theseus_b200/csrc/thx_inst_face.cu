@@ -26,6 +26,7 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
   THX_SET(SURF_LLF)
   THX_SET(SURF_ROE)
 #undef THX_SET
+  k.entropy = &launch_entropy<R, THX_DIM>;
 #if THX_PREC == 0
 #define THX_SETBND(S)                                   \
   k.bnd[S][0] = &launch_bnd<THX_DIM, S, false>;          \

@@ -35,7 +35,11 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   k.vol[VOL_CENTRAL][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false, true>;
   k.vol[VOL_CENTRAL][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, false>;
   k.vol[VOL_CENTRAL][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, true>;
-  k.grad = &launch_grad<R, THX_DIM, THX_N>;
+#if THX_PREC == 0
+  k.grad = &launch_grad_sv<R, THX_DIM, THX_N>;  // FP64: entropy variables precomputed
+#else
+  k.grad = &launch_grad<R, THX_DIM, THX_N>;     // FP32: evaluated in the kernel (cheaper)
+#endif
   k.blend = &launch_blend<R, THX_DIM, THX_N>;
   k.fv = &launch_fv<R, THX_DIM, THX_N>;
 #define THX_SETB(V)                                                              \

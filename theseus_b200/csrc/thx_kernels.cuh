@@ -590,9 +590,14 @@ struct FaceArgs {
   const R *vflux;
   R *fstar;
   GasT<R> gas;
+  // processing order of the faces (nullptr: face order): faces sorted by
+  // their minus-side element, so that the traces the CTAs in flight gather
+  // belong to a narrow window of elements and come from L2 (in face order
+  // the x-, y- and z-faces each sweep all of u and of the viscous flux)
+  const int *order;
 };
 
-// Face point t (face t / nfp, point t % nfp) of one case.
+// Face point t (face order[t / nfp], point t % nfp) of one case.
 template <typename R, int DIM, int SURF, bool NS>
 __device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long t) {
   constexpr int NEQ = DIM + 2;
@@ -600,7 +605,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long 
   const int nfp = DIM == 2 ? N : N * N;
   const int nd = DIM == 2 ? N * N : N * N * N;
   if (t >= (long long)a.nf * nfp) return;
-  const int f = (int)(t / nfp), fp = (int)(t % nfp);
+  const int fi = (int)(t / nfp), fp = (int)(t % nfp);
+  const int f = a.order ? a.order[fi] : fi;
   const long long L = (long long)a.ne * nd;
   const int em = a.face_elem[2 * f], ep = a.face_elem[2 * f + 1];
   const long long im = (long long)em * nd + trace_node<DIM>(N, a.face_lface[2 * f], fp);
@@ -664,6 +670,7 @@ struct GradArgs {
   long long w_fs, w_ps;
   const R *D;  // N*N
   GasT<R> gas;
+  const R *svars;  // entropy variables of every node [eq][elem][node] (SV kernels)
   unsigned *status;
   // boundary faces (FP64 ideal gas; bw == nullptr: none): face slots
   // nf_int + b, lift weights bw[b][fp], outward normals bnrm[b][fp][dim],
@@ -682,9 +689,30 @@ __host__ __device__ constexpr size_t grad_smem_bytes() {
   return sizeof(R) * (S::DPAD + (size_t)S::EPB * S::NEQ * (S::ND + 2 * DIM * S::NFP));
 }
 
+// Entropy variables of every node (include/EOS.hpp:206-234, as
+// include/NSOperator_impl.hpp:11-78 forms them), written once per right-hand
+// side: the gradient kernel reads its nodes and its neighbours' face traces
+// from here instead of evaluating them (2.2 evaluations per node, each two
+// logarithms and seven divisions).
+template <typename R, int DIM>
+__global__ void __launch_bounds__(256) entropy_kernel(const R *__restrict__ u, long long L,
+                                                      const GasT<R> gas, R *__restrict__ sv) {
+  constexpr int NEQ = DIM + 2;
+  const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (i >= L) return;
+  R raw[NEQ], q[NEQ], w[NEQ];
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) raw[k] = u[k * L + i];
+  reconstruct<R, DIM>(gas, raw, q);
+  entropy_vars<R, DIM>(gas, q, w);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) sv[k * L + i] = w[k];
+}
+
 // BR1 gradient (include/NSOperator_impl.hpp:11-159,194-517;
-// include/DGSEMIntegrator.hpp:764-850,1011-1044)
-template <typename R, int DIM, int N, bool LTE>
+// include/DGSEMIntegrator.hpp:764-850,1011-1044).  SV: the entropy variables
+// come from a.svars (entropy_kernel) instead of being evaluated here.
+template <typename R, int DIM, int N, bool LTE, bool SV = false>
 __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block) {
   static_assert(!LTE || !IsF32<R>::value, "LTE gas: FP64 only");
   using S = Shape<DIM, N>;
@@ -711,8 +739,14 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
     for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
     reconstruct<R, DIM>(a.gas, raw, q);
     R w[NEQ];
-    if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, q, a.gas.Tn[(long long)e * ND + n], w);
-    else entropy_vars<R, DIM>(a.gas, q, w);
+    if constexpr (SV) {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) w[k] = a.svars[k * L + (long long)e * ND + n];
+    } else if constexpr (LTE) {
+      lte_entropy_vars<DIM>(a.gas.lte, q, a.gas.Tn[(long long)e * ND + n], w);
+    } else {
+      entropy_vars<R, DIM>(a.gas, q, w);
+    }
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) sS[(el * NEQ + k) * ND + n] = w[k];
   }
@@ -728,12 +762,18 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
     if (a.bw && f >= a.nf_int) continue;  // boundary face: no neighbour
     const int eo = a.face_elem[2 * f + 1 - side];
     const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
-    R ro[NEQ], qo[NEQ], so[NEQ];
+    R so[NEQ];
+    if constexpr (SV) {
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
-    reconstruct<R, DIM>(a.gas, ro, qo);
-    if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], so);
-    else entropy_vars<R, DIM>(a.gas, qo, so);
+      for (int k = 0; k < NEQ; ++k) so[k] = a.svars[k * L + (long long)eo * ND + no];
+    } else {
+      R ro[NEQ], qo[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
+      reconstruct<R, DIM>(a.gas, ro, qo);
+      if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], so);
+      else entropy_vars<R, DIM>(a.gas, qo, so);
+    }
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) sN[((tel * NLF + lf) * NEQ + k) * NFP + fp] = so[k];
   }
@@ -889,9 +929,253 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
   }
 }
 
-template <typename R, int DIM, int N, bool LTE>
+// Shared memory of the gradient kernel that reads precomputed entropy
+// variables: D | own entropy variables [EPB][NEQ][ND] | own conserved state
+// [EPB][NEQ][ND] | lift data [EPB][2*DIM][NEQ+1+DIM][NFP] (the jump -- or the
+// boundary flux --, the weight and the normal of every face point) | face
+// kinds [EPB][2*DIM] (0 none, 1 interior, 2 boundary).
+template <typename R, int DIM, int N>
+__host__ __device__ constexpr size_t grad_sv_smem_bytes() {
+  using S = Shape<DIM, N>;
+  return sizeof(R) * (S::DPAD + 2 * (size_t)S::EPB * S::NEQ * S::ND +
+                      (size_t)S::EPB * 2 * DIM * (S::NEQ + 1 + DIM) * S::NFP) +
+         sizeof(int) * (size_t)S::EPB * 2 * DIM;
+}
+
+// The BR1 gradient of grad_body with the entropy variables read from a.svars
+// and the work laid out for fewer registers: the face-point tasks stage each
+// lift term's factors -- the jump 0.5 (S+ - S-) of interior faces or the
+// boundary flux of bc_grad_flux, the weight and the normal -- in shared
+// memory, and each node then forms w (jump n_c) per (component, variable),
+// sums its faces' terms in face order and adds the sum, as grad_body does;
+// the reference-direction derivatives are folded into the physical gradient
+// one direction at a time, and the viscous flux is stored as it is formed.
+// Same operations in the same order as grad_body, so the results are
+// identical.
+template <typename R, int DIM, int N>
+__device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int block) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NFP = S::NFP, NLF = 2 * DIM;
+  constexpr int NJ = NEQ + 1 + DIM;  // jump, weight, normal per face point
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded)
+  R *sS = sD + S::DPAD;                      // [EPB][NEQ][ND]
+  R *sQ = sS + EPB * NEQ * ND;               // [EPB][NEQ][ND]
+  R *sJ = sQ + EPB * NEQ * ND;               // [EPB][NLF][NJ][NFP]
+  int *sK = reinterpret_cast<int *>(sJ + EPB * NLF * NJ * NFP);  // [EPB][NLF]
+  if (dynamic_smem_bytes() < grad_sv_smem_bytes<R, DIM, N>()) {
+    if (threadIdx.x == 0 && a.status) atomicOr(a.status, STATUS_LAUNCH);
+    return;
+  }
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N * N; i += blockDim.x) sD[i] = a.D[i];
+  const int el = tid / ND, n = tid % ND;
+  const int e0 = block * EPB;
+  const int e = e0 + el;
+  const bool active = (el < EPB) && (e < a.ne);
+  const long long L = (long long)a.ne * ND;
+  if (active) {
+    R raw[NEQ], q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      raw[k] = a.u[k * L + (long long)e * ND + n];
+      sS[(el * NEQ + k) * ND + n] = a.svars[k * L + (long long)e * ND + n];
+    }
+    reconstruct<R, DIM>(a.gas, raw, q);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
+  }
+  for (int t = tid; t < EPB * NLF; t += blockDim.x) {
+    const int te = e0 + t / NLF;
+    int kind = 0;
+    if (te < a.ne) {
+      const int fs = a.elem_face[te * NLF + t % NLF];
+      if (fs >= 0) kind = (a.bw && (fs >> 1) >= a.nf_int) ? 2 : 1;
+    }
+    sK[t] = kind;
+  }
+  __syncthreads();
+  // lift factors of every face point of the CTA's elements
+  for (int t = tid; t < EPB * NLF * NFP; t += blockDim.x) {
+    const int tel = t / (NLF * NFP), lf = (t / NFP) % NLF, fp = t % NFP;
+    const int te = e0 + tel;
+    if (te >= a.ne) continue;
+    const int fs = a.elem_face[te * NLF + lf];
+    if (fs < 0) continue;
+    const int f = fs >> 1, side = fs & 1;
+    const int nown = trace_node<DIM>(N, lf, fp);
+    R *dst = sJ + ((tel * NLF + lf) * NJ) * NFP + fp;
+    if (a.bw && f >= a.nf_int) {
+      // boundary face (include/NSOperator_impl.hpp:285-404,
+      // include/DGSEMIntegrator.hpp:1068-1094): w_b (exterior - interior) n_c
+      if constexpr (!IsF32<R>::value) {
+        const int b = f - a.nf_int;
+        const long long bp = (long long)b * NFP + fp;
+        R w[NEQ], fl[NEQ];
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) w[k] = sS[(tel * NEQ + k) * ND + nown];
+        bc_grad_flux<DIM>(a.gas, a.bcs[a.bdr_bc[b]], a.bc_data, w, fl);
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) dst[k * NFP] = fl[k];
+        dst[NEQ * NFP] = a.bw[bp];
+#pragma unroll
+        for (int cc = 0; cc < DIM; ++cc) dst[(NEQ + 1 + cc) * NFP] = a.bnrm[bp * DIM + cc];
+      }
+      continue;
+    }
+    // interior face: w * 0.5 (S+ - S-) n_c
+    const int eo = a.face_elem[2 * f + 1 - side];
+    const int no = trace_node<DIM>(N, a.face_lface[2 * f + 1 - side], fp);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      const R so = a.svars[k * L + (long long)eo * ND + no];
+      const R sown = sS[(tel * NEQ + k) * ND + nown];
+      dst[k * NFP] = side == 0 ? R(0.5) * (so - sown) : R(0.5) * (sown - so);
+    }
+    const long long wi = (long long)f * a.w_fs + (long long)fp * a.w_ps;
+    dst[NEQ * NFP] = side == 0 ? a.wm[wi] : a.wp[wi];
+    const R *nr = a.normal + ((long long)f * a.n_fs + (long long)fp * a.n_ps) * DIM;
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc) dst[(NEQ + 1 + cc) * NFP] = nr[cc];
+  }
+  __syncthreads();
+  if (!active) return;
+  int c[3];
+  node_coords<DIM, N>(n, c);
+  const R *adj = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
+  // physical gradient: sum over directions of D-derivative x adjugate row
+  R g[DIM][NEQ];
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const int me = c[dir];
+    const int line = line_of<DIM, N>(dir, c);
+    R dr[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) dr[k] = R(0);
+    // rolled: an unrolled contraction keeps all N*NEQ operands in flight
+#pragma unroll 1
+    for (int l = 0; l < N; ++l) {
+      const int s = line_node<DIM, N>(dir, line, l);
+      const R co = sD[me * N + l];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) dr[k] += sS[(el * NEQ + k) * ND + s] * co;
+    }
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc) {
+      const R ar = adj[dir * DIM + cc];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        if (dir == 0) g[cc][k] = dr[k] * ar;
+        else g[cc][k] += dr[k] * ar;
+      }
+    }
+  }
+  {
+    const R invJ = R(1) / a.jac[(long long)e * a.jac_es + (long long)n * a.jac_ns];
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) g[cc][k] = invJ * g[cc][k];
+  }
+  // lift: interior faces summed, then added; then the boundary faces
+  int jb[DIM], kinds[DIM];
+  bool any_i = false, any_b = false;
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const int me = c[dir];
+    const bool tr = me == 0 || me == N - 1;
+    const int lf = 2 * dir + (me == N - 1 ? 1 : 0);
+    kinds[dir] = tr ? sK[el * NLF + lf] : 0;
+    jb[dir] = ((el * NLF + lf) * NJ) * NFP + face_point<DIM, N>(dir, c);
+    any_i |= kinds[dir] == 1;
+    any_b |= kinds[dir] == 2;
+  }
+#pragma unroll
+  for (int pass = 1; pass <= 2; ++pass) {
+    if (!(pass == 1 ? any_i : any_b)) continue;
+#pragma unroll
+    for (int cc = 0; cc < DIM; ++cc)
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        R acc = R(0);
+#pragma unroll
+        for (int dir = 0; dir < DIM; ++dir)
+          if (kinds[dir] == pass) {
+            const R *j = sJ + jb[dir];
+            acc += j[NEQ * NFP] * (j[k * NFP] * j[(NEQ + 1 + cc) * NFP]);
+          }
+        g[cc][k] += acc;
+      }
+  }
+  // entropy gradient -> primitive gradient (in place), then the physical
+  // viscous flux (include/NavierStokesFlux.hpp:160-290), stored as formed
+  const R *q = sQ + el * NEQ * ND + n;  // q[k * ND]
+  R qv[NEQ];
+#pragma unroll
+  for (int cc = 0; cc < DIM; ++cc) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) qv[k] = q[k * ND];
+    R dpc[NEQ];
+    grad_entropy_to_prim<R, DIM>(a.gas, qv, g[cc], dpc);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) g[cc][k] = dpc[k];
+  }
+  const R *dp = &g[0][0];  // dp[d*NEQ + eq]
+  constexpr int NV = NEQ - 1, E = DIM + 1;
+  const long long base = (long long)e * ND + n;
+  {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) qv[k] = q[k * ND];
+    const R mu = viscosity<R, DIM>(a.gas, qv);
+    const R kappa = mu * a.gas.cp * a.gas.Pr_inv;
+    const R rho = qv[0];
+    const R p = pressure<R, DIM>(a.gas, qv);
+    const R pressor = fdiv(p, rho);
+    const R fac = fdiv(a.gas.gm1_inv, a.gas.cv * rho);
+    R div = R(0);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) div += dp[i * NEQ + 1 + i];
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+      R ef = kappa * (fac * (dp[dir * NEQ + E] - pressor * dp[dir * NEQ + 0]));
+#pragma unroll
+      for (int mom = 0; mom < DIM; ++mom) {
+        R tau;
+        if (mom == dir) tau = mu * (R(2) * dp[dir * NEQ + 1 + mom] - a.gas.mu_bulk * div);
+        else tau = mu * (dp[dir * NEQ + 1 + mom] + dp[mom * NEQ + 1 + dir]);
+        a.vflux[((long long)dir * NV + mom) * L + base] = tau;
+        ef += fdiv(q[(1 + mom) * ND], rho) * tau;
+      }
+      a.vflux[((long long)dir * NV + DIM) * L + base] = ef;
+    }
+  }
+  // primitive gradients at this node's boundary points, for the viscous
+  // boundary fluxes
+  if constexpr (!IsF32<R>::value) {
+    if (any_b) {
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir) {
+        if (kinds[dir] != 2) continue;
+        const int me = c[dir];
+        const int fs = a.elem_face[e * NLF + 2 * dir + (me == N - 1 ? 1 : 0)];
+        const long long bp = (long long)((fs >> 1) - a.nf_int) * NFP + face_point<DIM, N>(dir, c);
+#pragma unroll
+        for (int i = 0; i < DIM * NEQ; ++i) a.bgrad[bp * DIM * NEQ + i] = dp[i];
+      }
+    }
+  }
+}
+
+template <typename R, int DIM, int N, bool LTE, bool SV = false>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
-  grad_body<R, DIM, N, LTE>(a, blockIdx.x);
+  grad_body<R, DIM, N, LTE, SV>(a, blockIdx.x);
+}
+
+// The gradient kernel that reads precomputed entropy variables, bounded to
+// three CTAs per SM (four spill about 230 bytes per thread at 64 registers).
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 3) grad_sv_kernel(const GradArgs<R> a) {
+  grad_body_sv<R, DIM, N>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -69,11 +69,36 @@ cudaError_t launch_grad(const GradArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
   constexpr size_t smem = grad_smem_bytes<R, DIM, N>();
   if (prepare)
-    return cudaFuncSetAttribute(grad_kernel<R, DIM, N, LTE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    return cudaFuncSetAttribute(grad_kernel<R, DIM, N, LTE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (a.ne <= 0) return cudaSuccess;
   const int grid = (a.ne + S::EPB - 1) / S::EPB;
   grad_kernel<R, DIM, N, LTE><<<grid, S::THREADS, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+// Gradient from precomputed entropy variables (a.svars, entropy_kernel).
+template <typename R, int DIM, int N>
+cudaError_t launch_grad_sv(const GradArgs<R> &a, cudaStream_t s, int prepare) {
+  using S = Shape<DIM, N>;
+  constexpr size_t smem = grad_sv_smem_bytes<R, DIM, N>();
+  if (prepare)
+    return cudaFuncSetAttribute(grad_sv_kernel<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+  if (a.ne <= 0) return cudaSuccess;
+  if (!a.svars) return cudaErrorInvalidValue;
+  const int grid = (a.ne + S::EPB - 1) / S::EPB;
+  grad_sv_kernel<R, DIM, N><<<grid, S::THREADS, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R>
+using EntropyLaunch = cudaError_t (*)(const R *, long long, const GasT<R> &, R *, cudaStream_t);
+
+template <typename R, int DIM>
+cudaError_t launch_entropy(const R *u, long long L, const GasT<R> &g, R *sv, cudaStream_t s) {
+  if (L <= 0) return cudaSuccess;
+  entropy_kernel<R, DIM><<<(unsigned)((L + 255) / 256), 256, 0, s>>>(u, L, g, sv);
   return cudaGetLastError();
 }
 
@@ -166,6 +191,7 @@ struct FaceKernelsT {
   FaceLaunch<R> face[6][2];      // [surface flux][ns]
   FaceBatchLaunch<R> faceb[6][2];
   BndLaunch bnd[6][2];           // boundary faces [surface flux][ns] (FP64)
+  EntropyLaunch<R> entropy;      // entropy variables of every node (NS)
 };
 using OrderKernels0 = OrderKernelsT<double>;
 using OrderKernels1 = OrderKernelsT<float>;

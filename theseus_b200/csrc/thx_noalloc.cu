@@ -177,7 +177,7 @@ extern "C" int thx_rhs_euler_noalloc(const thx_geometry *g, const thx_config *cf
     return r;
   }();
   FaceKernels0 fk = dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
-  FaceArgs<double> fa;
+  FaceArgs<double> fa{};  // value-initialised: order (face processing order) stays null
   fa.u = u; fa.ne = ne; fa.nf = nf; fa.N = N;
   fa.face_elem = fe_ok; fa.face_lface = fl_ok;
   fa.normal = g->face_normal; fa.n_fs = nfp; fa.n_ps = 1;

@@ -119,6 +119,8 @@ struct thx_operator_s {
   float *sub32[3] = {nullptr, nullptr, nullptr}, *ops32 = nullptr, *D32 = nullptr;
   int *face_elem = nullptr, *face_lface = nullptr, *elem_face = nullptr;
   void *fstar = nullptr, *vflux = nullptr;  // face fluxes; NS physical viscous flux
+  void *svars = nullptr;     // FP64 NS (ideal gas): entropy variables of every node
+  int *face_order = nullptr; // interior faces sorted by their minus-side element
   double *alpha = nullptr, *eta = nullptr, *vinv = nullptr;
   void *fvrate = nullptr;  // subcell FV rate of blended elements (blending only)
   // boundary faces: face slots nf .. nf+nbf-1 of fstar/elem_face
@@ -138,6 +140,8 @@ struct thx_operator_s {
   thx::BlendLaunch<double> blend64 = nullptr;
   thx::VolLaunch<double> fv64 = nullptr;
   thx::FaceLaunch<double> face64 = nullptr;
+  thx::EntropyLaunch<double> ent64 = nullptr;
+  thx::EntropyLaunch<float> ent32 = nullptr;
   thx::BndLaunch bnd64 = nullptr;   // boundary faces (FP64 Euler)
   thx::VolLaunch<float> vol32 = nullptr;
   thx::GradLaunch<float> grad32 = nullptr;
