@@ -330,7 +330,7 @@ def run_ours(args):
     m, u = build_case()
     prec = "fp32" if args.precision == "fp32" else "fp64"
     op = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"], surface_flux=WORKLOAD["surface_flux"],
-                      precision=prec, **physics())
+                      precision=prec, volume_staging=args.volume_staging, **physics())
     ud = torch.as_tensor(u, device="cuda").to(op.dtype).contiguous()
     du = torch.empty_like(ud)
     stream = torch.cuda.current_stream()
@@ -413,9 +413,23 @@ def run_ours(args):
                                "flops": vflops, "fp64_fma_peak_tflops": fp64_tf,
                                "pair_evals_per_s": pairs / (phases[3] * 1e-3)}
 
+    # the volume kernel with its element blocks' state staged by bulk copy
+    # (cp.async.bulk into a double buffer, persistent CTAs) against the
+    # default form, same state, per-kernel CUDA events
+    extra = {}
+    if prec == "fp64" and args.volume_staging == 0 and not args.no_mixed:
+        alt = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"],
+                           surface_flux=WORKLOAD["surface_flux"], volume_staging=1, **physics())
+        du_alt = torch.empty_like(du)
+        ph_alt = np.mean([alt.profile(ud, du_alt) for _ in range(nprof)], axis=0)
+        op.Mult(ud, du)
+        extra["volume_staging_trial"] = {
+            "volume_ms_loads": float(phases[3]), "volume_ms_bulk_copy": float(ph_alt[3]),
+            "same_result": bool(torch.equal(du, du_alt)), "status": alt.read_status(),
+            "kept": "loads" if phases[3] <= ph_alt[3] else "bulk_copy"}
+        del alt, du_alt
     # FP32-mixed companion number and its error against FP64: RHS and the
     # final solution after a fixed-dt SSP-RK3 run from the same state
-    extra = {}
     if prec == "fp64" and not args.no_mixed:
         off = [1.0, 0.0, 0.0, 0.0, 1.0 / (1.4 * WORKLOAD["mach"] ** 2) / 0.4]
         op32 = T.NSOperator(m, numerical_flux=WORKLOAD["volume_flux"],
@@ -946,6 +960,9 @@ def main():
                          "sedov, lte and serving unless --no-workloads); serving: the batched "
                          "case stream; lte: the LTE-gas Taylor-Green vortex; sedov: the blended "
                          "blast; setup: mesh set-up on the device; vortex: the 2-D isentropic vortex")
+    ap.add_argument("--volume-staging", type=int, default=0, choices=[0, 1],
+                    help="rhs: 1 stages each element block's state by bulk copy (TMA) in the "
+                         "volume kernel")
     ap.add_argument("--no-workloads", action="store_true",
                     help="rhs: skip the other configurations")
     ap.add_argument("--sedov-n", type=int, default=64, help="sedov: elements per direction")

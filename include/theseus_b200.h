@@ -101,6 +101,10 @@ typedef struct {
   double state_offset[5];    /* FP32-mixed only: constant reference state u_ref (rho, rho*u_0..,
                                 rho*E) subtracted from the FP32 working copy; pressure enters
                                 the momentum fluxes as p - p(u_ref).  Zeros: plain FP32 copy. */
+  int32_t volume_staging;    /* 0: the volume kernel loads each element block's state itself;
+                                1: persistent CTAs stage the next block's state by bulk copy
+                                (cp.async.bulk, mbarrier completion) while evaluating the
+                                current one (not with blending or the LTE gas: falls back to 0) */
 } thx_config;
 
 /* Mesh and geometric factors, in the layout of the reference's device cache
@@ -449,6 +453,7 @@ int thx_integral_measures(thx_handle h, const double *u, double *out);
 #define THX_STATUS_LAUNCH 4u       /* a kernel got too little shared memory and did nothing */
 #define THX_STATUS_EOS 8u          /* LTE temperature recovery failed or left the table */
 #define THX_STATUS_FACE_TABLE 16u  /* a face table entry was out of range (thx_rhs_euler_noalloc) */
+#define THX_STATUS_TIMEOUT 32u     /* a bulk copy into shared memory did not land within 1 s */
 int thx_read_status(thx_handle h, uint32_t *flags, void *stream);
 
 /* ---- batch engine (no counterpart in the reference) -----------------------

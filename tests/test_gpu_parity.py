@@ -222,6 +222,27 @@ def test_fp32_mixed_solution_error(cuda, vol, surf):
     assert err.max() <= 1e-6, err
 
 
+@pytest.mark.parametrize("dim,order,n,ns", [(3, 4, (3, 3, 3), True), (3, 4, (4, 3, 2), False),
+                                            (2, 3, (7, 5), False), (3, 2, (3, 3, 3), True)])
+def test_bulk_copy_staged_volume_kernel(cuda, dim, order, n, ns):
+    """volume_staging=1: persistent CTAs stage the next element block's state
+    by bulk copy while evaluating the current one.  Same result as the oracle
+    (odd element counts exercise the ordinary-load fallback of a short last
+    block); FP32-mixed within FP32 round-off of the unstaged FP32 kernel (the
+    two are separate compilations, free to contract multiply-adds differently)."""
+    import torch
+    m = box(dim, order, n)
+    u = smooth_state(m, seed=7)
+    kw = dict(numerical_flux="ranocha", surface_flux="hll", ns=ns, mu=0.01, Pr=0.71)
+    du, op = gpu_rhs(m, u, volume_staging=1, **kw)
+    assert op.read_status() == 0
+    ref, _, _ = oracle_rhs(m, u, volume_flux="ranocha", surface_flux="hll", ns=ns, mu=0.01, Pr=0.71)
+    assert rel_l2(du, ref).max() <= TOL
+    d32a, _ = gpu_rhs(m, u, precision="fp32", volume_staging=1, **kw)
+    d32b, _ = gpu_rhs(m, u, precision="fp32", **dict(kw))
+    assert rel_l2(d32a, d32b).max() <= 1e-6
+
+
 def test_status_flag(cuda):
     m = box(2, 2, (3, 3))
     u = smooth_state(m, seed=1)
@@ -229,6 +250,31 @@ def test_status_flag(cuda):
     du, op = gpu_rhs(m, u, numerical_flux="ranocha", surface_flux="hll")
     assert op.read_status() & 1
     assert op.read_status() == 0
+
+
+def test_fp32_mixed_positivity_checked_in_fp64(cuda):
+    """FP32-mixed: the positivity test runs on the FP64 state (the working
+    copy's narrowing and the RK stage epilogue).  A node whose FP64 pressure is
+    -1e-9 (p = (gamma-1)(rho E - |m|^2/(2 rho))) sets the status flag, for a
+    right-hand side and for an SSP-RK3 run; a positive state does not."""
+    import torch
+    m = box(2, 3, (3, 3))
+    u = smooth_state(m, seed=1)
+    rho, mx, my = 1.0, 3.0, 4.0
+    ke = 0.5 * (mx * mx + my * my) / rho
+    u[:, 4, 5] = [rho, mx, my, ke - 1e-9 / 0.4]  # p = -1e-9 in FP64
+    kw = dict(numerical_flux="ranocha", surface_flux="hll")
+    op = T.EulerOperator(m, precision="fp32", state_offset=[1.0, 0.0, 0.0, 2.5], **kw)
+    ud = to_dev(u)
+    op.Mult(ud, torch.empty_like(ud))
+    assert op.read_status() & T.STATUS_NONPOSITIVE
+    v = smooth_state(m, seed=1)
+    vd = to_dev(v)
+    op.rk3_steps(vd, 1e-4, 2)
+    assert op.read_status() == 0
+    vd = to_dev(u)
+    op.rk3_steps(vd, 1e-4, 1)
+    assert op.read_status() & T.STATUS_NONPOSITIVE
 
 
 @pytest.mark.parametrize("dim,order,n,ns", [(2, 3, (6, 5), False), (3, 4, (3, 2, 3), True),

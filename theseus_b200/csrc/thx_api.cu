@@ -173,13 +173,16 @@ bool pick_order_kernels(thx_operator_s *h, int vk) {
 #define THX_PICK(P, D, NN)                                                  \
   if (h->dim == D && h->N == NN) {                                          \
     auto k = order_kernels_##P##_##D##_##NN();                              \
+    const bool tma = h->cfg.volume_staging == 1 && !bl;                    \
     if (P == 0) {                                                           \
-      h->vol64 = reinterpret_cast<VolLaunch<double>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
+      h->vol64 = reinterpret_cast<VolLaunch<double>>(tma ? k.vol_tma[vk][ns ? 1 : 0]      \
+                                                         : k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad64 = reinterpret_cast<GradLaunch<double>>(k.grad);             \
       h->blend64 = reinterpret_cast<BlendLaunch<double>>(k.blend);          \
       h->fv64 = reinterpret_cast<VolLaunch<double>>(k.fv);                  \
     } else {                                                                \
-      h->vol32 = reinterpret_cast<VolLaunch<float>>(k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
+      h->vol32 = reinterpret_cast<VolLaunch<float>>(tma ? k.vol_tma[vk][ns ? 1 : 0]       \
+                                                        : k.vol[vk][ns ? 1 : 0][bl ? 1 : 0]); \
       h->grad32 = reinterpret_cast<GradLaunch<float>>(k.grad);              \
       h->blend32 = reinterpret_cast<BlendLaunch<float>>(k.blend);           \
       h->fv32 = reinterpret_cast<VolLaunch<float>>(k.fv);                   \
@@ -717,8 +720,9 @@ int to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
   const long long n = h->L * h->neq;
   int st;
   if (!h->yf && (st = dev_alloc(&h->yf, (size_t)n, h->allocs))) return st;
-  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  to_working<<<grid, 256, 0, s>>>(h->L, h->neq, u, h->yf, h->off);
+  const int gridn = (int)std::min<long long>((h->L + 255) / 256, 148LL * 16);
+  if (h->dim == 2) to_working<2><<<gridn, 256, 0, s>>>(h->L, u, h->yf, h->off, h->g64.gm1, h->status);
+  else to_working<3><<<gridn, 256, 0, s>>>(h->L, u, h->yf, h->off, h->g64.gm1, h->status);
   return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
 }
 

@@ -35,6 +35,14 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   k.vol[VOL_CENTRAL][0][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, false, true>;
   k.vol[VOL_CENTRAL][1][0] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, false>;
   k.vol[VOL_CENTRAL][1][1] = &launch_volume<R, THX_DIM, THX_N, VOL_CENTRAL, true, true>;
+#define THX_SETT(V)                                                              \
+  k.vol_tma[V][0] = &launch_volume_tma<R, THX_DIM, THX_N, V, false>;             \
+  k.vol_tma[V][1] = &launch_volume_tma<R, THX_DIM, THX_N, V, true>;
+  THX_SETT(VOL_CHANDRASHEKAR)
+  THX_SETT(VOL_RANOCHA)
+  THX_SETT(VOL_PIROZZOLI)
+  THX_SETT(VOL_CENTRAL)
+#undef THX_SETT
 #if THX_PREC == 0
   k.grad = &launch_grad_sv<R, THX_DIM, THX_N>;  // FP64: entropy variables precomputed
 #else

@@ -87,6 +87,16 @@ __device__ __forceinline__ void pair_decode(int k, int &a, int &b) {
 enum : unsigned { STATUS_NONPOSITIVE = 1u, STATUS_NONFINITE = 2u, STATUS_LAUNCH = 4u,
                   STATUS_EOS = 8u };
 
+// Density and pressure of an FP64 conserved state both positive (NaN fails).
+template <int DIM>
+__device__ __forceinline__ bool fp64_state_positive(const double *q, double gm1) {
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 += q[1 + d] * q[1 + d];
+  const double p = gm1 * (q[DIM + 1] - 0.5 * m2 / q[0]);
+  return q[0] > 0.0 && p > 0.0;
+}
+
 __device__ __forceinline__ unsigned dynamic_smem_bytes() {
   unsigned v;
   asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
@@ -165,8 +175,19 @@ __device__ __forceinline__ void surface_flux_rt(int kind, const GasT<R> &g, cons
 // One CTA's work of the volume kernel: elements [block*EPB, block*EPB + EPB).
 // Shared by the one-case kernel (block = blockIdx.x) and the batched
 // persistent kernel (block from its work list).
+// Stride (in R) between the NEQ arrays of a block's state staged in shared
+// memory: EPB*ND rounded up to 16 bytes, so every array starts 16-byte aligned.
+template <typename R, int DIM, int N>
+__host__ __device__ constexpr int stage_kstride() {
+  using S = Shape<DIM, N>;
+  return (int)(((size_t)S::EPB * S::ND * sizeof(R) + 15) / 16 * 16 / sizeof(R));
+}
+
+// su: the block's state staged in shared memory (array k at k*stage_kstride,
+// element el's node n at el*ND + n), or nullptr to read it from a.u.
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
-__device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block) {
+__device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block,
+                                            const R *su = nullptr) {
   using S = Shape<DIM, N>;
   static_assert(VOL != VOL_LTEEC || (!BLEND && !IsF32<R>::value), "LTEEC: FP64, no blending");
   using L_ = VolSmem<R, DIM, N, VOL, NS, BLEND>;
@@ -211,8 +232,13 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   const bool active = (el < EPB) && (e < a.ne);
   if (active) {
     R q[NEQ];
+    if (su) {
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+      for (int k = 0; k < NEQ; ++k) q[k] = su[k * stage_kstride<R, DIM, N>() + el * ND + n];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
+    }
     if constexpr (VOL == VOL_LTEEC) {
       // conserved state, recovered T, its table cell and the pressure
       const double T = a.gas.Tn[(long long)e * ND + n];
@@ -244,7 +270,10 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
 #pragma unroll
         for (int k = 0; k < NEQ; ++k) sQ[(el * NEQ + k) * ND + n] = q[k];
       }
-      if (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))) atomicOr(a.status, STATUS_NONPOSITIVE);
+      // FP64 path: positivity of the state read here.  FP32-mixed: checked
+      // on the FP64 master state instead (to_working, the RK stage epilogue)
+      if (!IsF32<R>::value && (!(pr[0] > R(0)) || !(pr[DIM + 1] > R(0))))
+        atomicOr(a.status, STATUS_NONPOSITIVE);
     }
     if (mns != 0 || n == 0) {
       const R *mp = a.met + (long long)e * a.met_es + (long long)n * a.met_ns;
@@ -440,6 +469,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   } else {
     // fused SSP-RK3 stage in the arithmetic order of mfem::RK3SSPSolver::Step
     const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+    double ynew[NEQ];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
       const long long i = k * L + base;
@@ -460,7 +490,12 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
         if (a.dt_dev && dt == 0.0) y = a.um[i];
         else a.um[i] = y;
       }
+      ynew[k] = y;
       if (a.yf) a.yf[i] = (float)(y - a.off[k]);
+    }
+    if constexpr (IsF32<R>::value) {
+      // FP32-mixed: positivity of the new FP64 stage state, in FP64
+      if (!fp64_state_positive<DIM>(ynew, (double)a.gas.gm1)) atomicOr(a.status, STATUS_NONPOSITIVE);
     }
   }
 }
@@ -572,6 +607,169 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) volume_kernel(const Vo
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int MINB>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB) volume_kernel_mb(const VolArgs<R> a) {
   volume_body<R, DIM, N, VOL, NS, BLEND>(a, blockIdx.x);
+}
+
+// ---- TMA-staged volume kernel ---------------------------------------------
+// Persistent CTAs walk the element blocks; while a CTA evaluates one block,
+// the bulk-copy engine (cp.async.bulk, completion counted on an mbarrier)
+// brings the state of its next block into the other half of a double buffer
+// in shared memory, so the state loads of a block never wait on HBM.  Each
+// of the NEQ state arrays of a block is one contiguous run of EPB*ND values
+// (byNODES layout); a block whose runs are not 16-byte aligned, or not a
+// multiple of 16 bytes long, is staged with ordinary loads instead.
+// Waits are bounded: a copy that has not landed within kTmaWaitNs of the
+// global timer sets STATUS_TIMEOUT and the CTA stops.
+enum : unsigned { STATUS_TIMEOUT = 32u };
+constexpr unsigned long long kTmaWaitNs = 1000000000ull;  // one second
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// true once the phase with the given parity has completed
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (global_ns() - t0 < kTmaWaitNs)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+struct VolTmaSmem {
+  using S = Shape<DIM, N>;
+  static constexpr size_t base(bool metric_per_node) {
+    return (VolSmem<R, DIM, N, VOL, NS, BLEND>::bytes(metric_per_node) + 15) / 16 * 16;
+  }
+  static constexpr size_t buf_elems = (size_t)S::NEQ * stage_kstride<R, DIM, N>();
+  static constexpr size_t bytes(bool metric_per_node) {
+    return base(metric_per_node) + 2 * buf_elems * sizeof(R) + 2 * sizeof(unsigned long long);
+  }
+};
+
+// Thread 0: stage block `blk` into buffer `dst` (bulk copies counted on bar),
+// or report that the block needs ordinary loads (returns false).
+template <typename R, int DIM, int N>
+__device__ __forceinline__ bool tma_stage_issue(const VolArgs<R> &a, int blk, R *dst,
+                                                unsigned long long *bar) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
+  const int e0 = blk * EPB;
+  const int cnt = min(EPB, a.ne - e0);
+  const unsigned bytes = (unsigned)(cnt * ND * (int)sizeof(R));
+  const long long L = (long long)a.ne * ND;
+  bool ok = (bytes % 16u) == 0;
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k)
+    ok = ok && ((reinterpret_cast<uintptr_t>(a.u + k * L + (long long)e0 * ND) & 15u) == 0);
+  if (!ok) return false;
+  mbar_expect_tx(bar, bytes * NEQ);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k)
+    bulk_g2s(dst + k * stage_kstride<R, DIM, N>(), a.u + k * L + (long long)e0 * ND, bytes, bar);
+  return true;
+}
+
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int MINB>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, MINB > 0 ? MINB : 1)
+volume_tma_kernel(const VolArgs<R> a) {
+  using S = Shape<DIM, N>;
+  using T_ = VolTmaSmem<R, DIM, N, VOL, NS, BLEND>;
+  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const bool mpn = a.met_ns != 0;
+  if (dynamic_smem_bytes() < T_::bytes(mpn)) {
+    if (threadIdx.x == 0) atomicOr(a.status, STATUS_LAUNCH);
+    return;
+  }
+  R *buf0 = reinterpret_cast<R *>(smem_raw + T_::base(mpn));
+  R *bufs[2] = {buf0, buf0 + T_::buf_elems};
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(buf0 + 2 * T_::buf_elems);
+  __shared__ int s_bulk[2];  // buffer staged by bulk copy (1) or to be loaded (0)
+  __shared__ int s_fail;
+  const int nblocks = (a.ne + EPB - 1) / EPB;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+    s_bulk[0] = s_bulk[1] = 0;
+    if ((int)blockIdx.x < nblocks) s_bulk[0] = tma_stage_issue<R, DIM, N>(a, blockIdx.x, bufs[0], &bars[0]);
+  }
+  __syncthreads();
+  unsigned phase[2] = {0u, 0u};
+  bool pending[2] = {s_bulk[0] != 0, false};  // a copy into the buffer not yet waited for
+  const long long L = (long long)a.ne * ND;
+  int it = 0;
+  for (int blk = blockIdx.x; blk < nblocks; blk += gridDim.x, ++it) {
+    const int b = it & 1;
+    // the other buffer was last read before the previous iteration's final
+    // barrier: refill it with the next block
+    const int nxt = blk + gridDim.x;
+    if (tid == 0)
+      s_bulk[b ^ 1] = nxt < nblocks ? tma_stage_issue<R, DIM, N>(a, nxt, bufs[b ^ 1], &bars[b ^ 1]) : 0;
+    if (s_bulk[b]) {
+      if (!mbar_wait_bounded(&bars[b], phase[b])) s_fail = 1;
+    } else {
+      // ordinary loads into the buffer
+      const int e0 = blk * EPB;
+      for (int i = tid; i < EPB * ND; i += blockDim.x) {
+        if (e0 * ND + i >= L) continue;
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) bufs[b][k * stage_kstride<R, DIM, N>() + i] = a.u[k * L + (long long)e0 * ND + i];
+      }
+    }
+    __syncthreads();
+    pending[b ^ 1] = s_bulk[b ^ 1] != 0;
+    if (s_fail) break;
+    if (s_bulk[b]) {
+      phase[b] ^= 1u;
+      pending[b] = false;
+    }
+    volume_body<R, DIM, N, VOL, NS, BLEND>(a, blk, bufs[b]);
+    __syncthreads();  // shared memory and the buffer are free for the next block
+  }
+  if (s_fail) {
+    if (tid == 0) atomicOr(a.status, STATUS_TIMEOUT);
+    // give the copies still in flight a bounded chance to land before exit
+    for (int q = 0; q < 2; ++q)
+      if (pending[q]) mbar_wait_bounded(&bars[q], phase[q]);
+  }
 }
 
 template <typename R, int VOL, bool BLEND>
@@ -1288,10 +1486,24 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const Ble
 // SSP-RK3 stage updates (mfem::RK3SSPSolver::Step order) for the unfused path.
 // Conversions between the FP64 L-vector and the FP32 working copy u - off.
 struct Offsets { double v[5]; };
-static __global__ void to_working(long long L, int neq, const double *src, float *dst, Offsets off) {
+// FP32 working copy of an FP64 state, node by node, with the positivity of
+// the FP64 state checked in FP64 (density and pressure; gm1 = gamma - 1).
+template <int DIM>
+static __global__ void to_working(long long L, const double *src, float *dst, Offsets off, double gm1,
+                                  unsigned *status) {
+  constexpr int NEQ = DIM + 2;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L * neq; i += stride)
-    dst[i] = (float)(src[i] - off.v[i / L]);
+  bool bad = false;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride) {
+    double q[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      q[k] = src[k * L + i];
+      dst[k * L + i] = (float)(q[k] - off.v[k]);
+    }
+    if (!fp64_state_positive<DIM>(q, gm1)) bad = true;
+  }
+  if (bad && status) atomicOr(status, STATUS_NONPOSITIVE);
 }
 
 // ---------------------------------------------------------------------------

@@ -54,6 +54,39 @@ cudaError_t launch_volume(const VolArgs<R> &a, cudaStream_t s, int prepare) {
   return cudaGetLastError();
 }
 
+// Persistent, bulk-copy-staged volume kernel (no blending): as many CTAs as
+// fit on the device at once, each walking the element blocks.
+template <typename R, int DIM, int N, int VOL, bool NS>
+cudaError_t launch_volume_tma(const VolArgs<R> &a, cudaStream_t s, int prepare) {
+  using S = Shape<DIM, N>;
+  using T_ = VolTmaSmem<R, DIM, N, VOL, NS, false>;
+  constexpr int MINB = VolMinBlocks<R, VOL, false>::value;
+  auto kern = volume_tma_kernel<R, DIM, N, VOL, NS, false, MINB>;
+  static int cap[2] = {0, 0};  // resident CTAs on the device: metric per element / per node
+  if (prepare) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)T_::bytes(true));
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    for (int m = 0; m < 2; ++m) {
+      int per = 0;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, S::THREADS, T_::bytes(m == 1))) !=
+          cudaSuccess)
+        return e;
+      cap[m] = (per > 0 ? per : 1) * sms;
+    }
+    return cudaSuccess;
+  }
+  if (a.ne <= 0) return cudaSuccess;
+  const int m = a.met_ns != 0 ? 1 : 0;
+  const int nblocks = (a.ne + S::EPB - 1) / S::EPB;
+  const int grid = std::min(nblocks, cap[m] > 0 ? cap[m] : 148);
+  kern<<<grid, S::THREADS, T_::bytes(a.met_ns != 0), s>>>(a);
+  return cudaGetLastError();
+}
+
 template <typename R, int DIM, int SURF, bool NS>
 cudaError_t launch_face(const FaceArgs<R> &a, cudaStream_t s) {
   const int nfp = DIM == 2 ? a.N : a.N * a.N;
@@ -180,6 +213,7 @@ cudaError_t launch_blend(const BlendArgs<R> &a, cudaStream_t s) {
 template <typename R>
 struct OrderKernelsT {
   VolLaunch<R> vol[4][2][2];     // [volume flux][ns][blend]
+  VolLaunch<R> vol_tma[4][2];    // bulk-copy-staged, no blending: [volume flux][ns]
   GradLaunch<R> grad;
   BlendLaunch<R> blend;
   VolLaunch<R> fv;               // subcell FV rate of blended elements
