@@ -522,7 +522,7 @@ def other_workloads(args):
     import torch
     out = {}
     for name, fn in (("vortex_2d", run_vortex), ("sedov", run_sedov), ("lte", run_lte),
-                     ("serving", run_serving)):
+                     ("serving", run_serving), ("contraction_trial", run_trials)):
         try:
             full = fn(args)
             out[name] = compact(name, full)
@@ -542,6 +542,7 @@ def compact(name, d):
                 "rhs_rel_l2_vs_oracle_3cubed", "rk3", "phase_ms"],
         "serving": ["value", "unit", "latency_s", "makespan_s", "dof_rhs_per_s", "one_at_a_time_fp64",
                     "speedup_vs_one_at_a_time", "final_solution_rel_l2_vs_fp64"],
+        "contraction_trial": ["results"],
     }[name]
     r = {k: d[k] for k in keep if k in d}
     if name == "sedov":
@@ -633,6 +634,57 @@ def run_vortex(args):
                                  "oracle": O.entropy_residual(om, cfg, u, ref_du)},
             "cpu": {"rhs_dof_rhs_per_s": m.num_nodes / cpu_s, "kind": kind, "build": build,
                     "cores": threads, "oracle_100_steps_s": port_s, "oracle_threads": nth}}
+
+
+def run_trials(args):
+    """Tensor-core trial of the gradient's element-local derivative
+    contraction (thx_trial_contraction) on the 32^3 p=4 mesh: SIMT FMA against
+    mma.sync tiles -- FP64 m8n8k4, and FP32 m16n8k8 TF32 with one or three
+    products -- device time per launch and the largest difference from the
+    SIMT form relative to its largest value."""
+    import ctypes as C
+    import torch
+    import theseus_b200 as T
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    lib = T.library()
+    lib.thx_trial_contraction.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                          C.POINTER(C.c_double), C.c_void_p, C.c_int,
+                                          C.POINTER(C.c_double), C.c_void_p]
+    n, order = 32, 4
+    ne, nd = n ** 3, (order + 1) ** 3
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    _, _, Dm, _, _ = O.operators(order)
+    Dm = np.ascontiguousarray(Dm, np.float64)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    fields = torch.rand((5, ne, nd), generator=g, dtype=torch.float64, device="cuda") * 2 - 1
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    for prec, name, dt, forms in ((T.PRECISION_FP64, "fp64", torch.float64, ("simt", "mma_m8n8k4_f64")),
+                                  (T.PRECISION_FP32_MIXED, "fp32", torch.float32,
+                                   ("simt", "mma_m16n8k8_tf32", "mma_m16n8k8_3xtf32"))):
+        f = fields.to(dt).contiguous()
+        res, ref = {}, None
+        for form, fname in enumerate(forms):
+            o = torch.empty((ne, nd), dtype=dt, device="cuda")
+            ms = C.c_double()
+            st = lib.thx_trial_contraction(3, order, ne, prec, form, C.c_void_p(f.data_ptr()),
+                                           Dm.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(o.data_ptr()),
+                                           20, C.byref(ms), stream)
+            if st != 0:
+                res[fname] = {"status": st}
+                continue
+            torch.cuda.synchronize()
+            if ref is None:
+                ref = o.double()
+            diff = float((o.double() - ref).abs().max() / ref.abs().max())
+            res[fname] = {"ms": ms.value, "max_rel_diff_vs_simt": diff}
+        out[name] = res
+    return {"metric": "element-local derivative contraction: SIMT vs tensor-core tiles",
+            "config": {"workload": "gradient_D_contraction_32^3_p4", "elements": ne, "fields": 5,
+                       "directions": 3, "padding": "rows of S^T to 8 (FP64) / 16 (TF32), K=5 to 8, "
+                                                    "N columns: 5 of 8 used"},
+            "results": out}
 
 
 def run_serving(args):
@@ -955,11 +1007,12 @@ def main():
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
     ap.add_argument("--workload", default="rhs",
-                    choices=["rhs", "serving", "lte", "sedov", "setup", "vortex"],
+                    choices=["rhs", "serving", "lte", "sedov", "setup", "vortex", "trials"],
                     help="rhs: the headline RHS throughput (with compact results of vortex, "
                          "sedov, lte and serving unless --no-workloads); serving: the batched "
                          "case stream; lte: the LTE-gas Taylor-Green vortex; sedov: the blended "
-                         "blast; setup: mesh set-up on the device; vortex: the 2-D isentropic vortex")
+                         "blast; setup: mesh set-up on the device; vortex: the 2-D isentropic vortex; "
+                         "trials: the tensor-core trial of the gradient's derivative contraction")
     ap.add_argument("--volume-staging", type=int, default=0, choices=[0, 1],
                     help="rhs: 1 stages each element block's state by bulk copy (TMA) in the "
                          "volume kernel")
@@ -979,7 +1032,7 @@ def main():
         run_ours(args)
     else:
         fn = {"serving": run_serving, "lte": run_lte, "sedov": run_sedov, "setup": run_setup,
-              "vortex": run_vortex}[args.workload]
+              "vortex": run_vortex, "trials": run_trials}[args.workload]
         print(json.dumps(fn(args)), flush=True)
 
 

@@ -313,6 +313,21 @@ int thx_rhs_euler_noalloc(const thx_geometry *geom_dev, const thx_config *cfg,
  * flux-differencing kernels. */
 int thx_measure_fp64_fma_peak(int iters, int repeats, double *flops_per_s, void *stream);
 
+/* Tensor-core trial of the gradient's element-local derivative contraction
+ * (no counterpart in the reference): for every element of a 3-D p=4 mesh, the
+ * LGL derivative matrix D_host (N*N, row-major) applied along every tensor
+ * line of the NEQ fields `fields` (device, [NEQ][elements][nodes], FP64 for
+ * THX_PRECISION_FP64, FP32 for THX_PRECISION_FP32_MIXED), reduced per node
+ * to out[elements][nodes] = sum over (direction d, field k) of
+ * (1 + (d*NEQ + k)/8) dS_k/dxi_d.  form 0: SIMT FMA, one thread per node;
+ * FP64 form 1: mma.sync m8n8k4 FP64 tensor-core tiles; FP32 form 1:
+ * mma.sync m16n8k8 TF32 (one product), form 2: TF32 split into high and low
+ * parts (three products).  *ms: mean device time of `reps` launches after one
+ * warm-up (CUDA events on `stream`). */
+int thx_trial_contraction(int dim, int order, int num_elements, int precision, int form,
+                          const void *fields, const double *D_host, void *out, int reps,
+                          double *ms, void *stream);
+
 /* Right-hand sides of n states held in HOST memory: dudt_host[i] = L(u_host[i])
  * (FP64 L-vectors; in FP32-mixed mode each state is evaluated as thx_rhs does).
  * The library copies state i+1 in and rate i-1 out while it evaluates state

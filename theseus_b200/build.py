@@ -27,7 +27,8 @@ def units():
     u = [("thx_api.o", "thx_api.cu", []), ("thx_host.o", "thx_host.cpp", []),
          ("thx_lte_host.o", "thx_lte_host.cpp", []), ("thx_engine.o", "thx_engine.cu", []),
          ("thx_noalloc.o", "thx_noalloc.cu", []), ("thx_checkpoint.o", "thx_checkpoint.cpp", []),
-         ("thx_geometry.o", "thx_geometry.cu", []), ("thx_peak.o", "thx_peak.cu", [])]
+         ("thx_geometry.o", "thx_geometry.cu", []), ("thx_peak.o", "thx_peak.cu", []),
+         ("thx_trials.o", "thx_trials.cu", ["-DTHX_TRIAL_FMA"])]
     for dim in (2, 3):
         u.append((f"lte_face_{dim}.o", "thx_inst_lte.cu", [f"-DTHX_DIM={dim}"]))
         for n in ORDERS:
@@ -59,7 +60,9 @@ def _compile(job):
     # reference's CPU builds (-ffp-contract=off), so that it reproduces the CPU
     # right-hand side to round-off even where the result cancels strongly.
     # The FP32-mixed units may contract to FMA.
-    if "-DTHX_PREC=1" not in defs:
+    # The tensor-core trial keeps contraction on: its SIMT form is the
+    # strongest (fused) baseline.
+    if "-DTHX_PREC=1" not in defs and "-DTHX_TRIAL_FMA" not in defs:
         defs = defs + ["--fmad=false"]
     cmd = [NVCC] + ARCH + FLAGS + defs + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
