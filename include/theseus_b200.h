@@ -105,6 +105,10 @@ typedef struct {
                                 1: persistent CTAs stage the next block's state by bulk copy
                                 (cp.async.bulk, mbarrier completion) while evaluating the
                                 current one (not with blending or the LTE gas: falls back to 0) */
+  int32_t mixed_blended_fp32; /* FP32-mixed Euler with blending: 0 (default) evaluates every
+                                block of elements holding a blended element, and its faces, in
+                                FP64 from the FP64 stage state ("FP64 islands"); 1 keeps them
+                                in FP32 */
 } thx_config;
 
 /* Mesh and geometric factors, in the layout of the reference's device cache

@@ -243,6 +243,45 @@ def test_bulk_copy_staged_volume_kernel(cuda, dim, order, n, ns):
     assert rel_l2(d32a, d32b).max() <= 1e-6
 
 
+def test_fp32_mixed_fp64_islands(cuda):
+    """FP32-mixed Euler with blending evaluates every block of elements (EPB
+    = 256 / nodes per element) holding a blended element, and its faces, in
+    FP64 from the FP64 state: those elements' right-hand side equals the FP64
+    operator's bit for bit, the rest differs by FP32 round-off, and an SSP-RK3
+    run stays closer to FP64 than with the blended elements kept in FP32."""
+    import torch
+    m = box(3, 3, (6, 6, 6), [-1.0] * 3, [1.0] * 3)
+    u = cases.sedov(m.coords, width=0.05)
+    kw = dict(numerical_flux="chandrashekar", surface_flux="llf", fv_flux="llf", blending=True,
+              alpha_max=0.5, alpha_min=0.001)
+    off = [1.0, 0.0, 0.0, 0.0, 1e-5 / 0.4]
+    op64 = T.EulerOperator(m, **kw)
+    op32 = T.EulerOperator(m, precision="fp32", state_offset=off, **kw)
+    op32f = T.EulerOperator(m, precision="fp32", state_offset=off, mixed_blended_fp32=True, **kw)
+    ud = to_dev(u)
+    d64, d32, d32f = (torch.empty_like(ud) for _ in range(3))
+    op64.Mult(ud, d64)
+    op32.Mult(ud, d32)
+    op32f.Mult(ud, d32f)
+    a32, _ = op32.blending_coefficients()
+    epb = max(1, 256 // m.nd)
+    blk = (a32.view(-1, epb) > 0).any(dim=1) if m.num_elements % epb == 0 else None
+    assert blk is not None and int(blk.sum()) > 0
+    elems = torch.repeat_interleave(blk, epb)
+    assert torch.equal(d32[:, elems], d64[:, elems])
+    assert not torch.equal(d32f[:, elems], d64[:, elems])
+    assert op32.read_status() == 0
+    dt = 0.5 * op64.estimate_dt(ud, 0.5)
+    ys = [to_dev(u) for _ in range(3)]
+    for op, y in zip((op64, op32, op32f), ys):
+        op.rk3_steps(y, dt, 20)
+    torch.cuda.synchronize()
+    e_isl = field_errors(ys[1].cpu().numpy(), ys[0].cpu().numpy(), 3).max()
+    e_f32 = field_errors(ys[2].cpu().numpy(), ys[0].cpu().numpy(), 3).max()
+    assert e_isl < e_f32, (e_isl, e_f32)
+    assert op32.read_status() == 0
+
+
 def test_status_flag(cuda):
     m = box(2, 2, (3, 3))
     u = smooth_state(m, seed=1)

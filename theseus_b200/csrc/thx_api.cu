@@ -525,6 +525,36 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     h->dif_scale = (p > 0 && p < 13) ? 1.25 * dif_cal[p] : 0.5 * std::pow(p + 1.0, 4);
     h->surf_scale = h->adv_scale / (1.0 / w[0]);
   }
+  // FP64 islands of the FP32-mixed Euler path with blending
+  if (h->mixed && h->blend && !h->ns && !h->lte && !cfg->mixed_blended_fp32) {
+    bool found = false;
+#define THX_PICK_ISL(P, D, NN)                                   \
+    if (h->dim == D && h->N == NN) {                             \
+      auto k = order_kernels_0_##D##_##NN();                     \
+      h->isl_vol = k.voll[vk];                                   \
+      h->isl_fv = k.fvl;                                         \
+      h->isl_blend = k.blendl;                                   \
+      found = true;                                              \
+    }
+    THX_FOR_ORDERS(THX_PICK_ISL, 0, 2)
+    THX_FOR_ORDERS(THX_PICK_ISL, 0, 3)
+#undef THX_PICK_ISL
+    const FaceKernels0 fk = dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
+    h->isl_face = fk.facel[cfg->surface_flux];
+    if (!found || !h->isl_vol || !h->isl_fv || !h->isl_blend || !h->isl_face) return THX_ERR_UNSUPPORTED;
+    h->isl_epb = std::max(1, 256 / nd);
+    const int nblk = (h->ne + h->isl_epb - 1) / h->isl_epb;
+    if ((st = dev_alloc(&h->isl_flag, (size_t)nblk, A))) return st;
+    if ((st = dev_alloc(&h->isl_blocks, (size_t)nblk, A))) return st;
+    if ((st = dev_alloc(&h->isl_faces, (size_t)std::max(1, h->nf), A))) return st;
+    if ((st = dev_alloc(&h->isl_count, 2, A))) return st;
+    if ((st = dev_alloc(&h->isl_fstar, (size_t)h->nf * h->neq * nfp, A))) return st;
+    if ((st = dev_alloc(&h->isl_alpha, (size_t)h->ne, A))) return st;
+    if ((st = dev_alloc(&h->isl_eta, (size_t)h->ne, A))) return st;
+    if ((st = dev_alloc(&h->isl_fvrate, (size_t)h->L * h->neq, A))) return st;
+    if ((st = dev_zero(h->isl_alpha, sizeof(double) * h->ne))) return st;
+    h->islands = true;
+  }
   // kernel attributes (dynamic shared memory)
   cudaError_t ce;
   if (h->mixed) {
@@ -533,6 +563,11 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     ce = h->vol32(va, 0, 1);
     if (ce == cudaSuccess && h->ns) ce = h->grad32(ga, 0, 1);
     if (ce == cudaSuccess && h->blend) ce = h->fv32(va, 0, 1);
+    if (ce == cudaSuccess && h->islands) {
+      VolArgs<double> v64{};
+      ce = h->isl_vol(v64, nullptr, nullptr, 0, 1);
+      if (ce == cudaSuccess) ce = h->isl_fv(v64, nullptr, nullptr, 0, 1);
+    }
   } else {
     VolArgs<double> va{};
     GradArgs<double> ga{};
@@ -648,10 +683,12 @@ namespace {
 
 // One right-hand side: [T recovery] [indicator] [gradient] face fluxes,
 // volume+lift.  stage 0 writes du; stages 1..3 apply the SSP-RK3 update in place.
+// FP32-mixed: u64 is the FP64 state the working copy u was narrowed from
+// (the FP64 islands read it).
 template <typename R>
 int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
             double *um, double *y, float *yf, cudaEvent_t *ev = nullptr, double *du64 = nullptr,
-            const double *dt_dev = nullptr) {
+            const double *dt_dev = nullptr, const double *u64 = nullptr) {
   R *tag = nullptr;
   if (ev) cudaEventRecord(ev[0], s);
   GradArgs<R> ga;
@@ -676,6 +713,37 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     b.alpha = h->alpha; b.eta = h->eta;
     if (blendk(h, tag)(b, s) != cudaSuccess) return THX_ERR_CUDA;
   }
+  // FP64 islands: list the blocks holding a blended element and their faces,
+  // then the FP64 indicator of those blocks
+  const bool isl = IsF32<R>::value && h->islands && u64;
+  GradArgs<double> ga64;
+  FaceArgs<double> fa64;
+  VolArgs<double> va64;
+  if (isl) {
+    const int nblk = (h->ne + h->isl_epb - 1) / h->isl_epb;
+    if (cudaMemsetAsync(h->isl_count, 0, 2 * sizeof(int), s) != cudaSuccess) return THX_ERR_CUDA;
+    island_blocks_kernel<R><<<(nblk + 255) / 256, 256, 0, s>>>(h->ne, h->isl_epb, h->alpha, h->isl_flag,
+                                                               h->isl_blocks, h->isl_count);
+    if (h->nf > 0)
+      island_faces_kernel<<<(h->nf + 255) / 256, 256, 0, s>>>(h->nf, h->isl_epb, h->face_elem, h->isl_flag,
+                                                              h->isl_faces, h->isl_count + 1);
+    BlendArgs<double> b;
+    b.u = u64; b.ne = h->ne; b.vinv = h->vinv; b.gas = h->g64;
+    b.threshold = h->threshold; b.sharpness = h->cfg.sharpness;
+    b.alpha_min = h->cfg.alpha_min; b.alpha_max = h->cfg.alpha_max;
+    b.alpha = h->isl_alpha; b.eta = h->isl_eta;
+    if (h->isl_blend(b, h->isl_blocks, h->isl_count, s) != cudaSuccess) return THX_ERR_CUDA;
+    op_args<double>(h, u64, du64, stage, dt, um, y, yf, ga64, fa64, va64);
+    fa64.fstar = h->isl_fstar;
+    fa64.order = h->isl_faces;
+    va64.fstar = h->isl_fstar;
+    va64.alpha = h->isl_alpha;
+    va64.fvrate = h->isl_fvrate;
+    va64.yf = yf;
+    va64.dt_dev = dt_dev;
+    for (int k = 0; k < 5; ++k) va64.off[k] = h->off.v[k];
+    va.skip_block = h->isl_flag;
+  }
   if (ev) cudaEventRecord(ev[1], s);
   // FP64 Navier-Stokes (ideal gas): the entropy variables of every node
   // first, read by the gradient kernel
@@ -685,6 +753,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if (h->ns && gradk(h, tag)(ga, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[2], s);
   if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;
+  if (isl && h->isl_face(fa64, h->isl_count + 1, s) != cudaSuccess) return THX_ERR_CUDA;
   if constexpr (!IsF32<R>::value) {
     if (h->nbf > 0) {
       BndArgs ba;
@@ -696,8 +765,15 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     }
   }
   if (ev) cudaEventRecord(ev[3], s);
-  if (h->blend && fvk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
+  if (isl) {
+    // the FP64 subcell rate of the listed blocks; the FP32 kernel has no
+    // blended block left to evaluate
+    if (h->isl_fv(va64, h->isl_blocks, h->isl_count, s, 0) != cudaSuccess) return THX_ERR_CUDA;
+  } else if (h->blend && fvk(h, tag)(va, s, 0) != cudaSuccess) {
+    return THX_ERR_CUDA;
+  }
   if (volk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
+  if (isl && h->isl_vol(va64, h->isl_blocks, h->isl_count, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[4], s);
   return THX_OK;
 }
@@ -720,7 +796,7 @@ int to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
   const long long n = h->L * h->neq;
   int st;
   if (!h->yf && (st = dev_alloc(&h->yf, (size_t)n, h->allocs))) return st;
-  const int gridn = (int)std::min<long long>((h->L + 255) / 256, 148LL * 16);
+  const int gridn = (int)std::min<long long>((h->L + 255) / 256, 1LL << 24);  // one node per thread
   if (h->dim == 2) to_working<2><<<gridn, 256, 0, s>>>(h->L, u, h->yf, h->off, h->g64.gm1, h->status);
   else to_working<3><<<gridn, 256, 0, s>>>(h->L, u, h->yf, h->off, h->g64.gm1, h->status);
   return cudaGetLastError() == cudaSuccess ? THX_OK : THX_ERR_CUDA;
@@ -730,7 +806,7 @@ int rhs_mixed(thx_operator_s *h, const double *u, double *dudt, cudaStream_t s, 
   // the volume kernel writes the FP32 rate widened to FP64 directly
   int st;
   if ((st = to_working_copy(h, u, s))) return st;
-  return run_rhs<float>(h, h->yf, nullptr, s, 0, 0.0, nullptr, nullptr, nullptr, ev, dudt);
+  return run_rhs<float>(h, h->yf, nullptr, s, 0, 0.0, nullptr, nullptr, nullptr, ev, dudt, nullptr, u);
 }
 
 }  // namespace
@@ -1022,7 +1098,9 @@ int thx_rk3_steps(thx_handle h, double *u, double dt, int nsteps, void *stream) 
   for (int step = 0; step < nsteps; ++step) {
     if (h->mixed) {
       for (int stage = 1; stage <= 3; ++stage)
-        if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, dt, u, h->y, h->yf))) return st;
+        if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, dt, u, h->y, h->yf, nullptr, nullptr,
+                                 nullptr, stage == 1 ? u : h->y)))
+          return st;
     } else {
       if ((st = run_rhs<double>(h, u, nullptr, s, 1, dt, u, h->y, nullptr))) return st;
       if ((st = run_rhs<double>(h, h->y, nullptr, s, 2, dt, u, h->y, nullptr))) return st;
@@ -1052,7 +1130,7 @@ int thx_rk3_steps_cfl(thx_handle h, double *u, double cfl, int nsteps, double *d
     if (h->mixed) {
       for (int stage = 1; stage <= 3; ++stage)
         if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, 0.0, u, h->y, h->yf, nullptr, nullptr,
-                                 h->dtd)))
+                                 h->dtd, stage == 1 ? u : h->y)))
           return st;
     } else {
       if ((st = run_rhs<double>(h, u, nullptr, s, 1, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;
@@ -1116,7 +1194,7 @@ int thx_rk3_time_loop(thx_handle h, double *u, double cfl, int ncycles, thx_time
     if (h->mixed) {
       for (int stage = 1; stage <= 3; ++stage)
         if ((st = run_rhs<float>(h, h->yf, nullptr, s, stage, 0.0, u, h->y, h->yf, nullptr, nullptr,
-                                 h->dtd)))
+                                 h->dtd, stage == 1 ? u : h->y)))
           return st;
     } else {
       if ((st = run_rhs<double>(h, u, nullptr, s, 1, 0.0, u, h->y, nullptr, nullptr, nullptr, h->dtd))) return st;

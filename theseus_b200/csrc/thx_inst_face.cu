@@ -28,6 +28,16 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM)() {
 #undef THX_SET
   k.entropy = &launch_entropy<R, THX_DIM>;
 #if THX_PREC == 0
+  k.facel[SURF_CHANDRASHEKAR] = &launch_face_list<R, THX_DIM, SURF_CHANDRASHEKAR>;
+  k.facel[SURF_RANOCHA] = &launch_face_list<R, THX_DIM, SURF_RANOCHA>;
+  k.facel[SURF_PIROZZOLI] = &launch_face_list<R, THX_DIM, SURF_PIROZZOLI>;
+  k.facel[SURF_HLL] = &launch_face_list<R, THX_DIM, SURF_HLL>;
+  k.facel[SURF_LLF] = &launch_face_list<R, THX_DIM, SURF_LLF>;
+  k.facel[SURF_ROE] = &launch_face_list<R, THX_DIM, SURF_ROE>;
+#else
+  for (auto &f : k.facel) f = nullptr;
+#endif
+#if THX_PREC == 0
 #define THX_SETBND(S)                                   \
   k.bnd[S][0] = &launch_bnd<THX_DIM, S, false>;          \
   k.bnd[S][1] = &launch_bnd<THX_DIM, S, true>;

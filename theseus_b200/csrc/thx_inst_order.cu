@@ -59,6 +59,18 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   THX_SETB(VOL_CENTRAL)
 #undef THX_SETB
   k.gradb = &launch_grad_batched<R, THX_DIM, THX_N>;
+#if THX_PREC == 0
+  k.voll[VOL_CHANDRASHEKAR] = &launch_volume_list<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR>;
+  k.voll[VOL_RANOCHA] = &launch_volume_list<R, THX_DIM, THX_N, VOL_RANOCHA>;
+  k.voll[VOL_PIROZZOLI] = &launch_volume_list<R, THX_DIM, THX_N, VOL_PIROZZOLI>;
+  k.voll[VOL_CENTRAL] = &launch_volume_list<R, THX_DIM, THX_N, VOL_CENTRAL>;
+  k.fvl = &launch_fv_list<R, THX_DIM, THX_N>;
+  k.blendl = &launch_blend_list<R, THX_DIM, THX_N>;
+#else
+  for (auto &v : k.voll) v = nullptr;
+  k.fvl = nullptr;
+  k.blendl = nullptr;
+#endif
   return k;
 }
 

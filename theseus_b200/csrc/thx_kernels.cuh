@@ -155,6 +155,9 @@ struct VolArgs {
   float *yf;              // FP32 working copy of the next RHS input (mixed mode) or nullptr
   double off[5];          // yf = (float)(y - off[eq])
   unsigned *status;
+  // FP32-mixed with FP64 islands: blocks (of EPB elements) flagged here are
+  // evaluated by the FP64 kernels instead; this kernel skips them
+  const int *skip_block;
 };
 
 // Surface flux with a run-time selector (used on subcell faces).  Inlined:
@@ -195,6 +198,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   constexpr int MB = DIM * DIM;
   constexpr bool NEEDQ = L_::NEEDQ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (a.skip_block && a.skip_block[block]) return;  // block-uniform: before any barrier
   if (dynamic_smem_bytes() < L_::bytes(a.met_ns != 0)) {
     if (threadIdx.x == 0) atomicOr(a.status, STATUS_LAUNCH);
     return;
@@ -469,29 +473,43 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
   } else {
     // fused SSP-RK3 stage in the arithmetic order of mfem::RK3SSPSolver::Step
     const double dt = a.dt_dev ? *a.dt_dev : a.dt;
-    double ynew[NEQ];
+    // every load before the first store: the state arrays may alias as far
+    // as the compiler knows, so interleaving would serialise the round trips
+    double umv[NEQ], yv[NEQ];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
       const long long i = k * L + base;
+      umv[k] = a.um[i];
+      yv[k] = a.stage == 1 ? 0.0 : a.y[i];
+    }
+    double ynew[NEQ];
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
       const double kk = (double)du[k];
       double y;
       if (a.stage == 1) {
-        y = a.um[i] + dt * kk;
-        a.y[i] = y;
+        y = umv[k] + dt * kk;
       } else if (a.stage == 2) {
-        y = a.y[i] + dt * kk;
-        y = 0.75 * a.um[i] + 0.25 * y;
-        a.y[i] = y;
+        y = yv[k] + dt * kk;
+        y = 0.75 * umv[k] + 0.25 * y;
       } else {
-        y = a.y[i] + dt * kk;
-        y = (1.0 / 3.0) * a.um[i] + (2.0 / 3.0) * y;
+        y = yv[k] + dt * kk;
+        y = (1.0 / 3.0) * umv[k] + (2.0 / 3.0) * y;
         // a device-side step of 0 (a finished time loop, or no valid rate)
         // leaves the state exactly as it was
-        if (a.dt_dev && dt == 0.0) y = a.um[i];
-        else a.um[i] = y;
+        if (a.dt_dev && dt == 0.0) y = umv[k];
       }
       ynew[k] = y;
-      if (a.yf) a.yf[i] = (float)(y - a.off[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      const long long i = k * L + base;
+      if (a.stage == 3) {
+        if (!(a.dt_dev && dt == 0.0)) a.um[i] = ynew[k];
+      } else {
+        a.y[i] = ynew[k];
+      }
+      if (a.yf) a.yf[i] = (float)(ynew[k] - a.off[k]);
     }
     if constexpr (IsF32<R>::value) {
       // FP32-mixed: positivity of the new FP64 stage state, in FP64
@@ -518,11 +536,11 @@ struct FvSmem {
 };
 
 template <typename R, int DIM, int N>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) fv_kernel(const VolArgs<R> a) {
+__device__ __forceinline__ void fv_body(const VolArgs<R> &a, const int block) {
   using S = Shape<DIM, N>;
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NL = S::NLINE;
   constexpr int FACES = FvSmem<R, DIM, N>::FACES;
-  const int e0 = blockIdx.x * EPB;
+  const int e0 = block * EPB;
   bool any = false;
   for (int k = 0; k < EPB; ++k)
     if (e0 + k < a.ne && a.alpha[e0 + k] > 1e-16) any = true;
@@ -594,6 +612,11 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) fv_kernel(const VolArg
   }
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) a.fvrate[((long long)e * NEQ + k) * ND + n] = rate[k];
+}
+
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) fv_kernel(const VolArgs<R> a) {
+  fv_body<R, DIM, N>(a, blockIdx.x);
 }
 
 template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
@@ -1415,57 +1438,75 @@ struct BlendArgs {
   double *alpha, *eta;
 };
 
+// The indicator of one element by one warp: lanes own nodes lane, lane+32,
+// ...; the sum-factorised transform runs through two warp-private shared
+// buffers (__syncwarp between directions) and the mode sums through a fixed
+// shuffle tree -- no block-wide barrier (include/RHSOperator_impl.hpp:355-437:
+// modal energy of p*rho, eta, the sigmoid alpha with its alpha_min/alpha_max
+// clipping).
 template <typename R, int DIM, int N>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const BlendArgs<R> a) {
+__device__ __forceinline__ void blend_element_warp(const BlendArgs<R> &a, const int e, const double *sV,
+                                                   double *bufA, double *bufB) {
   using S = Shape<DIM, N>;
-  constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB;
-  __shared__ double sV[N * N];
-  __shared__ double sA[EPB * ND], sB[EPB * ND];
-  const int tid = threadIdx.x;
-  for (int i = tid; i < N * N; i += blockDim.x) sV[i] = a.vinv[i];
-  const int el = tid / ND, n = tid % ND;
-  const int e = blockIdx.x * EPB + el;
-  const bool active = (el < EPB) && (e < a.ne);
+  constexpr int ND = S::ND, NEQ = S::NEQ, J = (ND + 31) / 32;
+  const int lane = threadIdx.x & 31;
   const long long L = (long long)a.ne * ND;
-  if (active) {
-    R raw[NEQ], q[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
-    reconstruct<R, DIM>(a.gas, raw, q);
-    sA[el * ND + n] = (double)(pressure<R, DIM>(a.gas, q) * q[0]);
+  for (int j = 0; j < J; ++j) {
+    const int n = lane + 32 * j;
+    if (n < ND) {
+      R raw[NEQ], q[NEQ];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
+      reconstruct<R, DIM>(a.gas, raw, q);
+      bufA[n] = (double)(pressure<R, DIM>(a.gas, q) * q[0]);
+    }
   }
-  __syncthreads();
-  int c[3];
-  node_coords<DIM, N>(n, c);
-  // contract direction by direction: after pass d, index c[d] is a mode degree
-  double *src = sA, *dst = sB;
+  __syncwarp();
+  double *src = bufA, *dst = bufB;
 #pragma unroll
   for (int dir = 0; dir < DIM; ++dir) {
-    if (active) {
-      const int line = line_of<DIM, N>(dir, c);
-      double s = 0.0;
 #pragma unroll
-      for (int l = 0; l < N; ++l) s += sV[c[dir] * N + l] * src[el * ND + line_node<DIM, N>(dir, line, l)];
-      dst[el * ND + n] = s;
+    for (int j = 0; j < J; ++j) {
+      const int n = lane + 32 * j;
+      if (n < ND) {
+        int c[3];
+        node_coords<DIM, N>(n, c);
+        const int line = line_of<DIM, N>(dir, c);
+        double s = 0.0;
+#pragma unroll
+        for (int l = 0; l < N; ++l) s += sV[c[dir] * N + l] * src[line_node<DIM, N>(dir, line, l)];
+        dst[n] = s;
+      }
     }
-    __syncthreads();
+    __syncwarp();
     double *t = src; src = dst; dst = t;
   }
-  // deterministic per-element sums in mode order
-  if (active && n == 0) {
-    double mm = 0.0, m1 = 0.0, m2 = 0.0;
-    for (int m = 0; m < ND; ++m) {
-      int cm[3];
-      node_coords<DIM, N>(m, cm);
-      int mx = cm[0];
+  double mm = 0.0, m1 = 0.0, m2 = 0.0;
 #pragma unroll
-      for (int d = 1; d < DIM; ++d) mx = cm[d] > mx ? cm[d] : mx;
-      const double mode = src[el * ND + m];
+  for (int j = 0; j < J; ++j) {
+    const int n = lane + 32 * j;
+    if (n < ND) {
+      int c[3];
+      node_coords<DIM, N>(n, c);
+      int mx = c[0];
+#pragma unroll
+      for (int d = 1; d < DIM; ++d) mx = c[d] > mx ? c[d] : mx;
+      const double mode = src[n];
       const double sq = mode * mode;
       mm += sq;
       if (mx <= N - 2) m1 += sq;
       if (mx <= N - 3) m2 += sq;
     }
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    mm += __shfl_xor_sync(0xffffffffu, mm, off);
+    m1 += __shfl_xor_sync(0xffffffffu, m1, off);
+    m2 += __shfl_xor_sync(0xffffffffu, m2, off);
+  }
+  __syncwarp();  // the buffers are free for the warp's next element
+  if (lane == 0) {
     const double eps = 1.0e-30;
     double val = 0.0;
     if (mm > eps) {
@@ -1482,6 +1523,31 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) blend_kernel(const Ble
   }
 }
 
+constexpr int kBlendWarps = 8;
+
+// Elements [e_begin + i) for i over the grid's warps (nsel: element count;
+// list: nullptr, or blocks of EPB elements to take the elements from).
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(32 * kBlendWarps) blend_warp_kernel(const BlendArgs<R> a,
+                                                                      const int *__restrict__ list,
+                                                                      const int *__restrict__ count) {
+  using S = Shape<DIM, N>;
+  constexpr int ND = S::ND;
+  __shared__ double sV[N * N];
+  __shared__ double sBuf[kBlendWarps][2][ND];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) sV[i] = a.vinv[i];
+  __syncthreads();
+  const int w = threadIdx.x >> 5;
+  const long long nitems = list ? (long long)(*count) * S::EPB : (long long)a.ne;
+  for (long long it = (long long)blockIdx.x * kBlendWarps + w; it < nitems;
+       it += (long long)gridDim.x * kBlendWarps) {
+    const int e = list ? list[it / S::EPB] * S::EPB + (int)(it % S::EPB) : (int)it;
+    if (e >= a.ne) continue;  // warp-uniform
+    blend_element_warp<R, DIM, N>(a, e, sV, sBuf[w][0], sBuf[w][1]);
+  }
+}
+
+
 // ---------------------------------------------------------------------------
 // SSP-RK3 stage updates (mfem::RK3SSPSolver::Step order) for the unfused path.
 // Conversions between the FP64 L-vector and the FP32 working copy u - off.
@@ -1489,18 +1555,17 @@ struct Offsets { double v[5]; };
 // FP32 working copy of an FP64 state, node by node, with the positivity of
 // the FP64 state checked in FP64 (density and pressure; gm1 = gamma - 1).
 template <int DIM>
-static __global__ void to_working(long long L, const double *src, float *dst, Offsets off, double gm1,
-                                  unsigned *status) {
+static __global__ void to_working(long long L, const double *__restrict__ src, float *__restrict__ dst,
+                                  Offsets off, double gm1, unsigned *status) {
   constexpr int NEQ = DIM + 2;
   const long long stride = (long long)gridDim.x * blockDim.x;
   bool bad = false;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride) {
     double q[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) {
-      q[k] = src[k * L + i];
-      dst[k * L + i] = (float)(q[k] - off.v[k]);
-    }
+    for (int k = 0; k < NEQ; ++k) q[k] = src[k * L + i];  // all loads in flight before the stores
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) dst[k * L + i] = (float)(q[k] - off.v[k]);
     if (!fp64_state_positive<DIM>(q, gm1)) bad = true;
   }
   if (bad && status) atomicOr(status, STATUS_NONPOSITIVE);
@@ -1779,6 +1844,74 @@ face_batched(const FaceArgs<R> *__restrict__ args, const BatchWork *__restrict__
     const BatchWork it = work[w];
     face_body<R, DIM, SURF, NS>(args[it.item], (long long)it.block * 128 + threadIdx.x);
   }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 islands of the FP32-mixed Euler path with blending.  The blended
+// (troubled) elements are where FP32 rounding of the state matters: a blast
+// core's energy density is large while its pressure may be small.  After the
+// FP32 indicator, every block (of EPB elements) holding a blended element is
+// flagged and listed, and so is every face touching a flagged block; the
+// FP64 kernels then evaluate the indicator, the face fluxes, the subcell FV
+// rate and the volume term with the stage update for exactly those blocks
+// and faces from the FP64 stage state, while the FP32 volume kernel skips
+// the flagged blocks.  The list walkers are persistent grids that read the
+// list length on the device, so a captured graph stays valid.
+
+// flag[b] = block b holds an element with alpha > 0; flagged blocks are
+// appended to list (count zeroed beforehand)
+template <typename R>
+__global__ void island_blocks_kernel(int ne, int epb, const double *__restrict__ alpha,
+                                     int *__restrict__ flag, int *__restrict__ list, int *count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = (ne + epb - 1) / epb;
+  if (b >= nb) return;
+  bool any = false;
+  for (int k = 0; k < epb; ++k) {
+    const int e = b * epb + k;
+    if (e < ne && alpha[e] > 0.0) any = true;
+  }
+  flag[b] = any ? 1 : 0;
+  if (any) list[atomicAdd(count, 1)] = b;
+}
+
+// faces with a side in a flagged block, appended to list (count zeroed beforehand)
+static __global__ void island_faces_kernel(int nf, int epb, const int *__restrict__ face_elem,
+                                    const int *__restrict__ flag, int *__restrict__ list, int *count) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  if (flag[face_elem[2 * f] / epb] || flag[face_elem[2 * f + 1] / epb]) list[atomicAdd(count, 1)] = f;
+}
+
+template <typename R, int DIM, int N, int VOL>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 4)
+volume_list_kernel(const VolArgs<R> a, const int *__restrict__ list, const int *__restrict__ count) {
+  const int n = *count;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    __syncthreads();  // the previous block's shared memory is free
+    volume_body<R, DIM, N, VOL, false, true>(a, list[w]);
+  }
+}
+
+template <typename R, int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+fv_list_kernel(const VolArgs<R> a, const int *__restrict__ list, const int *__restrict__ count) {
+  const int n = *count;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    __syncthreads();
+    fv_body<R, DIM, N>(a, list[w]);
+  }
+}
+
+// face points of the listed faces (a.order = the face list)
+template <typename R, int DIM, int SURF>
+__global__ void __launch_bounds__(128)
+face_list_kernel(const FaceArgs<R> a, const int *__restrict__ count) {
+  const int nfp = DIM == 2 ? a.N : a.N * a.N;
+  const long long total = (long long)(*count) * nfp;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    face_body<R, DIM, SURF, false>(a, t);
 }
 
 }  // namespace thx

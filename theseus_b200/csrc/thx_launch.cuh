@@ -178,6 +178,53 @@ cudaError_t launch_face_batched(const FaceArgs<R> *args, const BatchWork *work, 
   return cudaGetLastError();
 }
 
+// FP64 islands: walkers over device-side lists (grid fixed, length read on
+// the device)
+template <typename R>
+using VolListLaunch = cudaError_t (*)(const VolArgs<R> &, const int *, const int *, cudaStream_t, int);
+template <typename R>
+using BlendListLaunch = cudaError_t (*)(const BlendArgs<R> &, const int *, const int *, cudaStream_t);
+template <typename R>
+using FaceListLaunch = cudaError_t (*)(const FaceArgs<R> &, const int *, cudaStream_t);
+constexpr int kIslandGrid = 148 * 4;
+
+template <typename R, int DIM, int N, int VOL>
+cudaError_t launch_volume_list(const VolArgs<R> &a, const int *list, const int *count, cudaStream_t s,
+                               int prepare) {
+  using S = Shape<DIM, N>;
+  const int bytes = (int)volume_smem_bytes<R, DIM, N, VOL, false, true>(true);
+  if (prepare)
+    return cudaFuncSetAttribute(volume_list_kernel<R, DIM, N, VOL>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const size_t smem = volume_smem_bytes<R, DIM, N, VOL, false, true>(a.met_ns != 0);
+  volume_list_kernel<R, DIM, N, VOL><<<kIslandGrid, S::THREADS, smem, s>>>(a, list, count);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int N>
+cudaError_t launch_fv_list(const VolArgs<R> &a, const int *list, const int *count, cudaStream_t s,
+                           int prepare) {
+  using S = Shape<DIM, N>;
+  constexpr size_t smem = FvSmem<R, DIM, N>::bytes();
+  if (prepare)
+    return cudaFuncSetAttribute(fv_list_kernel<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+  fv_list_kernel<R, DIM, N><<<kIslandGrid, S::THREADS, smem, s>>>(a, list, count);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int N>
+cudaError_t launch_blend_list(const BlendArgs<R> &a, const int *list, const int *count, cudaStream_t s) {
+  blend_warp_kernel<R, DIM, N><<<kIslandGrid, 32 * kBlendWarps, 0, s>>>(a, list, count);
+  return cudaGetLastError();
+}
+
+template <typename R, int DIM, int SURF>
+cudaError_t launch_face_list(const FaceArgs<R> &a, const int *count, cudaStream_t s) {
+  face_list_kernel<R, DIM, SURF><<<148 * 8, 128, 0, s>>>(a, count);
+  return cudaGetLastError();
+}
+
 using BndLaunch = cudaError_t (*)(const BndArgs &, cudaStream_t);
 
 template <int DIM, int SURF, bool NS>
@@ -203,10 +250,9 @@ cudaError_t launch_fv(const VolArgs<R> &a, cudaStream_t s, int prepare) {
 
 template <typename R, int DIM, int N>
 cudaError_t launch_blend(const BlendArgs<R> &a, cudaStream_t s) {
-  using S = Shape<DIM, N>;
   if (a.ne <= 0) return cudaSuccess;
-  const int grid = (a.ne + S::EPB - 1) / S::EPB;
-  blend_kernel<R, DIM, N><<<grid, S::THREADS, 0, s>>>(a);
+  const int grid = (a.ne + kBlendWarps - 1) / kBlendWarps;  // one warp per element
+  blend_warp_kernel<R, DIM, N><<<grid, 32 * kBlendWarps, 0, s>>>(a, nullptr, nullptr);
   return cudaGetLastError();
 }
 
@@ -219,6 +265,10 @@ struct OrderKernelsT {
   VolLaunch<R> fv;               // subcell FV rate of blended elements
   VolBatchLaunch<R> volb[4][2];  // [volume flux][ns]
   GradBatchLaunch<R> gradb;
+  // FP64 islands (Euler, blending; set in the FP64 units only)
+  VolListLaunch<R> voll[4];      // [volume flux]
+  VolListLaunch<R> fvl;
+  BlendListLaunch<R> blendl;
 };
 template <typename R>
 struct FaceKernelsT {
@@ -226,6 +276,7 @@ struct FaceKernelsT {
   FaceBatchLaunch<R> faceb[6][2];
   BndLaunch bnd[6][2];           // boundary faces [surface flux][ns] (FP64)
   EntropyLaunch<R> entropy;      // entropy variables of every node (NS)
+  FaceListLaunch<R> facel[6];    // FP64 islands: listed faces (Euler; FP64 units only)
 };
 using OrderKernels0 = OrderKernelsT<double>;
 using OrderKernels1 = OrderKernelsT<float>;

@@ -141,6 +141,16 @@ struct thx_operator_s {
   thx::VolLaunch<double> fv64 = nullptr;
   thx::FaceLaunch<double> face64 = nullptr;
   thx::EntropyLaunch<double> ent64 = nullptr;
+  // FP32-mixed Euler with blending: FP64 islands (blocks holding blended
+  // elements and their faces evaluated in FP64; thx_kernels.cuh)
+  bool islands = false;
+  int isl_epb = 1;
+  int *isl_flag = nullptr, *isl_blocks = nullptr, *isl_faces = nullptr;
+  int *isl_count = nullptr;  // [0] blocks, [1] faces
+  double *isl_fstar = nullptr, *isl_alpha = nullptr, *isl_eta = nullptr, *isl_fvrate = nullptr;
+  thx::VolListLaunch<double> isl_vol = nullptr, isl_fv = nullptr;
+  thx::BlendListLaunch<double> isl_blend = nullptr;
+  thx::FaceListLaunch<double> isl_face = nullptr;
   thx::EntropyLaunch<float> ent32 = nullptr;
   thx::BndLaunch bnd64 = nullptr;   // boundary faces (FP64 Euler)
   thx::VolLaunch<float> vol32 = nullptr;
