@@ -797,7 +797,7 @@ volume_tma_kernel(const VolArgs<R> a) {
 
 template <typename R, int VOL, bool BLEND>
 struct VolMinBlocks {
-  static constexpr int value = VOL == VOL_LTEEC ? 2 : (!IsF32<R>::value ? 4 : 0);
+  static constexpr int value = VOL == VOL_LTEEC ? 2 : (!IsF32<R>::value ? 4 : 6);
 };
 
 // ---------------------------------------------------------------------------
