@@ -109,6 +109,11 @@ typedef struct {
                                 block of elements holding a blended element, and its faces, in
                                 FP64 from the FP64 stage state ("FP64 islands"); 1 keeps them
                                 in FP32 */
+  int32_t mixed_flux_no_perturbation; /* FP32-mixed with the Chandrashekar volume flux and an
+                                HLL/LLF/Roe surface flux about a physical offset state: 0
+                                (default) evaluates the fluxes in perturbation form, F - F(offset),
+                                from the state's deviations (the constant cancels in the
+                                right-hand side); 1 evaluates F itself */
 } thx_config;
 
 /* Mesh and geometric factors, in the layout of the reference's device cache

@@ -31,6 +31,7 @@ class Config(C.Structure):
         ("alpha_max", C.c_double), ("alpha_min", C.c_double), ("sharpness", C.c_double),
         ("modal_threshold", C.c_double), ("state_offset", C.c_double * 5),
         ("volume_staging", C.c_int32), ("mixed_blended_fp32", C.c_int32),
+        ("mixed_flux_no_perturbation", C.c_int32),
     ]
 
 
@@ -175,7 +176,8 @@ def make_config(flow="euler", volume_flux="chandrashekar", surface_flux=None, fv
                 blending=False, precision="fp64", gamma=1.4, Pr=0.72, R_gas=287.05, mu=0.02,
                 mu0=1.716e-5, mu_bulk=2.0 / 3.0, T0=273.15, Ts=110.4, alpha_max=0.5,
                 alpha_min=0.001, sharpness=9.21024, modal_threshold=0.0, sutherland=False,
-                geometry_layout=0, state_offset=None, volume_staging=0, mixed_blended_fp32=False):
+                geometry_layout=0, state_offset=None, volume_staging=0, mixed_blended_fp32=False,
+                mixed_flux_no_perturbation=False):
     cfg = Config()
     f = str(flow).lower()
     viscous = f.startswith(("visc", "nav", "cns", "ns"))
@@ -193,6 +195,7 @@ def make_config(flow="euler", volume_flux="chandrashekar", surface_flux=None, fv
     cfg.modal_threshold = modal_threshold
     cfg.volume_staging = int(volume_staging)
     cfg.mixed_blended_fp32 = 1 if mixed_blended_fp32 else 0
+    cfg.mixed_flux_no_perturbation = 1 if mixed_flux_no_perturbation else 0
     if state_offset is not None:
         for i, v in enumerate(state_offset):
             cfg.state_offset[i] = float(v)

@@ -64,7 +64,32 @@ GasT<R> make_gas(const thx_config &c, int dim) {
     const double ke = rho > 0.0 ? 0.5 * m2 / rho : 0.0;
     for (int k = 0; k < dim + 2; ++k) g.qref[k] = (R)c.state_offset[k];
     g.ke_ref = (R)ke;
-    g.p_ref = (R)((c.gamma - 1.0) * (c.state_offset[dim + 1] - ke));
+    const double pr = (c.gamma - 1.0) * (c.state_offset[dim + 1] - ke);
+    g.p_ref = (R)pr;
+    // perturbation form of the fluxes about the offset state: for the
+    // Chandrashekar volume flux with physical-flux surface fluxes (and subcell
+    // fluxes), and an offset that is a physical state
+    auto physical_face = [](int f) { return f == THX_FLUX_HLL || f == THX_FLUX_LLF || f == THX_FLUX_ROE; };
+    g.pert = (c.volume_flux == THX_FLUX_CHANDRASHEKAR && physical_face(c.surface_flux) &&
+              (!c.blending || physical_face(c.fv_flux)) && rho > 0.0 && pr > 0.0 &&
+              !c.mixed_flux_no_perturbation) ? 1 : 0;
+    g.rho_r = (R)rho;
+    double v2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double v = (d < dim && rho > 0.0) ? c.state_offset[1 + d] / rho : 0.0;
+      g.v_r[d] = (R)v;
+      v2 += v * v;
+    }
+    g.p_r = (R)pr;
+    const double beta = pr > 0.0 ? 0.5 * rho / pr : 0.0;
+    g.beta_r = (R)beta;
+    const double gav = 2.0 / (c.gamma + c.gamma - 2.0);
+    g.h_r = beta > 0.0 ? (R)(0.5 / beta * gav + 0.5 * v2 + pr / rho) : R(0);
+    g.Hr = (R)(c.state_offset[dim + 1] + pr);
+  } else {
+    g.pert = 0;
+    g.rho_r = g.p_r = g.beta_r = g.h_r = g.Hr = R(0);
+    g.v_r[0] = g.v_r[1] = g.v_r[2] = R(0);
   }
   const double gm1 = c.gamma - 1.0;
   const double gm1_inv = 1.0 / gm1;

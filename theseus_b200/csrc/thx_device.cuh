@@ -30,6 +30,12 @@ struct GasT {
   // unused in FP64.
   R qref[5];
   R ke_ref, p_ref;
+  // FP32 perturbation form (pert = 1): the fluxes are evaluated as
+  // G = F - F(qref), from the deviations of the state from qref, whose
+  // primitive values follow (rho_r, v_r, p_r, beta_r = rho_r/(2 p_r),
+  // h_r = Chandrashekar's averaged enthalpy of qref with itself, Hr = E_r + p_r)
+  int pert;
+  R rho_r, v_r[3], p_r, beta_r, h_r, Hr;
   // LTE Helmholtz gas (FP64 only): the device table and the per-node
   // temperatures recovered once per right-hand side, [elem][node].
   LteDev lte{};
@@ -134,6 +140,32 @@ __device__ __forceinline__ void node_prims(const GasT<R> &g, const R *raw, R *ou
     const R ke = ke_density<R, DIM>(q);
     const R pp = g.gm1 * (raw[DIM + 1] - (ke - g.ke_ref));
     const R p = g.p_ref + pp;
+    if (VOL == VOL_CHANDRASHEKAR && g.pert) {
+      // perturbation form: rho, dv = v - v_r, beta, dbeta = beta - beta_r,
+      // drho; the pressure deviation from the kinetic-energy deviation
+      // ke - ke_r = drho |v|^2/2 + rho_r (v_r.dv + |dv|^2/2), free of the
+      // cancellation of ke - ke_r formed from the two
+      R dv[DIM];
+      R v2 = R(0), vrdv = R(0), dvdv = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        dv[d] = fdiv(raw[1 + d] - raw[0] * g.v_r[d], rho);
+        const R v = g.v_r[d] + dv[d];
+        v2 += v * v;
+        vrdv += g.v_r[d] * dv[d];
+        dvdv += dv[d] * dv[d];
+      }
+      const R dke = R(0.5) * raw[0] * v2 + g.rho_r * (vrdv + R(0.5) * dvdv);
+      const R ppp = g.gm1 * (raw[DIM + 1] - dke);
+      const R pq = g.p_r + ppp;
+      out[0] = rho;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) out[1 + d] = dv[d];
+      out[DIM + 1] = fdiv(R(0.5) * rho, pq);
+      out[DIM + 2] = fdiv(R(0.5) * (raw[0] * g.p_r - g.rho_r * ppp), pq * g.p_r);
+      out[DIM + 3] = raw[0];
+      return;
+    }
     out[0] = rho;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) out[1 + d] = fdiv(q[1 + d], rho);
@@ -169,11 +201,81 @@ __device__ __forceinline__ R mom_p(const R *a) {
   else return a[DIM + 1];
 }
 
+// ---- FP32 perturbation form ------------------------------------------------
+// Log mean of x1 = xr + d1, x2 = xr + d2 and its deviation from xr, both to
+// FP32 accuracy relative to their own size: for u = ((x2-x1)/(x2+x1))^2 <
+// 1/16 the mean is ((x1+x2)/2) / S(u) with S(u) = artanh(f)/f = sum u^k/(2k+1)
+// (f^2 = u; terms through u^6, truncation below 5e-9), so the deviation is
+// (d1+d2)/2 - ((x1+x2)/2) (S-1)/S with no cancellation; beyond, the closed
+// form, whose deviation is formed by difference.
+__device__ __forceinline__ void log_mean_dev(float x1, float x2, float d1, float d2, float xr,
+                                             float &val, float &dev) {
+  const float s = x1 + x2, d = x2 - x1;
+  const float f = fdiv(d, s);
+  const float u = f * f;
+  if (u < 0.0625f) {
+    const float sm1 =
+        u * (1.f / 3.f + u * (1.f / 5.f + u * (1.f / 7.f + u * (1.f / 9.f + u * (1.f / 11.f + u * (1.f / 13.f))))));
+    const float mean = 0.5f * s;
+    val = fdiv(mean, 1.f + sm1);
+    dev = 0.5f * (d1 + d2) - val * sm1;
+  } else {
+    val = fdiv(d, logf(fdiv(x2, x1)));
+    dev = val - xr;
+  }
+}
+
+// Chandrashekar's two-point flux minus its value at the reference state,
+// G = F(a, b) - F(ref, ref), from the per-node deviations (node_prims layout
+// rho, dv, beta, dbeta, drho):
+//   G_rho = drho_ln vn + rho_r dvn
+//   G_m   = G_rho vbar + rho_r vn_r dvbar + dp_hat m
+//   G_E   = G_rho h_hat + rho_r vn_r dh_hat
+// with dp_hat = ((drho1+drho2)/2 - p_r (dbeta1+dbeta2)) / (beta1+beta2) and
+// dh_hat = -dbeta_ln g1/(2 beta_ln beta_r) + v_r.dvbar + |dvbar|^2
+//          - (|dv1|^2 + |dv2|^2)/4 + (dp_hat rho_r - p_r drho_ln)/(rho_ln rho_r).
+template <int DIM>
+__device__ __forceinline__ void vol_chandrashekar_pert(const GasT<float> &g, const float *a, const float *b,
+                                                       const float *met, float *F) {
+  float rho_ln, drho_ln, beta_ln, dbeta_ln;
+  log_mean_dev(a[0], b[0], a[DIM + 3], b[DIM + 3], g.rho_r, rho_ln, drho_ln);
+  log_mean_dev(a[DIM + 1], b[DIM + 1], a[DIM + 2], b[DIM + 2], g.beta_r, beta_ln, dbeta_ln);
+  float dvb[DIM], vb[DIM];
+  float dvn = 0.f, vnr = 0.f, vrdv = 0.f, dv2 = 0.f, dvs = 0.f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const float d1 = a[1 + d], d2 = b[1 + d];
+    dvb[d] = 0.5f * (d1 + d2);
+    vb[d] = g.v_r[d] + dvb[d];
+    dvn += dvb[d] * met[d];
+    vnr += g.v_r[d] * met[d];
+    vrdv += g.v_r[d] * dvb[d];
+    dv2 += dvb[d] * dvb[d];
+    dvs += d1 * d1 + d2 * d2;
+  }
+  const float vn = vnr + dvn;
+  const float bsum = a[DIM + 1] + b[DIM + 1];
+  const float dph = fdiv(0.5f * (a[DIM + 3] + b[DIM + 3]) - g.p_r * (a[DIM + 2] + b[DIM + 2]), bsum);
+  const float Gr = drho_ln * vn + g.rho_r * dvn;
+  const float dh = -fdiv(dbeta_ln * g.gm1_av_inv, 2.f * beta_ln * g.beta_r) + vrdv + dv2 - 0.25f * dvs +
+                   fdiv(dph * g.rho_r - g.p_r * drho_ln, rho_ln * g.rho_r);
+  F[0] = Gr;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = Gr * vb[d] + g.rho_r * vnr * dvb[d] + dph * met[d];
+  F[DIM + 1] = Gr * (g.h_r + dh) + g.rho_r * vnr * dh;
+}
+
 // ---- two-point volume fluxes (metric rows already averaged) --------------
 // include/ChandrashekarFlux.hpp:20-89
 template <typename R, int DIM>
 __device__ __forceinline__ void vol_chandrashekar(const GasT<R> &g, const R *a, const R *b,
                                                   const R *met, R *F) {
+  if constexpr (IsF32<R>::value) {
+    if (g.pert) {
+      vol_chandrashekar_pert<DIM>(g, a, b, met, F);
+      return;
+    }
+  }
   const R rho1 = a[0], rho2 = b[0];
   const R rho_ln = log_mean(rho1, rho2);
   R mom_hat[DIM];
@@ -284,6 +386,7 @@ __device__ __forceinline__ void vol_central(const R *qa, const R *qb, const R *a
 template <typename R, int DIM>
 struct FState {
   R q[DIM + 2], d[DIM + 2], p, pp;
+  R dv[DIM];  // FP32 perturbation form: v - v_r
 };
 
 template <typename R, int DIM>
@@ -291,8 +394,22 @@ __device__ __forceinline__ void make_fstate(const GasT<R> &g, const R *raw, FSta
   if constexpr (IsF32<R>::value) {
 #pragma unroll
     for (int k = 0; k < DIM + 2; ++k) { s.d[k] = raw[k]; s.q[k] = g.qref[k] + raw[k]; }
-    const R ke = ke_density<R, DIM>(s.q);
-    s.pp = g.gm1 * (raw[DIM + 1] - (ke - g.ke_ref));
+    if (g.pert) {
+      // deviations as in node_prims' perturbation form
+      R v2 = R(0), vrdv = R(0), dvdv = R(0);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        s.dv[d] = fdiv(raw[1 + d] - raw[0] * g.v_r[d], s.q[0]);
+        const R v = g.v_r[d] + s.dv[d];
+        v2 += v * v;
+        vrdv += g.v_r[d] * s.dv[d];
+        dvdv += s.dv[d] * s.dv[d];
+      }
+      s.pp = g.gm1 * (raw[DIM + 1] - (R(0.5) * raw[0] * v2 + g.rho_r * (vrdv + R(0.5) * dvdv)));
+    } else {
+      const R ke = ke_density<R, DIM>(s.q);
+      s.pp = g.gm1 * (raw[DIM + 1] - (ke - g.ke_ref));
+    }
     s.p = g.p_ref + s.pp;
   } else {
 #pragma unroll
@@ -341,6 +458,39 @@ __device__ __forceinline__ R normal_flux(const R *q, const NState<R, DIM> &s, co
     r += pf * n[dir];
   }
   return r;
+}
+
+// FP32 perturbation form of normal_flux: component eq of (F(q) - F(q_ref)).n
+// from the state's deviations d (raw working copy), dv = v - v_r and the
+// pressure deviation pp:
+//   mass      d_m.n
+//   momentum  d_(m_c) (v.n) + m_rc (dv.n) + pp n_c
+//   energy    (d_E + pp)(v.n) + (E_r + p_r)(dv.n)
+template <int DIM>
+__device__ __forceinline__ float normal_flux_dev(const GasT<float> &g, const FState<float, DIM> &s,
+                                                 const NState<float, DIM> &ns, const float *n, int eq) {
+  float vn = 0.f, dvn = 0.f, dmn = 0.f;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    vn += s.q[1 + d] * ns.inv_rho * n[d];
+    dvn += s.dv[d] * n[d];
+    dmn += s.d[1 + d] * n[d];
+  }
+  if (eq == 0) return dmn;
+  if (eq <= DIM) return s.d[eq] * vn + g.qref[eq] * dvn + s.pp * n[eq - 1];
+  return (s.d[DIM + 1] + s.pp) * vn + g.Hr * dvn;
+}
+
+// component eq of the normal flux: F(q).n (FP64; FP32 without a reference
+// state, the pressure entering as its fluctuation) or its deviation
+// (FP32 perturbation form)
+template <typename R, int DIM>
+__device__ __forceinline__ R normal_flux_s(const GasT<R> &g, const FState<R, DIM> &s,
+                                           const NState<R, DIM> &ns, const R *n, int eq) {
+  if constexpr (IsF32<R>::value) {
+    if (g.pert) return normal_flux_dev<DIM>(g, s, ns, n, eq);
+  }
+  return normal_flux<R, DIM>(s.q, ns, n, eq);
 }
 
 // include/DissipationOperator.hpp:57-172
@@ -554,7 +704,7 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const FState<R, D
     const R sR = (sR1 > sR2) ? sR1 : sR2;
 #pragma unroll
     for (int e = 0; e < DIM + 2; ++e) {
-      const R fn1 = normal_flux<R, DIM>(q1, L, n, e), fn2 = normal_flux<R, DIM>(q2, Rs, n, e);
+      const R fn1 = normal_flux_s<R, DIM>(g, A, L, n, e), fn2 = normal_flux_s<R, DIM>(g, B, Rs, n, e);
       if (sL >= R(0)) F[e] = fn1;
       else if (sR <= R(0)) F[e] = fn2;
       else F[e] = (sR * fn1 - sL * fn2 + sL * sR * (B.d[e] - A.d[e])) / (sR - sL);
@@ -574,7 +724,7 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const FState<R, D
                         rabs(vn2) + rsqrt_(g.gamma * Rs.p / q2[0]) * nm);
 #pragma unroll
     for (int e = 0; e < DIM + 2; ++e) {
-      const R nl = normal_flux<R, DIM>(q1, L, n, e), nr = normal_flux<R, DIM>(q2, Rs, n, e);
+      const R nl = normal_flux_s<R, DIM>(g, A, L, n, e), nr = normal_flux_s<R, DIM>(g, B, Rs, n, e);
       F[e] = R(0.5) * (nl + nr) - R(0.5) * lmax * (B.d[e] - A.d[e]);
     }
   } else {
@@ -626,7 +776,7 @@ __device__ __forceinline__ void surface_flux(const GasT<R> &g, const FState<R, D
     diss[E] = lm * am * (H - a * un) + lz * (R(0.5) * az * u2 + rho_roe * udt) + lp * ap * (H + a * un);
 #pragma unroll
     for (int e = 0; e < DIM + 2; ++e) {
-      const R central = R(0.5) * (normal_flux<R, DIM>(q1, left, n, e) + normal_flux<R, DIM>(q2, right, n, e));
+      const R central = R(0.5) * (normal_flux_s<R, DIM>(g, A, left, n, e) + normal_flux_s<R, DIM>(g, B, right, n, e));
       F[e] = central - R(0.5) * diss[e];
     }
   }
