@@ -502,6 +502,11 @@ typedef struct {
   double dt;                 /* fixed step */
   double mu, Pr;             /* transport (Navier-Stokes) */
   double state_offset[5];    /* FP32 working-copy offset (FP32-mixed engines) */
+  int64_t geometry_key;      /* 0: the case's geometry is uploaded for it alone; otherwise cases
+                                with the same key share one device copy of the geometry (built from
+                                the first such case's mesh and kept until the engine is destroyed;
+                                the caller guarantees the key names one mesh -- a later case with a
+                                different element/face count under the key is refused) */
 } thx_case;
 
 typedef struct {

@@ -71,6 +71,34 @@ def run_engine(engine, batch):
     return out
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_engine_shared_geometry(cuda, precision):
+    """Cases that name the same mesh with a geometry key share one device copy
+    of its geometry; their results equal those of cases with their own copies,
+    bit for bit, and a key reused with a different mesh size is refused."""
+    import dataclasses
+    base = [vortex_case(2, 3, (6, 6), v, 15, seed=i) for i, v in enumerate((False, True, False))]
+    mesh = base[0].mesh
+    base = [dataclasses.replace(c, mesh=mesh) for c in base]
+    keyed = [dataclasses.replace(c, geometry_key=7) for c in base]
+    eng = BatchEngine(precision=precision, steps_per_launch=5, **FLUX)
+    try:
+        own = run_engine(eng, base)
+        shared = run_engine(eng, keyed)
+    finally:
+        eng.close()
+    for a, b in zip(own, shared):
+        assert np.array_equal(a, b)
+    eng = BatchEngine(precision=precision, steps_per_launch=5, **FLUX)
+    try:
+        run_engine(eng, keyed[:1])
+        other = dataclasses.replace(vortex_case(2, 3, (5, 6), False, 5), geometry_key=7)
+        with pytest.raises(T.THXError):
+            eng.admit(other)
+    finally:
+        eng.close()
+
+
 MIX = [(2, 2, (6, 6), False, 20), (2, 3, (5, 7), True, 20), (2, 5, (4, 4), False, 25),
        (2, 2, (8, 5), False, 30), (3, 3, (2, 2, 3), True, 10), (2, 4, (3, 3), True, 7)]
 

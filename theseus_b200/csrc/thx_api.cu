@@ -328,8 +328,27 @@ void subcell_element(int dim, int N, const double *metric_el, const double *D, c
           }
 }
 
+// Copies a donor operator's device geometry (factors, face tables, element-to-
+// face table, operators, subcell metrics, modal transform) into h by pointer:
+// h does not own them.  The donor must be built from the same mesh, order,
+// precision, blending and geometry layout, periodic, and outlive h.
+void share_geometry(thx_operator_s *h, const thx_operator_s *d) {
+  h->lay = d->lay;
+  h->jac64 = d->jac64; h->jac32 = d->jac32;
+  h->met64 = d->met64; h->met32 = d->met32;
+  h->nrm64 = d->nrm64; h->nrm32 = d->nrm32;
+  h->wm64 = d->wm64; h->wm32 = d->wm32;
+  h->wp64 = d->wp64; h->wp32 = d->wp32;
+  h->face_elem = d->face_elem; h->face_lface = d->face_lface;
+  h->face_order = d->face_order; h->elem_face = d->elem_face;
+  h->ops64 = d->ops64; h->ops32 = d->ops32;
+  h->D64 = d->D64; h->D32 = d->D32;
+  for (int k = 0; k < 3; ++k) { h->sub64[k] = d->sub64[k]; h->sub32[k] = d->sub32[k]; }
+  h->vinv = d->vinv;
+}
+
 int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
-                const thx_lte_table *table = nullptr) {
+                const thx_lte_table *table = nullptr, const thx_operator_s *donor = nullptr) {
   AllocOwner owner(h);
   h->cfg = *cfg;
   h->dim = g->dim;
@@ -400,8 +419,16 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if ((st = dev_alloc(&h->Tn, (size_t)h->L, A))) return st;
     h->g64.Tn = h->Tn;
   }
+  // a donor's device geometry is shared, not rebuilt (batch engine: cases
+  // that name the same mesh)
+  if (donor && (donor->dim != dim || donor->order != h->order || donor->ne != h->ne ||
+                donor->nf != h->nf || donor->nbf != 0 || h->nbf != 0 || donor->mixed != h->mixed ||
+                donor->blend != h->blend || donor->cfg.geometry_layout != cfg->geometry_layout))
+    return THX_ERR_INVALID_ARGUMENT;
+  if (donor) share_geometry(h, donor);
   // geometry
   std::vector<double> tmp;
+  if (!donor) {
   pack_strided(g->jac, h->ne, nd, 1, full, tmp, h->lay.jac_es, h->lay.jac_ns);
   if ((st = upload_both(tmp, &h->jac64, &h->jac32, w32, A))) return st;
   pack_strided(g->metric, h->ne, nd, MB, full, tmp, h->lay.met_es, h->lay.met_ns);
@@ -465,11 +492,12 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if ((st = upload(&h->bc_data, g->bc_data, (size_t)std::max(1, (int)g->bc_data_len), A))) return st;
     if (h->ns && (st = dev_alloc(&h->bgrad, (size_t)h->nbf * nfp * dim * h->neq, A))) return st;
   }
+  }  // !donor
   // operators
   std::vector<double> x(N), w(N), D(N * N), Dh(N * N), Dh2(N * N);
   lgl_rule(N, x.data(), w.data());
   derivative_operators(N, x.data(), w.data(), D.data(), Dh.data(), Dh2.data());
-  {
+  if (!donor) {
     std::vector<double> ops(2 * N * N + N);
     std::memcpy(ops.data(), Dh2.data(), sizeof(double) * N * N);
     std::memcpy(ops.data() + N * N, Dh.data(), sizeof(double) * N * N);
@@ -514,7 +542,7 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
   // blending: modal transform and subcell metrics
   h->threshold = cfg->modal_threshold > 0 ? cfg->modal_threshold
                                           : 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->order, 0.25));
-  if (h->blend) {
+  if (h->blend && !donor) {
     std::vector<double> vinv(N * N);
     if (!legendre_vinv(N, x.data(), vinv.data())) return THX_ERR_NUMERICS;
     if ((st = upload(&h->vinv, vinv.data(), vinv.size(), A))) return st;
@@ -839,9 +867,9 @@ int rhs_mixed(thx_operator_s *h, const double *u, double *dudt, cudaStream_t s, 
 namespace thx {
 
 int op_create(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
-              const thx_lte_table *table) {
+              const thx_lte_table *table, const thx_operator_s *donor) {
   try {
-    return create_impl(g, cfg, h, table);
+    return create_impl(g, cfg, h, table, donor);
   } catch (...) {
     return THX_ERR_OUT_OF_MEMORY;
   }

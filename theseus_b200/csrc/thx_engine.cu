@@ -158,6 +158,12 @@ class Engine final : public EngineBase {
     for (auto &kv : cases_) release(kv.second.get(), false);
     cases_.clear();
     for (auto &kv : groups_) destroy_group(*kv.second);
+    if (setup_) cudaStreamSynchronize(setup_);
+    for (auto &kv : donors_) {
+      op_free(kv.second);
+      delete kv.second;
+    }
+    donors_.clear();
     if (setup_) {
       cudaStreamSynchronize(setup_);
       cudaStreamDestroy(setup_);
@@ -202,6 +208,30 @@ class Engine final : public EngineBase {
     cc.mu = c->mu;
     cc.Pr = c->Pr;
     for (int k = 0; k < 5; ++k) cc.state_offset[k] = c->state_offset[k];
+    // cases naming the same mesh share one device copy of its geometry
+    const thx_operator_s *donor = nullptr;
+    if (c->geometry_key != 0) {
+      std::lock_guard<std::mutex> dl(donor_mu_);
+      auto it = donors_.find(c->geometry_key);
+      if (it != donors_.end()) {
+        donor = it->second;
+      } else {
+        thx_operator_s *d = new (std::nothrow) thx_operator_s();
+        if (!d) return unreserve(THX_ERR_OUT_OF_MEMORY);
+        d->device = device_;
+        d->pool = pool_;
+        d->setup_stream = setup_;
+        d->ring = &ring_;
+        const int dst = op_create(g, &cc, d, nullptr);
+        if (dst) {
+          op_free(d);
+          delete d;
+          return unreserve(dst);
+        }
+        donors_[c->geometry_key] = d;
+        donor = d;
+      }
+    }
     auto ec = std::make_unique<EngineCase>();
     thx_operator_s *h = new (std::nothrow) thx_operator_s();
     if (!h) return unreserve(THX_ERR_OUT_OF_MEMORY);
@@ -216,7 +246,7 @@ class Engine final : public EngineBase {
       ec->h = nullptr;
       return unreserve(st);
     };
-    int st = op_create(g, &cc, h, nullptr);
+    int st = op_create(g, &cc, h, nullptr, donor);
     if (st) return fail(st);
     const size_t n = (size_t)h->L * h->neq;
     if ((st = alloc(h, &ec->u, n)) || (st = alloc(h, &h->y, n)) ||
@@ -713,6 +743,9 @@ class Engine final : public EngineBase {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   }
   std::mutex mu_;
+  // device geometry shared by cases with the same thx_case::geometry_key
+  std::mutex donor_mu_;
+  std::map<int64_t, thx_operator_s *> donors_;
 };
 
 template <>

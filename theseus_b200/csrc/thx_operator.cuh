@@ -183,7 +183,7 @@ namespace thx {
 // Builds the operator's device data (geometry, operators, scratch, kernel
 // choice); LTE gas when table != nullptr.  On failure the caller frees.
 int op_create(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
-              const thx_lte_table *table);
+              const thx_lte_table *table, const thx_operator_s *donor = nullptr);
 void op_free(thx_operator_s *h);
 
 // Kernel arguments of one right-hand side (stage 0: du = L(u); stages 1..3:

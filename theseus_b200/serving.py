@@ -32,7 +32,8 @@ THX_ERR_BUSY = 7
 
 class CaseDesc(C.Structure):
     _fields_ = [("flow_model", C.c_int32), ("nsteps", C.c_int32), ("dt", C.c_double),
-                ("mu", C.c_double), ("Pr", C.c_double), ("state_offset", C.c_double * 5)]
+                ("mu", C.c_double), ("Pr", C.c_double), ("state_offset", C.c_double * 5),
+                ("geometry_key", C.c_int64)]
 
 
 class EngineStats(C.Structure):
@@ -75,6 +76,7 @@ class Case:
     arrival: float = 0.0
     tag: dict = field(default_factory=dict)
     factory: object = None   # builds u0 on first use when u0 is None
+    geometry_key: int = 0    # nonzero: cases with the same key share the device geometry
 
     def state(self):
         if self.u0 is None:
@@ -84,7 +86,7 @@ class Case:
     def desc(self):
         off = (C.c_double * 5)(*[float(x) for x in self.state_offset])
         return CaseDesc(FLOW_NAVIER_STOKES if self.viscous else FLOW_EULER, int(self.nsteps),
-                        float(self.dt), float(self.mu), float(self.Pr), off)
+                        float(self.dt), float(self.mu), float(self.Pr), off, int(self.geometry_key))
 
 
 class BatchEngine:
@@ -363,4 +365,5 @@ class SyntheticStream:
             dt = min(dt, self.cfl * h * h / ((p["order"] + 1) ** 4 * nu))
         off = (1.0, v, v, 1.0 / (self.gamma - 1.0) + v * v, 0.0)
         return Case(mesh=m, u0=u0, nsteps=self.nsteps, dt=dt, viscous=not p["inviscid"], mu=mu,
-                    Pr=0.72, state_offset=off, arrival=p["arrival"], tag=p, factory=build)
+                    Pr=0.72, state_offset=off, arrival=p["arrival"], tag=p, factory=build,
+                    geometry_key=1 + 16 * p["side"] + p["order"])
