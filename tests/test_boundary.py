@@ -208,7 +208,45 @@ def test_gpu_ns_mixed_walls_sutherland(cuda):
 def test_gpu_boundaries_unsupported_forms_are_refused(cuda):
     m = bmesh(2, 3, (3, 3), {"x-": "slip", "x+": "slip"})
     with pytest.raises(T.THXError, match="unsupported"):
-        T.EulerOperator(m, numerical_flux="chandrashekar", surface_flux="roe", precision="fp32")
+        T.NSOperator(m, numerical_flux="chandrashekar", surface_flux="roe", precision="fp32",
+                     mu=0.01, Pr=0.72)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("blending", [False, True])
+def test_gpu_fp32_mixed_boundaries_fp64_islands(cuda, blending):
+    """FP32-mixed Euler on a mesh with boundary faces: every block of elements
+    next to a boundary face is an FP64 island (with its faces, the boundary
+    fluxes and, with blending, the blended blocks): those elements' rate
+    equals the FP64 operator's bit for bit, the rest is FP32-accurate, and an
+    SSP-RK3 run stays within FP32 round-off of FP64."""
+    import torch
+    sides = {"x-": spec("supersonic-inflow", 2), "x+": "supersonic-outflow",
+             "y-": "slip", "y+": "symmetry"}
+    m = bmesh(2, 3, (8, 6), sides, seed=5, perturb=False)
+    u = smooth_state(m, seed=9)
+    kw = dict(numerical_flux="chandrashekar", surface_flux="roe", blending=blending)
+    off = [1.0, 0.3, 0.0, 2.5 + 0.045]
+    op64 = T.EulerOperator(m, **kw)
+    op32 = T.EulerOperator(m, precision="fp32", state_offset=off, **kw)
+    ud = torch.as_tensor(u, device="cuda").contiguous()
+    d64, d32 = torch.empty_like(ud), torch.empty_like(ud)
+    op64.Mult(ud, d64)
+    op32.Mult(ud, d32)
+    epb = max(1, 256 // m.nd)
+    blk = np.zeros((m.num_elements + epb - 1) // epb, bool)
+    blk[np.asarray(m.boundary.elem) // epb] = True
+    elems = np.repeat(blk, epb)[:m.num_elements]
+    a64, a32 = d64.cpu().numpy(), d32.cpu().numpy()
+    assert np.array_equal(a32[:, elems], a64[:, elems])
+    assert rel_l2(a32, a64).max() <= 1e-5
+    assert op32.read_status() == 0
+    dt = 0.3 * op64.estimate_dt(ud, 1.0)
+    ya, yb = ud.clone(), ud.clone()
+    op64.rk3_steps(ya, dt, 20)
+    op32.rk3_steps(yb, dt, 20)
+    assert rel_l2(yb.cpu().numpy(), ya.cpu().numpy()).max() <= 1e-6
+    assert op32.read_status() == 0
 
 
 @pytest.mark.gpu

@@ -369,7 +369,9 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     if (!g->bdr_elem || !g->bdr_lface || !g->bdr_normal || !g->bdr_weight || !g->bdr_bc || !g->bcs ||
         g->num_bcs <= 0 || g->bc_data_len < 0 || (g->bc_data_len > 0 && !g->bc_data))
       return THX_ERR_INVALID_ARGUMENT;
-    if (h->mixed || table) return THX_ERR_UNSUPPORTED;
+    // FP32-mixed: Euler only, the boundary-adjacent blocks evaluated in FP64
+    // (FP64 islands); the LTE gas has no boundary conditions here
+    if (table || (h->mixed && cfg->flow_model == THX_FLOW_NAVIER_STOKES)) return THX_ERR_UNSUPPORTED;
     for (int i = 0; i < g->num_bcs; ++i) {
       const thx_bc &bc = g->bcs[i];
       if (bc.type < THX_BC_SLIP_WALL || bc.type > THX_BC_NOSLIP_ISOTHERMAL) return THX_ERR_INVALID_ARGUMENT;
@@ -578,8 +580,9 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     h->dif_scale = (p > 0 && p < 13) ? 1.25 * dif_cal[p] : 0.5 * std::pow(p + 1.0, 4);
     h->surf_scale = h->adv_scale / (1.0 / w[0]);
   }
-  // FP64 islands of the FP32-mixed Euler path with blending
-  if (h->mixed && h->blend && !h->ns && !h->lte && !cfg->mixed_blended_fp32) {
+  // FP64 islands of the FP32-mixed Euler path: the blocks holding a blended
+  // element (unless switched off) and the blocks next to a boundary face
+  if (h->mixed && !h->ns && !h->lte && ((h->blend && !cfg->mixed_blended_fp32) || h->nbf > 0)) {
     bool found = false;
 #define THX_PICK_ISL(P, D, NN)                                   \
     if (h->dim == D && h->N == NN) {                             \
@@ -594,14 +597,23 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
 #undef THX_PICK_ISL
     const FaceKernels0 fk = dim == 2 ? face_kernels_0_2() : face_kernels_0_3();
     h->isl_face = fk.facel[cfg->surface_flux];
-    if (!found || !h->isl_vol || !h->isl_fv || !h->isl_blend || !h->isl_face) return THX_ERR_UNSUPPORTED;
+    h->isl_bnd = fk.bnd[cfg->surface_flux][0];
+    if (!found || !h->isl_vol || !h->isl_fv || !h->isl_blend || !h->isl_face || (h->nbf > 0 && !h->isl_bnd))
+      return THX_ERR_UNSUPPORTED;
     h->isl_epb = std::max(1, 256 / nd);
     const int nblk = (h->ne + h->isl_epb - 1) / h->isl_epb;
+    h->isl_alpha_in = h->blend && !cfg->mixed_blended_fp32;
+    if (h->nbf > 0) {
+      // blocks next to a boundary face are islands at every right-hand side
+      std::vector<int> stat(nblk, 0);
+      for (int b = 0; b < h->nbf; ++b) stat[g->bdr_elem[b] / h->isl_epb] = 1;
+      if ((st = upload(&h->isl_static, stat.data(), stat.size(), A))) return st;
+    }
     if ((st = dev_alloc(&h->isl_flag, (size_t)nblk, A))) return st;
     if ((st = dev_alloc(&h->isl_blocks, (size_t)nblk, A))) return st;
     if ((st = dev_alloc(&h->isl_faces, (size_t)std::max(1, h->nf), A))) return st;
     if ((st = dev_alloc(&h->isl_count, 2, A))) return st;
-    if ((st = dev_alloc(&h->isl_fstar, (size_t)h->nf * h->neq * nfp, A))) return st;
+    if ((st = dev_alloc(&h->isl_fstar, (size_t)(h->nf + h->nbf) * h->neq * nfp, A))) return st;
     if ((st = dev_alloc(&h->isl_alpha, (size_t)h->ne, A))) return st;
     if ((st = dev_alloc(&h->isl_eta, (size_t)h->ne, A))) return st;
     if ((st = dev_alloc(&h->isl_fvrate, (size_t)h->L * h->neq, A))) return st;
@@ -775,8 +787,9 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if (isl) {
     const int nblk = (h->ne + h->isl_epb - 1) / h->isl_epb;
     if (cudaMemsetAsync(h->isl_count, 0, 2 * sizeof(int), s) != cudaSuccess) return THX_ERR_CUDA;
-    island_blocks_kernel<R><<<(nblk + 255) / 256, 256, 0, s>>>(h->ne, h->isl_epb, h->alpha, h->isl_flag,
-                                                               h->isl_blocks, h->isl_count);
+    island_blocks_kernel<R><<<(nblk + 255) / 256, 256, 0, s>>>(
+        h->ne, h->isl_epb, h->isl_alpha_in ? h->alpha : nullptr, h->isl_static, h->isl_flag,
+        h->isl_blocks, h->isl_count);
     if (h->nf > 0)
       island_faces_kernel<<<(h->nf + 255) / 256, 256, 0, s>>>(h->nf, h->isl_epb, h->face_elem, h->isl_flag,
                                                               h->isl_faces, h->isl_count + 1);
@@ -785,7 +798,7 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     b.threshold = h->threshold; b.sharpness = h->cfg.sharpness;
     b.alpha_min = h->cfg.alpha_min; b.alpha_max = h->cfg.alpha_max;
     b.alpha = h->isl_alpha; b.eta = h->isl_eta;
-    if (h->isl_blend(b, h->isl_blocks, h->isl_count, s) != cudaSuccess) return THX_ERR_CUDA;
+    if (h->blend && h->isl_blend(b, h->isl_blocks, h->isl_count, s) != cudaSuccess) return THX_ERR_CUDA;
     op_args<double>(h, u64, du64, stage, dt, um, y, yf, ga64, fa64, va64);
     fa64.fstar = h->isl_fstar;
     fa64.order = h->isl_faces;
@@ -807,6 +820,15 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if (ev) cudaEventRecord(ev[2], s);
   if (facek(h, tag)(fa, s) != cudaSuccess) return THX_ERR_CUDA;
   if (isl && h->isl_face(fa64, h->isl_count + 1, s) != cudaSuccess) return THX_ERR_CUDA;
+  if (isl && h->nbf > 0) {
+    // boundary faces in FP64 into the islands' face fluxes
+    BndArgs ba;
+    ba.u = u64; ba.ne = h->ne; ba.N = h->N; ba.nbf = h->nbf; ba.f0 = h->nf;
+    ba.bdr_elem = h->bdr_elem; ba.bdr_lface = h->bdr_lface; ba.bdr_bc = h->bdr_bc;
+    ba.normal = h->bdr_nrm; ba.bcs = h->bcs; ba.bc_data = h->bc_data; ba.bgrad = h->bgrad;
+    ba.fstar = h->isl_fstar; ba.gas = h->g64;
+    if (h->isl_bnd(ba, s) != cudaSuccess) return THX_ERR_CUDA;
+  }
   if constexpr (!IsF32<R>::value) {
     if (h->nbf > 0) {
       BndArgs ba;
@@ -818,13 +840,12 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
     }
   }
   if (ev) cudaEventRecord(ev[3], s);
-  if (isl) {
-    // the FP64 subcell rate of the listed blocks; the FP32 kernel has no
-    // blended block left to evaluate
+  if (isl && h->blend) {
+    // the FP64 subcell rate of the listed blocks
     if (h->isl_fv(va64, h->isl_blocks, h->isl_count, s, 0) != cudaSuccess) return THX_ERR_CUDA;
-  } else if (h->blend && fvk(h, tag)(va, s, 0) != cudaSuccess) {
-    return THX_ERR_CUDA;
   }
+  // the FP32 subcell rate, for blended elements outside the islands
+  if (h->blend && !(isl && h->isl_alpha_in) && fvk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (volk(h, tag)(va, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (isl && h->isl_vol(va64, h->isl_blocks, h->isl_count, s, 0) != cudaSuccess) return THX_ERR_CUDA;
   if (ev) cudaEventRecord(ev[4], s);

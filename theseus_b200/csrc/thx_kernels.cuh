@@ -1858,16 +1858,18 @@ face_batched(const FaceArgs<R> *__restrict__ args, const BatchWork *__restrict__
 // the flagged blocks.  The list walkers are persistent grids that read the
 // list length on the device, so a captured graph stays valid.
 
-// flag[b] = block b holds an element with alpha > 0; flagged blocks are
-// appended to list (count zeroed beforehand)
+// flag[b] = block b holds an element with alpha > 0 (alpha may be null) or is
+// flagged in stat (may be null: blocks next to a boundary face); flagged
+// blocks are appended to list (count zeroed beforehand)
 template <typename R>
 __global__ void island_blocks_kernel(int ne, int epb, const double *__restrict__ alpha,
-                                     int *__restrict__ flag, int *__restrict__ list, int *count) {
+                                     const int *__restrict__ stat, int *__restrict__ flag,
+                                     int *__restrict__ list, int *count) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nb = (ne + epb - 1) / epb;
   if (b >= nb) return;
-  bool any = false;
-  for (int k = 0; k < epb; ++k) {
+  bool any = stat && stat[b];
+  for (int k = 0; alpha && k < epb; ++k) {
     const int e = b * epb + k;
     if (e < ne && alpha[e] > 0.0) any = true;
   }

@@ -147,6 +147,9 @@ struct thx_operator_s {
   int isl_epb = 1;
   int *isl_flag = nullptr, *isl_blocks = nullptr, *isl_faces = nullptr;
   int *isl_count = nullptr;  // [0] blocks, [1] faces
+  int *isl_static = nullptr; // blocks next to a boundary face (islands at every RHS)
+  bool isl_alpha_in = false; // blended blocks are islands
+  thx::BndLaunch isl_bnd = nullptr;
   double *isl_fstar = nullptr, *isl_alpha = nullptr, *isl_eta = nullptr, *isl_fvrate = nullptr;
   thx::VolListLaunch<double> isl_vol = nullptr, isl_fv = nullptr;
   thx::BlendListLaunch<double> isl_blend = nullptr;
