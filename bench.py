@@ -785,7 +785,7 @@ def run_serving(args):
     host = {}
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         try:
-            _, lat, makespan = serve(eng, reqs, on_result=keep, host=host)
+            _, lat, makespan = serve(eng, reqs, on_result=keep, host=host, admitters=args.admitters)
         except Exception:
             free, total = torch.cuda.mem_get_info()
             print(json.dumps({"serving_failed": True, "engine": eng.stats(), "host_seconds": host,
@@ -802,6 +802,7 @@ def run_serving(args):
                        "arrival_rate_per_s": 2000.0, "sides": [8, 64], "orders": [2, 5],
                        "mach": [0.1, 2.0], "reynolds": [100, 1e4], "inviscid_fraction": 0.5,
                        "steps_per_case": 200, "steps_per_launch": args.chunk,
+                       "admitters": args.admitters,
                        "mean_nodes_per_case": float(np.mean(nodes)), "fluxes": flux},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
@@ -1073,6 +1074,8 @@ def main():
     ap.add_argument("--cases", type=int, default=4096, help="serving: cases in the stream")
     ap.add_argument("--sample", type=int, default=256, help="serving: cases also run one at a time")
     ap.add_argument("--chunk", type=int, default=10, help="serving: SSP-RK3 steps per graph launch")
+    ap.add_argument("--admitters", type=int, default=1,
+                    help="serving: host threads setting up arriving cases (1: strict arrival order)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
