@@ -793,6 +793,7 @@ def run_serving(args):
                               "budget_bytes": eng.hbm_budget}), file=sys.stderr, flush=True)
             raise
     st = eng.stats()
+    tuned = eng.groups()
     eng.close()
     nodes = [r.mesh.num_nodes for r in reqs]
     line = {"metric": "solves/s (batched serving, FP32-mixed, 200 SSP-RK3 steps per case)",
@@ -817,7 +818,7 @@ def run_serving(args):
                                               "norm": "per conserved field (rho, momentum, E)",
                                               "worst": [dict(p, err=e) for e, p in
                                                         sorted(worst, key=lambda x: -x[0])[:3]]},
-            "engine": st, "host_seconds": host, "clocks": clk.summary()}
+            "engine": st, "engine_groups": tuned, "host_seconds": host, "clocks": clk.summary()}
     return line
 
 

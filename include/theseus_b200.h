@@ -547,6 +547,26 @@ int thx_engine_poll(thx_engine e, int64_t *ids, int cap, int *count);
 int thx_engine_fetch(thx_engine e, int64_t id, double *u_host);
 int thx_engine_get_stats(thx_engine e, thx_engine_stats *out);
 
+/* One batch group of the engine (cases of the same dimension, order and
+ * flow model share persistent batched kernels and one CUDA graph).  The
+ * engine tunes the grids of those kernels online by coordinate search: the
+ * volume grid over {1,2,4} x SMs, then the face grid over {4,8,16} x SMs,
+ * then (Navier-Stokes) the gradient grid over {1,2,4} x SMs, each candidate
+ * timed with CUDA events around one launch that advances real cases; cost =
+ * device milliseconds per (case work item x step).  Elements per CTA are
+ * fixed per (dimension, order) at compile time. */
+typedef struct {
+  int32_t dim, order, navier_stokes;
+  int32_t active_cases;
+  int32_t tuned;          /* 1 once every axis has been searched */
+  int32_t volume_grid, face_grid, gradient_grid;  /* the best so far */
+  int32_t elements_per_block;
+  double best_cost_ms;    /* cost of the best grids on the axis being searched
+                             (-1 before its first timing) */
+} thx_engine_group;
+/* Up to cap groups in key order; *count = the number of groups. */
+int thx_engine_groups(thx_engine e, thx_engine_group *out, int cap, int *count);
+
 /* Diagnostics of the configured kernels (for roofline bookkeeping). */
 int thx_describe(thx_handle h, char *buf, size_t len);
 

@@ -120,6 +120,44 @@ def test_engine_matches_one_case_runs(cuda, precision):
     eng.close()
 
 
+def test_engine_grid_tuning(cuda):
+    """The online tuner searches the volume, face and (Navier-Stokes) gradient
+    grids of each batch group; the result stays bit-identical to the one-case
+    run whatever grids the launches used."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    batch = [vortex_case(2, 3, (6, 6), True, 300, seed=1), vortex_case(2, 3, (5, 7), True, 300, seed=2),
+             vortex_case(2, 4, (6, 6), False, 300, seed=3)]
+    eng = BatchEngine(precision="fp64", steps_per_launch=3, **FLUX)
+    ids = {eng.admit(c): i for i, c in enumerate(batch)}
+    seen = None
+    out = [None] * len(batch)
+    for _ in range(100000):
+        if not ids:
+            break
+        eng.advance()
+        if len(ids) == len(batch):
+            seen = eng.groups()
+        for cid in eng.poll():
+            i = ids.pop(cid)
+            out[i] = eng.fetch(cid, batch[i].u0.shape)
+    assert seen is not None and len(seen) == 2
+    ns = {g["navier_stokes"]: g for g in seen}
+    assert set(ns) == {0, 1}
+    for g in seen:
+        assert g["dim"] == 2 and g["order"] in (3, 4)
+        assert g["volume_grid"] in (sms, 2 * sms, 4 * sms)
+        assert g["face_grid"] in (4 * sms, 8 * sms, 16 * sms)
+        assert g["elements_per_block"] >= 1
+    assert ns[1]["gradient_grid"] in (sms, 2 * sms, 4 * sms) and ns[0]["gradient_grid"] == 0
+    final = eng.groups()
+    # 100 launches per group are far more than the 9 timed ones the search needs
+    assert all(g["tuned"] == 1 and g["active_cases"] == 0 and g["best_cost_ms"] > 0 for g in final), final
+    for c, g in zip(batch, out):
+        assert np.array_equal(g, alone(c, "fp64"))
+    eng.close()
+
+
 def test_engine_result_independent_of_the_mix(cuda):
     target = vortex_case(2, 3, (5, 5), True, 20, seed=42)
     e1 = BatchEngine(precision="fp32", steps_per_launch=5, **FLUX)

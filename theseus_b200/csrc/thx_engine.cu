@@ -80,6 +80,7 @@ struct EngineBase {
   virtual int poll(int64_t *ids, int cap, int *count) = 0;
   virtual int fetch(int64_t id, double *u_host) = 0;
   virtual void stats(thx_engine_stats *st) = 0;
+  virtual int groups(thx_engine_group *out, int cap) = 0;
 };
 
 template <typename R>
@@ -111,17 +112,27 @@ struct Group {
   FaceBatchLaunch<R> faceb = nullptr;
   GradBatchLaunch<R> gradb = nullptr;
   cudaGraphExec_t exec = nullptr;
-  int exec_grid = -1;
+  // grids of the persistent kernels in the captured graph
+  struct Grids {
+    int vol = 0, face = 0, grad = 0;
+    bool operator==(const Grids &o) const { return vol == o.vol && face == o.face && grad == o.grad; }
+  };
+  Grids exec_grids;
   // launches in flight: at most two per group, so that newly admitted cases
   // join after a short queue
   cudaEvent_t ring[2] = {nullptr, nullptr};
   int ring_pos = 0;
-  // online tuning of the volume grid
-  std::vector<int> candidates;
-  std::vector<double> cost;
-  int next_candidate = 0, chosen = -1;
+  // online tuning: coordinate search over the volume grid, then the face
+  // grid, then (Navier-Stokes) the gradient grid, each over a few multiples
+  // of the SM count, cost = device time of a launch / work items; every
+  // tuning launch advances real cases
+  Grids best;
+  double best_cost = -1.0;
+  int tune_axis = 0, tune_index = 0;  // axis 0 volume, 1 face, 2 gradient; 3: done
+  bool tuned = false;
+  Grids timing_grids;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
-  int timing_candidate = -1;
+  bool timing = false;
   long long timing_work = 0;
 };
 
@@ -369,6 +380,29 @@ class Engine final : public EngineBase {
     return THX_OK;
   }
 
+  int groups(thx_engine_group *out, int cap) override {
+    std::lock_guard<std::mutex> lock(mu_);
+    int n = 0;
+    for (auto &kv : groups_) {
+      Group<R> &G = *kv.second;
+      if (n < cap) {
+        thx_engine_group &o = out[n];
+        o.dim = G.dim;
+        o.order = G.N - 1;
+        o.navier_stokes = G.ns ? 1 : 0;
+        o.active_cases = (int32_t)G.cases.size();
+        o.tuned = G.tuned ? 1 : 0;
+        o.volume_grid = G.best.vol;
+        o.face_grid = G.best.face;
+        o.gradient_grid = G.ns ? G.best.grad : 0;
+        o.elements_per_block = G.epb;
+        o.best_cost_ms = G.best_cost;
+      }
+      ++n;
+    }
+    return n;
+  }
+
   void stats(thx_engine_stats *st) override {
     std::lock_guard<std::mutex> lock(mu_);
     st->active_cases = (int32_t)cases_.size();
@@ -479,8 +513,9 @@ class Engine final : public EngineBase {
       cudaGetLastError();
       return THX_ERR_CUDA;
     }
-    for (int m : {1, 2, 4}) G->candidates.push_back(m * sms_);
-    G->cost.assign(G->candidates.size(), -1.0);
+    G->best.vol = 1 * sms_;
+    G->best.face = 8 * sms_;
+    G->best.grad = 2 * sms_;
     *out = G.get();
     groups_[key] = std::move(G);
     return THX_OK;
@@ -608,12 +643,12 @@ class Engine final : public EngineBase {
     return THX_OK;
   }
 
-  int capture(Group<R> &G, int grid) {
+  int capture(Group<R> &G, const typename Group<R>::Grids &gr) {
     if (G.exec) {
       cudaGraphExecDestroy(G.exec);
       G.exec = nullptr;
     }
-    const int gf = 8 * sms_, gg = 2 * sms_;
+    const int grid = gr.vol, gf = gr.face, gg = gr.grad;
     cudaGraph_t graph = nullptr;
     THX_CU(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaSuccess;
@@ -636,25 +671,45 @@ class Engine final : public EngineBase {
       G.exec = nullptr;
       return cuda_failed(e, "cudaGraphInstantiate");
     }
-    G.exec_grid = grid;
+    G.exec_grids = gr;
     return THX_OK;
+  }
+
+  // candidate `index` on the current tuning axis (false when the axis is done)
+  bool tune_candidate(const Group<R> &G, int index, typename Group<R>::Grids &out) const {
+    static const int vol_m[] = {1, 2, 4}, face_m[] = {4, 8, 16}, grad_m[] = {1, 2, 4};
+    if (index >= 3) return false;
+    out = G.best;
+    if (G.tune_axis == 0) out.vol = vol_m[index] * sms_;
+    else if (G.tune_axis == 1) out.face = face_m[index] * sms_;
+    else out.grad = grad_m[index] * sms_;
+    return true;
   }
 
   // collect the timing of the previous tuning launch, if it has finished
   void collect_timing(Group<R> &G) {
-    if (G.timing_candidate < 0) return;
+    if (!G.timing) return;
     if (cudaEventQuery(G.t1) != cudaSuccess) {
       cudaGetLastError();
       return;
     }
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, G.t0, G.t1) == cudaSuccess && G.timing_work > 0)
-      G.cost[G.timing_candidate] = ms / (double)G.timing_work;
-    G.timing_candidate = -1;
-    bool all = true;
-    for (double c : G.cost) all = all && c >= 0.0;
-    if (all && G.chosen < 0)
-      G.chosen = (int)(std::min_element(G.cost.begin(), G.cost.end()) - G.cost.begin());
+    G.timing = false;
+    if (cudaEventElapsedTime(&ms, G.t0, G.t1) == cudaSuccess && G.timing_work > 0) {
+      const double c = ms / (double)G.timing_work;
+      if (G.best_cost < 0.0 || c < G.best_cost) {
+        G.best_cost = c;
+        G.best = G.timing_grids;
+      }
+    }
+    if (++G.tune_index >= 3) {
+      G.tune_index = 0;
+      ++G.tune_axis;
+      if (G.tune_axis == 2 && !G.ns) ++G.tune_axis;
+      if (G.tune_axis >= 3) G.tuned = true;
+      // a new axis starts from the best so far: its cost is re-measured
+      else G.best_cost = -1.0;
+    }
   }
 
   int advance_group(Group<R> &G) {
@@ -686,23 +741,19 @@ class Engine final : public EngineBase {
     THX_CU(cudaStreamWaitEvent(G.stream, setup_done_, 0));
     int st;
     if (G.dirty && (st = upload_tables(G))) return st;
-    int cand = -1, grid;
-    if (G.chosen >= 0) {
-      grid = G.candidates[G.chosen];
-    } else if (G.timing_candidate < 0 && G.next_candidate < (int)G.candidates.size()) {
-      cand = G.next_candidate++;
-      grid = G.candidates[cand];
-    } else {
-      grid = G.exec_grid > 0 ? G.exec_grid : G.candidates[0];
+    typename Group<R>::Grids grids = G.best;
+    bool measure = false;
+    if (!G.tuned && !G.timing && tune_candidate(G, G.tune_index, grids)) measure = true;
+    else if (!G.tuned && G.timing && G.exec) grids = G.exec_grids;
+    if (!G.exec || !(G.exec_grids == grids)) {
+      if ((st = capture(G, grids))) return st;
     }
-    if (!G.exec || G.exec_grid != grid) {
-      if ((st = capture(G, grid))) return st;
-    }
-    if (cand >= 0) cudaEventRecord(G.t0, G.stream);
+    if (measure) cudaEventRecord(G.t0, G.stream);
     THX_CU(cudaGraphLaunch(G.exec, G.stream));
-    if (cand >= 0) {
+    if (measure) {
       cudaEventRecord(G.t1, G.stream);
-      G.timing_candidate = cand;
+      G.timing = true;
+      G.timing_grids = grids;
       G.timing_work = (long long)G.nwv * k_;
     }
     ++launches_;
@@ -873,6 +924,12 @@ int thx_engine_fetch(thx_engine e, int64_t id, double *u_host) {
 int thx_engine_get_stats(thx_engine e, thx_engine_stats *out) {
   if (!e || !out) return THX_ERR_INVALID_ARGUMENT;
   e->impl->stats(out);
+  return THX_OK;
+}
+
+int thx_engine_groups(thx_engine e, thx_engine_group *out, int cap, int *count) {
+  if (!e || !count || cap < 0 || (cap > 0 && !out)) return THX_ERR_INVALID_ARGUMENT;
+  *count = e->impl->groups(out, cap);
   return THX_OK;
 }
 

@@ -44,6 +44,13 @@ class EngineStats(C.Structure):
                 ("pool_reserved_bytes", C.c_int64), ("pool_used_bytes", C.c_int64)]
 
 
+class EngineGroup(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("order", C.c_int32), ("navier_stokes", C.c_int32),
+                ("active_cases", C.c_int32), ("tuned", C.c_int32), ("volume_grid", C.c_int32),
+                ("face_grid", C.c_int32), ("gradient_grid", C.c_int32),
+                ("elements_per_block", C.c_int32), ("best_cost_ms", C.c_double)]
+
+
 def _bind(lib):
     if getattr(lib, "_engine_bound", False):
         return lib
@@ -56,6 +63,7 @@ def _bind(lib):
     lib.thx_engine_poll.argtypes = [P, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]
     lib.thx_engine_fetch.argtypes = [P, C.c_int64, C.c_void_p]
     lib.thx_engine_get_stats.argtypes = [P, C.POINTER(EngineStats)]
+    lib.thx_engine_groups.argtypes = [P, C.POINTER(EngineGroup), C.c_int, C.POINTER(C.c_int)]
     lib.thx_case_footprint.argtypes = [C.POINTER(Geometry), C.c_void_p, C.c_int,
                                        C.POINTER(C.c_size_t)]
     lib._engine_bound = True
@@ -162,6 +170,16 @@ class BatchEngine:
         s = EngineStats()
         _check(self.lib.thx_engine_get_stats(self._h, C.byref(s)), "thx_engine_get_stats")
         return {k: getattr(s, k) for k, _ in EngineStats._fields_}
+
+    def groups(self):
+        """Per batch group: dimension, order, flow model, active cases and the
+        kernel grids the online tuner has chosen so far (tuned = 1 once the
+        volume, face and gradient grids have all been searched)."""
+        n = C.c_int()
+        _check(self.lib.thx_engine_groups(self._h, None, 0, C.byref(n)), "thx_engine_groups")
+        arr = (EngineGroup * max(1, n.value))()
+        _check(self.lib.thx_engine_groups(self._h, arr, n.value, C.byref(n)), "thx_engine_groups")
+        return [{k: getattr(arr[i], k) for k, _ in EngineGroup._fields_} for i in range(n.value)]
 
 
 def serve(engine, requests, clock=time.perf_counter, idle_sleep=2e-4, on_result=None, host=None,
