@@ -522,6 +522,12 @@ typedef struct {
   double fetch_copy_s;       /* host seconds copying results to the host */
   int64_t pool_reserved_bytes;  /* device memory the engine's pool holds */
   int64_t pool_used_bytes;      /* of which allocated to cases */
+  int64_t advance_calls;        /* calls of thx_engine_advance */
+  double advance_tables_s;      /* of advance_s: rewriting and uploading group tables */
+  double advance_launch_s;      /* of advance_s: graph captures and launches */
+  int64_t table_bytes;          /* bytes of group tables uploaded */
+  double ring_wait_s;           /* host seconds uploads waited for pinned staging space */
+  double ring_copy_s;           /* host seconds copying uploads into pinned staging */
 } thx_engine_stats;
 
 /* Device bytes one case needs (state, stage copies, scratch, geometry). */

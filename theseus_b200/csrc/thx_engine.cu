@@ -65,6 +65,7 @@ struct EngineCase {
   int steps_left = 0;
   size_t bytes = 0;
   cudaEvent_t done = nullptr;
+  cudaEvent_t ready = nullptr;  // recorded on the set-up stream after the case's uploads
   bool finished = false;   // all steps enqueued; done recorded
   bool fetching = false;   // a fetch is copying the result
   // the case's kernel arguments of SSP-RK3 stages 1..3 (VolArgs, FaceArgs,
@@ -89,6 +90,10 @@ struct Group {
   bool ns = false;
   int epb = 1, nfp = 1;
   std::vector<EngineCase *> cases;
+  // admitted cases whose set-up may still run on the set-up stream: they join
+  // `cases` once their ready event has completed, so a group's launches never
+  // wait on the set-up stream
+  std::vector<EngineCase *> pending;
   bool dirty = true;
   cudaStream_t stream = nullptr;
   // device tables: [stage 1..3][cap] argument records, work lists, counts
@@ -106,6 +111,7 @@ struct Group {
   size_t staging_bytes[kStaging] = {0, 0, 0};
   cudaEvent_t staged[kStaging] = {nullptr, nullptr, nullptr};
   int stage_pos = 0;
+  std::vector<unsigned char *> retired;  // outgrown staging buffers
   int nwv = 0, nwf = 0;
   // kernels and graph
   VolBatchLaunch<R> volb = nullptr;
@@ -154,9 +160,13 @@ class Engine final : public EngineBase {
     THX_CU(cudaMemPoolCreate(&pool_, &props));
     uint64_t keep = ~uint64_t(0);  // keep freed memory in the pool
     cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
-    THX_CU(cudaStreamCreateWithFlags(&setup_, cudaStreamNonBlocking));
+    // set-up work (uploads, the working-copy conversion) at the highest
+    // priority: its small kernels take the first free CTA slots between the
+    // persistent batched kernels
+    int least = 0, greatest = 0;
+    THX_CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    THX_CU(cudaStreamCreateWithPriority(&setup_, cudaStreamNonBlocking, greatest));
     if (ring_.init(size_t(64) << 20) != THX_OK) return THX_ERR_OUT_OF_MEMORY;
-    THX_CU(cudaEventCreateWithFlags(&setup_done_, cudaEventDisableTiming));
     return THX_OK;
   }
 
@@ -179,7 +189,6 @@ class Engine final : public EngineBase {
       cudaStreamSynchronize(setup_);
       cudaStreamDestroy(setup_);
     }
-    if (setup_done_) cudaEventDestroy(setup_done_);
     for (Bounce &b : bounce_) cudaFreeHost(b.ptr);
     if (pool_) cudaMemPoolDestroy(pool_);
   }
@@ -255,6 +264,9 @@ class Engine final : public EngineBase {
       op_free(h);
       delete h;
       ec->h = nullptr;
+      if (ec->done) cudaEventDestroy(ec->done);
+      if (ec->ready) cudaEventDestroy(ec->ready);
+      ec->done = ec->ready = nullptr;
       return unreserve(st);
     };
     int st = op_create(g, &cc, h, nullptr, donor);
@@ -281,7 +293,9 @@ class Engine final : public EngineBase {
     const double t2 = now();
     if (ring_.copy(ec->u, u0, n * sizeof(double), setup_) != THX_OK ||
         (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
-        cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ec->ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(ec->ready, setup_) != cudaSuccess) {
       cudaGetLastError();
       return fail(THX_ERR_CUDA);
     }
@@ -290,26 +304,16 @@ class Engine final : public EngineBase {
     t_lock_ += now() - t3;
     t_setup_ += t2 - t1;
     t_copy_ += t3 - t2;
-    // the groups wait on the latest record before their next launch
-    if (cudaEventRecord(setup_done_, setup_) != cudaSuccess) {
-      cudaGetLastError();
-      op_free(h);
-      delete h;
-      bytes_ -= bytes;
-      return THX_ERR_CUDA;
-    }
     Group<R> *G = nullptr;
     if ((st = group_for(h, &G))) {
-      op_free(h);
-      delete h;
-      bytes_ -= bytes;
+      ec->bytes = bytes;
+      release(ec.get(), true);
       return st;
     }
     ec->id = next_id_++;
     ec->steps_left = c->nsteps;
     ec->bytes = bytes;
-    G->cases.push_back(ec.get());
-    G->dirty = true;
+    G->pending.push_back(ec.get());
     *id = ec->id;
     cases_[ec->id] = std::move(ec);
     return THX_OK;
@@ -318,6 +322,7 @@ class Engine final : public EngineBase {
   int advance() override {
     std::lock_guard<std::mutex> lock(mu_);
     const double t0 = now();
+    ++n_advance_;
     for (auto &kv : groups_) {
       int st = advance_group(*kv.second);
       if (st) return st;
@@ -390,7 +395,7 @@ class Engine final : public EngineBase {
         o.dim = G.dim;
         o.order = G.N - 1;
         o.navier_stokes = G.ns ? 1 : 0;
-        o.active_cases = (int32_t)G.cases.size();
+        o.active_cases = (int32_t)(G.cases.size() + G.pending.size());
         o.tuned = G.tuned ? 1 : 0;
         o.volume_grid = G.best.vol;
         o.face_grid = G.best.face;
@@ -421,6 +426,11 @@ class Engine final : public EngineBase {
     v = 0;
     st->pool_used_bytes =
         cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrUsedMemCurrent, &v) == cudaSuccess ? (int64_t)v : -1;
+    st->advance_calls = n_advance_;
+    st->advance_tables_s = t_tables_;
+    st->advance_launch_s = t_launch_;
+    st->table_bytes = table_bytes_;
+    ring_.times(&st->ring_wait_s, &st->ring_copy_s);
   }
 
  private:
@@ -475,6 +485,8 @@ class Engine final : public EngineBase {
     }
     if (c->done) cudaEventDestroy(c->done);
     c->done = nullptr;
+    if (c->ready) cudaEventDestroy(c->ready);
+    c->ready = nullptr;
     if (account) bytes_ -= c->bytes;
   }
 
@@ -536,6 +548,7 @@ class Engine final : public EngineBase {
       if (G.staging[i]) cudaFreeHost(G.staging[i]);
       if (G.staged[i]) cudaEventDestroy(G.staged[i]);
     }
+    for (unsigned char *p : G.retired) cudaFreeHost(p);
     if (G.t0) cudaEventDestroy(G.t0);
     if (G.t1) cudaEventDestroy(G.t1);
     for (cudaEvent_t ev : G.ring)
@@ -553,28 +566,37 @@ class Engine final : public EngineBase {
     }
     bool grow = nc > G.cap_cases || nwv > G.cap_wv || nwf > G.cap_wf;
     if (grow) {
-      // buffers may be read by a launch in flight: wait, then reallocate
-      THX_CU(cudaStreamSynchronize(G.stream));
-      auto grow_to = [](int need, int have) { return std::max(need, std::max(16, 2 * have)); };
+      // Stream-ordered reallocation on the group's stream: the old tables are
+      // freed after the launches in flight that read them, and nothing here
+      // waits for the device (cudaMalloc/cudaFree would synchronise it with
+      // every other group's launches).  A graph in flight is released by the
+      // runtime when it completes.
+      auto grow_to = [](int need, int have) { return std::max(need, std::max(64, 2 * have)); };
       const int cc = nc > G.cap_cases ? grow_to(nc, G.cap_cases) : G.cap_cases;
       const int cv = nwv > G.cap_wv ? grow_to(nwv, G.cap_wv) : G.cap_wv;
       const int cf = nwf > G.cap_wf ? grow_to(nwf, G.cap_wf) : G.cap_wf;
-      cudaFree(G.dvol); cudaFree(G.dface); cudaFree(G.dgrad); cudaFree(G.dwv); cudaFree(G.dwf);
+      void *old[5] = {G.dvol, G.dface, G.dgrad, G.dwv, G.dwf};
       G.dvol = nullptr; G.dface = nullptr; G.dgrad = nullptr; G.dwv = nullptr; G.dwf = nullptr;
-      if (cudaMalloc(&G.dvol, sizeof(VolArgs<R>) * 3 * cc) != cudaSuccess ||
-          cudaMalloc(&G.dface, sizeof(FaceArgs<R>) * 3 * cc) != cudaSuccess ||
-          cudaMalloc(&G.dgrad, sizeof(GradArgs<R>) * 3 * cc) != cudaSuccess ||
-          cudaMalloc(&G.dwv, sizeof(BatchWork) * cv) != cudaSuccess ||
-          cudaMalloc(&G.dwf, sizeof(BatchWork) * cf) != cudaSuccess ||
-          (!G.dcount && cudaMalloc(&G.dcount, sizeof(int) * 2) != cudaSuccess))
-        return cuda_failed(cudaGetLastError(), "cudaMalloc(group tables)", THX_ERR_OUT_OF_MEMORY);
-      G.cap_cases = cc;
-      G.cap_wv = cv;
-      G.cap_wf = cf;
       if (G.exec) {
         cudaGraphExecDestroy(G.exec);
         G.exec = nullptr;
       }
+      for (void *q : old)
+        if (q) cudaFreeAsync(q, G.stream);
+      auto get = [&](void **q, size_t bytes) {
+        return cudaMallocFromPoolAsync(q, bytes, pool_, G.stream) == cudaSuccess;
+      };
+      if (!get((void **)&G.dvol, sizeof(VolArgs<R>) * 3 * cc) ||
+          !get((void **)&G.dface, sizeof(FaceArgs<R>) * 3 * cc) ||
+          !get((void **)&G.dgrad, sizeof(GradArgs<R>) * 3 * cc) ||
+          !get((void **)&G.dwv, sizeof(BatchWork) * cv) || !get((void **)&G.dwf, sizeof(BatchWork) * cf) ||
+          (!G.dcount && !get((void **)&G.dcount, sizeof(int) * 2))) {
+        G.cap_cases = G.cap_wv = G.cap_wf = 0;
+        return cuda_failed(cudaGetLastError(), "cudaMallocFromPoolAsync(group tables)", THX_ERR_OUT_OF_MEMORY);
+      }
+      G.cap_cases = cc;
+      G.cap_wv = cv;
+      G.cap_wf = cf;
     }
     const size_t bv = sizeof(VolArgs<R>) * 3 * nc, bf = sizeof(FaceArgs<R>) * 3 * nc;
     const size_t bg = sizeof(GradArgs<R>) * 3 * nc;
@@ -583,9 +605,11 @@ class Engine final : public EngineBase {
     const int slot = G.stage_pos;
     THX_CU(cudaEventSynchronize(G.staged[slot]));  // this slot's last copies are done
     if (need > G.staging_bytes[slot]) {
-      if (G.staging[slot]) cudaFreeHost(G.staging[slot]);
+      // cudaFreeHost would synchronise the device: the outgrown buffer is
+      // kept until the group is destroyed (at most the final size again)
+      if (G.staging[slot]) G.retired.push_back(G.staging[slot]);
       G.staging[slot] = nullptr;
-      G.staging_bytes[slot] = std::max(need, 2 * G.staging_bytes[slot]);
+      G.staging_bytes[slot] = std::max(need, std::max(size_t(1) << 20, 2 * G.staging_bytes[slot]));
       const cudaError_t e =
           cudaHostAlloc((void **)&G.staging[slot], G.staging_bytes[slot], cudaHostAllocDefault);
       if (e != cudaSuccess) {
@@ -636,6 +660,7 @@ class Engine final : public EngineBase {
         cudaMemcpyAsync(G.dcount, hc, sizeof(int) * 2, cudaMemcpyHostToDevice, G.stream) != cudaSuccess ||
         cudaEventRecord(G.staged[slot], G.stream) != cudaSuccess)
       return cuda_failed(cudaGetLastError(), "work list upload");
+    table_bytes_ += (int64_t)(bv + bf + bg + bw + 2 * sizeof(int));
     G.stage_pos = (slot + 1) % Group<R>::kStaging;
     G.nwv = nwv;
     G.nwf = nwf;
@@ -714,11 +739,23 @@ class Engine final : public EngineBase {
 
   int advance_group(Group<R> &G) {
     collect_timing(G);
+    // admitted cases join once their set-up has finished on the device
+    for (size_t i = 0; i < G.pending.size();) {
+      EngineCase *c = G.pending[i];
+      const cudaError_t q = cudaEventQuery(c->ready);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      if (q != cudaSuccess) return cuda_failed(q, "cudaEventQuery(case set-up)");
+      G.cases.push_back(c);
+      G.pending.erase(G.pending.begin() + i);
+      G.dirty = true;
+    }
     // cases with fewer steps left than a launch holds finish one at a time
     for (size_t i = 0; i < G.cases.size();) {
       EngineCase *c = G.cases[i];
       if (c->steps_left < k_) {
-        THX_CU(cudaStreamWaitEvent(G.stream, setup_done_, 0));
         if (c->steps_left > 0) {
           int st = thx_rk3_steps(c->h, c->u, c->dt, c->steps_left, G.stream);
           if (st) return st;
@@ -738,9 +775,11 @@ class Engine final : public EngineBase {
       if (q == cudaErrorNotReady) return THX_OK;  // two launches still queued
       if (q != cudaSuccess) return cuda_failed(q, "cudaEventQuery(launch ring)");
     }
-    THX_CU(cudaStreamWaitEvent(G.stream, setup_done_, 0));
     int st;
+    const double ta = now();
     if (G.dirty && (st = upload_tables(G))) return st;
+    const double tb = now();
+    t_tables_ += tb - ta;
     typename Group<R>::Grids grids = G.best;
     bool measure = false;
     if (!G.tuned && !G.timing && tune_candidate(G, G.tune_index, grids)) measure = true;
@@ -757,6 +796,7 @@ class Engine final : public EngineBase {
       G.timing_work = (long long)G.nwv * k_;
     }
     ++launches_;
+    t_launch_ += now() - tb;
     THX_CU(cudaEventRecord(G.ring[G.ring_pos], G.stream));
     G.ring_pos ^= 1;
     for (size_t i = 0; i < G.cases.size();) {
@@ -780,7 +820,6 @@ class Engine final : public EngineBase {
   int device_ = 0, sms_ = 148;
   cudaMemPool_t pool_ = nullptr;
   cudaStream_t setup_ = nullptr;
-  cudaEvent_t setup_done_ = nullptr;
   HostRing ring_;                 // pinned staging of admission uploads
   std::mutex bounce_mu_;
   std::vector<Bounce> bounce_;    // pinned buffers of result copies
@@ -790,6 +829,8 @@ class Engine final : public EngineBase {
   int64_t next_id_ = 1, launches_ = 0, done_ = 0;
   // host time accounting (seconds)
   double t_lock_ = 0, t_setup_ = 0, t_copy_ = 0, t_advance_ = 0, t_fetch_ = 0;
+  double t_tables_ = 0, t_launch_ = 0;
+  int64_t n_advance_ = 0, table_bytes_ = 0;
   static double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
   }

@@ -12,6 +12,8 @@
 #include <deque>
 #include <mutex>
 
+#include <chrono>
+
 #include "thx_ring.h"
 
 namespace thx {
@@ -60,6 +62,7 @@ class HostRing {
       return e == cudaSuccess ? THX_OK : cuda_failed(e, "cudaMemcpyAsync(upload)");
     }
     size_t off;
+    const auto t0 = std::chrono::steady_clock::now();
     while (!space_.place(need, &off)) {  // wait for the oldest copy
       const cudaError_t e = cudaEventSynchronize(busy_.front());
       if (e != cudaSuccess) return cuda_failed(e, "cudaEventSynchronize(upload ring)");
@@ -67,7 +70,11 @@ class HostRing {
       busy_.pop_front();
       space_.pop();
     }
+    const auto t1 = std::chrono::steady_clock::now();
     std::memcpy(buf_ + off, src, bytes);
+    const auto t2 = std::chrono::steady_clock::now();
+    wait_s_ += std::chrono::duration<double>(t1 - t0).count();
+    copy_s_ += std::chrono::duration<double>(t2 - t1).count();
     cudaError_t e = cudaMemcpyAsync(dst, buf_ + off, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_failed(e, "cudaMemcpyAsync(upload ring)");
     cudaEvent_t ev;
@@ -88,9 +95,16 @@ class HostRing {
     }
     return THX_OK;
   }
+  // host seconds spent waiting for space and copying into the ring
+  void times(double *wait_s, double *copy_s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    *wait_s = wait_s_;
+    *copy_s = copy_s_;
+  }
 
  private:
   std::mutex mu_;
+  double wait_s_ = 0.0, copy_s_ = 0.0;
   unsigned char *buf_ = nullptr;
   RingSpace space_;
   std::deque<cudaEvent_t> busy_;  // one per live span, oldest first

@@ -41,7 +41,10 @@ class EngineStats(C.Structure):
                 ("launches", C.c_int64), ("cases_done", C.c_int64), ("admit_lock_s", C.c_double),
                 ("admit_setup_s", C.c_double), ("admit_copy_s", C.c_double),
                 ("advance_s", C.c_double), ("fetch_copy_s", C.c_double),
-                ("pool_reserved_bytes", C.c_int64), ("pool_used_bytes", C.c_int64)]
+                ("pool_reserved_bytes", C.c_int64), ("pool_used_bytes", C.c_int64),
+                ("advance_calls", C.c_int64), ("advance_tables_s", C.c_double),
+                ("advance_launch_s", C.c_double), ("table_bytes", C.c_int64),
+                ("ring_wait_s", C.c_double), ("ring_copy_s", C.c_double)]
 
 
 class EngineGroup(C.Structure):
