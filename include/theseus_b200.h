@@ -555,18 +555,18 @@ int thx_engine_get_stats(thx_engine e, thx_engine_stats *out);
 
 /* One batch group of the engine (cases of the same dimension, order and
  * flow model share persistent batched kernels and one CUDA graph).  The
- * engine tunes the grids of those kernels online by coordinate search: the
- * volume grid over {1,2,4} x SMs, then the face grid over {4,8,16} x SMs,
- * then (Navier-Stokes) the gradient grid over {1,2,4} x SMs, each candidate
- * timed with CUDA events around one launch that advances real cases; cost =
- * device milliseconds per (case work item x step).  Elements per CTA are
- * fixed per (dimension, order) at compile time. */
+ * engine tunes those kernels online by coordinate search: the elements per
+ * CTA of the volume and gradient kernels (as many as fit 256 threads, or
+ * half as many), then the volume grid over {1,2,4} x SMs, the face grid over
+ * {4,8,16} x SMs and (Navier-Stokes) the gradient grid over {1,2,4} x SMs,
+ * each candidate timed with CUDA events around one launch that advances real
+ * cases; cost = device milliseconds per (solution node x step). */
 typedef struct {
   int32_t dim, order, navier_stokes;
   int32_t active_cases;
   int32_t tuned;          /* 1 once every axis has been searched */
   int32_t volume_grid, face_grid, gradient_grid;  /* the best so far */
-  int32_t elements_per_block;
+  int32_t elements_per_block;  /* of the best configuration */
   double best_cost_ms;    /* cost of the best grids on the axis being searched
                              (-1 before its first timing) */
 } thx_engine_group;

@@ -121,9 +121,10 @@ def test_engine_matches_one_case_runs(cuda, precision):
 
 
 def test_engine_grid_tuning(cuda):
-    """The online tuner searches the volume, face and (Navier-Stokes) gradient
-    grids of each batch group; the result stays bit-identical to the one-case
-    run whatever grids the launches used."""
+    """The online tuner searches the elements per CTA and the volume, face and
+    (Navier-Stokes) gradient grids of each batch group; the result stays
+    bit-identical to the one-case run whatever configuration the launches
+    used."""
     import torch
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     batch = [vortex_case(2, 3, (6, 6), True, 300, seed=1), vortex_case(2, 3, (5, 7), True, 300, seed=2),
@@ -148,10 +149,11 @@ def test_engine_grid_tuning(cuda):
         assert g["dim"] == 2 and g["order"] in (3, 4)
         assert g["volume_grid"] in (sms, 2 * sms, 4 * sms)
         assert g["face_grid"] in (4 * sms, 8 * sms, 16 * sms)
-        assert g["elements_per_block"] >= 1
+        full = max(1, 256 // (g["order"] + 1) ** g["dim"])
+        assert g["elements_per_block"] in (full, full // 2)
     assert ns[1]["gradient_grid"] in (sms, 2 * sms, 4 * sms) and ns[0]["gradient_grid"] == 0
     final = eng.groups()
-    # 100 launches per group are far more than the 9 timed ones the search needs
+    # 100 launches per group are far more than the 11 timed ones the search needs
     assert all(g["tuned"] == 1 and g["active_cases"] == 0 and g["best_cost_ms"] > 0 for g in final), final
     for c, g in zip(batch, out):
         assert np.array_equal(g, alone(c, "fp64"))

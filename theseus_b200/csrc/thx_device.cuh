@@ -815,6 +815,83 @@ __device__ __forceinline__ void viscous_flux(const GasT<R> &g, const R *q, const
   }
 }
 
+// Per-node gas quantities shared by the entropy-to-primitive gradient map and
+// the viscous flux at one node, each formed once: the same operations as
+// grad_entropy_to_prim and viscous_flux evaluate (and so the same results),
+// without repeating the divisions for every gradient direction.
+template <typename R, int DIM>
+struct NodeGas {
+  R rho, ke, p, p_rho;  // p_rho = p / rho
+  R v[DIM];             // q[1+d] / rho
+};
+template <typename R, int DIM>
+__device__ __forceinline__ NodeGas<R, DIM> node_gas(const GasT<R> &g, const R *q) {
+  NodeGas<R, DIM> s;
+  s.rho = q[0];
+  s.ke = ke_density<R, DIM>(q);
+  s.p = g.gm1 * (q[DIM + 1] - s.ke);
+  s.p_rho = fdiv(s.p, s.rho);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) s.v[d] = fdiv(q[1 + d], s.rho);
+  return s;
+}
+// grad_entropy_to_prim with the node's quantities precomputed
+template <typename R, int DIM>
+__device__ __forceinline__ void grad_entropy_to_prim_ng(const NodeGas<R, DIM> &s, const R *q, const R *dE,
+                                                        R *dP) {
+  constexpr int E = DIM + 1;
+  const R ie = q[E] - s.ke;
+  R drho = R(0);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    dP[1 + d] = s.p_rho * (dE[1 + d] + s.v[d] * dE[E]);
+    drho += q[1 + d] * dP[1 + d];
+  }
+  drho = s.rho * dE[0] - dE[E] * (s.ke - ie) + fdiv(s.rho * drho, s.p);
+  dP[0] = drho;
+  dP[E] = s.p_rho * (dP[0] + s.p * dE[E]);
+}
+// viscosity() with the node's pressure precomputed
+template <typename R, int DIM>
+__device__ __forceinline__ R viscosity_ng(const GasT<R> &g, const NodeGas<R, DIM> &s) {
+  if (g.sutherland) {
+    const R T = s.p / (s.rho * g.R_gas);
+    const R Trel = T / g.T0;
+    const R T0pTs = g.T0 + g.Ts;
+    return g.mu0 * T0pTs * Trel * rsqrt_(Trel) / (T + g.Ts);
+  }
+  return g.mu;
+}
+
+// viscous_flux with the node's quantities precomputed
+template <typename R, int DIM>
+__device__ __forceinline__ void viscous_flux_ng(const GasT<R> &g, const R *q, const NodeGas<R, DIM> &s,
+                                                const R *dp, R *vf) {
+  constexpr int NEQ = DIM + 2, E = DIM + 1;
+  const R mu = viscosity_ng<R, DIM>(g, s);
+  const R kappa = mu * g.cp * g.Pr_inv;
+  const R fac = fdiv(g.gm1_inv, g.cv * s.rho);
+  R div = R(0);
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) div += dp[i * NEQ + 1 + i];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) vf[d] = R(0);
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    R ef = kappa * (fac * (dp[dir * NEQ + E] - s.p_rho * dp[dir * NEQ + 0]));
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) {
+      R tau;
+      if (mom == dir) tau = mu * (R(2) * dp[dir * NEQ + 1 + mom] - g.mu_bulk * div);
+      else tau = mu * (dp[dir * NEQ + 1 + mom] + dp[mom * NEQ + 1 + dir]);
+      vf[(1 + mom) * DIM + dir] = tau;
+    }
+#pragma unroll
+    for (int mom = 0; mom < DIM; ++mom) ef += s.v[mom] * vf[(1 + mom) * DIM + dir];
+    vf[E * DIM + dir] = ef;
+  }
+}
+
 // include/EOS.hpp:206-234: entropy variables (s_rho, beta*u, -beta), beta = rho/p
 template <typename R, int DIM>
 __device__ __forceinline__ void entropy_vars(const GasT<R> &g, const R *q, R *w) {

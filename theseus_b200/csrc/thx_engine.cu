@@ -88,7 +88,8 @@ template <typename R>
 struct Group {
   int dim = 0, N = 0;
   bool ns = false;
-  int epb = 1, nfp = 1;
+  int epb = 1, nfp = 1;  // epb: elements per CTA of the current tables
+  int epb_full = 1, epb_half = 0;
   std::vector<EngineCase *> cases;
   // admitted cases whose set-up may still run on the set-up stream: they join
   // `cases` once their ready event has completed, so a group's launches never
@@ -113,28 +114,33 @@ struct Group {
   int stage_pos = 0;
   std::vector<unsigned char *> retired;  // outgrown staging buffers
   int nwv = 0, nwf = 0;
+  long long nodes = 0;  // solution nodes of the cases in the tables
   // kernels and graph
-  VolBatchLaunch<R> volb = nullptr;
+  VolBatchLaunch<R> volb = nullptr, volb_half = nullptr;
   FaceBatchLaunch<R> faceb = nullptr;
-  GradBatchLaunch<R> gradb = nullptr;
+  GradBatchLaunch<R> gradb = nullptr, gradb_half = nullptr;
   cudaGraphExec_t exec = nullptr;
   // grids of the persistent kernels in the captured graph
   struct Grids {
     int vol = 0, face = 0, grad = 0;
-    bool operator==(const Grids &o) const { return vol == o.vol && face == o.face && grad == o.grad; }
+    bool half = false;  // half-size CTAs for the volume and gradient kernels
+    bool operator==(const Grids &o) const {
+      return vol == o.vol && face == o.face && grad == o.grad && half == o.half;
+    }
   };
   Grids exec_grids;
   // launches in flight: at most two per group, so that newly admitted cases
   // join after a short queue
   cudaEvent_t ring[2] = {nullptr, nullptr};
   int ring_pos = 0;
-  // online tuning: coordinate search over the volume grid, then the face
-  // grid, then (Navier-Stokes) the gradient grid, each over a few multiples
-  // of the SM count, cost = device time of a launch / work items; every
-  // tuning launch advances real cases
+  // online tuning: coordinate search over the elements per CTA (full or
+  // half-size CTAs), then the volume grid, the face grid and (Navier-Stokes)
+  // the gradient grid, each over a few multiples of the SM count; cost =
+  // device time of a launch / (case nodes x steps); every tuning launch
+  // advances real cases
   Grids best;
   double best_cost = -1.0;
-  int tune_axis = 0, tune_index = 0;  // axis 0 volume, 1 face, 2 gradient; 3: done
+  int tune_axis = 0, tune_index = 0;  // 0 CTA size, 1 volume, 2 face, 3 gradient; 4: done
   bool tuned = false;
   Grids timing_grids;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -400,7 +406,7 @@ class Engine final : public EngineBase {
         o.volume_grid = G.best.vol;
         o.face_grid = G.best.face;
         o.gradient_grid = G.ns ? G.best.grad : 0;
-        o.elements_per_block = G.epb;
+        o.elements_per_block = G.best.half ? G.epb_half : G.epb_full;
         o.best_cost_ms = G.best_cost;
       }
       ++n;
@@ -501,7 +507,6 @@ class Engine final : public EngineBase {
     G->dim = h->dim;
     G->N = h->N;
     G->ns = h->ns;
-    G->epb = std::max(1, 256 / h->nd);
     G->nfp = h->nfp;
     const int vk = (cfg_.volume_flux == THX_FLUX_CHANDRASHEKAR) ? VOL_CHANDRASHEKAR
                  : (cfg_.volume_flux == THX_FLUX_RANOCHA)     ? VOL_RANOCHA
@@ -510,8 +515,12 @@ class Engine final : public EngineBase {
     const int ns = h->ns ? 1 : 0;
     pick_kernels(*G, vk, ns);
     if (!G->volb || !G->faceb || !G->gradb) return THX_ERR_UNSUPPORTED;
+    if (G->epb_half > 0 && (!G->volb_half || !G->gradb_half)) return THX_ERR_UNSUPPORTED;
+    G->epb = G->epb_full;
     if (G->volb(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess ||
-        G->gradb(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess) {
+        G->gradb(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess ||
+        (G->epb_half > 0 && (G->volb_half(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess ||
+                             G->gradb_half(nullptr, nullptr, nullptr, 0, nullptr, 1) != cudaSuccess))) {
       cudaGetLastError();
       return THX_ERR_CUDA;
     }
@@ -528,6 +537,7 @@ class Engine final : public EngineBase {
     G->best.vol = 1 * sms_;
     G->best.face = 8 * sms_;
     G->best.grad = 2 * sms_;
+    G->tune_axis = next_axis(*G, 0);
     *out = G.get();
     groups_[key] = std::move(G);
     return THX_OK;
@@ -663,6 +673,8 @@ class Engine final : public EngineBase {
     table_bytes_ += (int64_t)(bv + bf + bg + bw + 2 * sizeof(int));
     G.stage_pos = (slot + 1) % Group<R>::kStaging;
     G.nwv = nwv;
+    G.nodes = 0;
+    for (EngineCase *c : G.cases) G.nodes += c->h->L;
     G.nwf = nwf;
     G.dirty = false;
     return THX_OK;
@@ -674,15 +686,17 @@ class Engine final : public EngineBase {
       G.exec = nullptr;
     }
     const int grid = gr.vol, gf = gr.face, gg = gr.grad;
+    const VolBatchLaunch<R> volb = gr.half ? G.volb_half : G.volb;
+    const GradBatchLaunch<R> gradb = gr.half ? G.gradb_half : G.gradb;
     cudaGraph_t graph = nullptr;
     THX_CU(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaSuccess;
     for (int step = 0; step < k_ && e == cudaSuccess; ++step)
       for (int stage = 0; stage < 3 && e == cudaSuccess; ++stage) {
         const size_t o = (size_t)stage * G.cap_cases;
-        if (G.ns) e = G.gradb(G.dgrad + o, G.dwv, G.dcount, gg, G.stream, 0);
+        if (G.ns) e = gradb(G.dgrad + o, G.dwv, G.dcount, gg, G.stream, 0);
         if (e == cudaSuccess) e = G.faceb(G.dface + o, G.dwf, G.dcount + 1, gf, G.stream, 0);
-        if (e == cudaSuccess) e = G.volb(G.dvol + o, G.dwv, G.dcount, grid, G.stream, 0);
+        if (e == cudaSuccess) e = volb(G.dvol + o, G.dwv, G.dcount, grid, G.stream, 0);
       }
     const cudaError_t ee = cudaStreamEndCapture(G.stream, &graph);
     if (e != cudaSuccess || ee != cudaSuccess || !graph) {
@@ -701,14 +715,25 @@ class Engine final : public EngineBase {
   }
 
   // candidate `index` on the current tuning axis (false when the axis is done)
+  static int axis_size(const Group<R> &G, int axis) {
+    if (axis == 0) return G.epb_half > 0 ? 2 : 0;
+    if (axis == 3) return G.ns ? 3 : 0;
+    return 3;
+  }
   bool tune_candidate(const Group<R> &G, int index, typename Group<R>::Grids &out) const {
     static const int vol_m[] = {1, 2, 4}, face_m[] = {4, 8, 16}, grad_m[] = {1, 2, 4};
-    if (index >= 3) return false;
+    if (index >= axis_size(G, G.tune_axis)) return false;
     out = G.best;
-    if (G.tune_axis == 0) out.vol = vol_m[index] * sms_;
-    else if (G.tune_axis == 1) out.face = face_m[index] * sms_;
+    if (G.tune_axis == 0) out.half = index == 1;
+    else if (G.tune_axis == 1) out.vol = vol_m[index] * sms_;
+    else if (G.tune_axis == 2) out.face = face_m[index] * sms_;
     else out.grad = grad_m[index] * sms_;
     return true;
+  }
+  // the next axis with candidates (4: the search is done)
+  static int next_axis(const Group<R> &G, int axis) {
+    while (axis < 4 && axis_size(G, axis) == 0) ++axis;
+    return axis;
   }
 
   // collect the timing of the previous tuning launch, if it has finished
@@ -727,11 +752,10 @@ class Engine final : public EngineBase {
         G.best = G.timing_grids;
       }
     }
-    if (++G.tune_index >= 3) {
+    if (++G.tune_index >= axis_size(G, G.tune_axis)) {
       G.tune_index = 0;
-      ++G.tune_axis;
-      if (G.tune_axis == 2 && !G.ns) ++G.tune_axis;
-      if (G.tune_axis >= 3) G.tuned = true;
+      G.tune_axis = next_axis(G, G.tune_axis + 1);
+      if (G.tune_axis >= 4) G.tuned = true;
       // a new axis starts from the best so far: its cost is re-measured
       else G.best_cost = -1.0;
     }
@@ -776,14 +800,20 @@ class Engine final : public EngineBase {
       if (q != cudaSuccess) return cuda_failed(q, "cudaEventQuery(launch ring)");
     }
     int st;
-    const double ta = now();
-    if (G.dirty && (st = upload_tables(G))) return st;
-    const double tb = now();
-    t_tables_ += tb - ta;
     typename Group<R>::Grids grids = G.best;
     bool measure = false;
     if (!G.tuned && !G.timing && tune_candidate(G, G.tune_index, grids)) measure = true;
     else if (!G.tuned && G.timing && G.exec) grids = G.exec_grids;
+    // the work lists follow the CTA size
+    const int epb = grids.half ? G.epb_half : G.epb_full;
+    if (epb != G.epb) {
+      G.epb = epb;
+      G.dirty = true;
+    }
+    const double ta = now();
+    if (G.dirty && (st = upload_tables(G))) return st;
+    const double tb = now();
+    t_tables_ += tb - ta;
     if (!G.exec || !(G.exec_grids == grids)) {
       if ((st = capture(G, grids))) return st;
     }
@@ -793,7 +823,7 @@ class Engine final : public EngineBase {
       cudaEventRecord(G.t1, G.stream);
       G.timing = true;
       G.timing_grids = grids;
-      G.timing_work = (long long)G.nwv * k_;
+      G.timing_work = G.nodes * k_;
     }
     ++launches_;
     t_launch_ += now() - tb;
@@ -847,6 +877,10 @@ void Engine<double>::pick_kernels(Group<double> &G, int vk, int ns) {
     const OrderKernels0 k = order_kernels_##P##_##D##_##NN(); \
     G.volb = k.volb[vk][ns];                                \
     G.gradb = k.gradb;                                      \
+    G.epb_full = k.epb;                                     \
+    G.epb_half = k.epb_half;                                \
+    G.volb_half = k.volb_half[vk][ns];                      \
+    G.gradb_half = k.gradb_half;                            \
   }
   THX_FOR_ORDERS(THX_PICKB, 0, 2)
   THX_FOR_ORDERS(THX_PICKB, 0, 3)
@@ -862,6 +896,10 @@ void Engine<float>::pick_kernels(Group<float> &G, int vk, int ns) {
     const OrderKernels1 k = order_kernels_##P##_##D##_##NN(); \
     G.volb = k.volb[vk][ns];                                \
     G.gradb = k.gradb;                                      \
+    G.epb_full = k.epb;                                     \
+    G.epb_half = k.epb_half;                                \
+    G.volb_half = k.volb_half[vk][ns];                      \
+    G.gradb_half = k.gradb_half;                            \
   }
   THX_FOR_ORDERS(THX_PICKB, 1, 2)
   THX_FOR_ORDERS(THX_PICKB, 1, 3)

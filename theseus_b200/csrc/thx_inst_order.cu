@@ -59,6 +59,23 @@ THX_TYPE(THX_PREC) THX_NAME(THX_PREC, THX_DIM, THX_N)() {
   THX_SETB(VOL_CENTRAL)
 #undef THX_SETB
   k.gradb = &launch_grad_batched<R, THX_DIM, THX_N>;
+  k.epb = Shape<THX_DIM, THX_N>::EPB;
+  k.epb_half = half_epb<THX_DIM, THX_N>();
+  for (auto &row : k.volb_half)
+    for (auto &v : row) v = nullptr;
+  k.gradb_half = nullptr;
+  if constexpr (half_epb<THX_DIM, THX_N>() > 0) {
+    constexpr int H = half_epb<THX_DIM, THX_N>();
+#define THX_SETH(V)                                                                \
+  k.volb_half[V][0] = &launch_volume_batched<R, THX_DIM, THX_N, V, false, H>;      \
+  k.volb_half[V][1] = &launch_volume_batched<R, THX_DIM, THX_N, V, true, H>;
+    THX_SETH(VOL_CHANDRASHEKAR)
+    THX_SETH(VOL_RANOCHA)
+    THX_SETH(VOL_PIROZZOLI)
+    THX_SETH(VOL_CENTRAL)
+#undef THX_SETH
+    k.gradb_half = &launch_grad_batched<R, THX_DIM, THX_N, H>;
+  }
 #if THX_PREC == 0
   k.voll[VOL_CHANDRASHEKAR] = &launch_volume_list<R, THX_DIM, THX_N, VOL_CHANDRASHEKAR>;
   k.voll[VOL_RANOCHA] = &launch_volume_list<R, THX_DIM, THX_N, VOL_RANOCHA>;

@@ -23,12 +23,14 @@
 
 namespace thx {
 
-template <int DIM, int N>
+template <int DIM, int N, int EPBX = 0>
 struct Shape {
   static constexpr int ND = DIM == 2 ? N * N : N * N * N;
   static constexpr int NFP = DIM == 2 ? N : N * N;
   static constexpr int NEQ = DIM + 2;
-  static constexpr int EPB = (256 / ND) > 0 ? 256 / ND : 1;
+  // elements per CTA: as many as fit 256 threads, or EPBX when given (the
+  // batched kernels' half-size variant)
+  static constexpr int EPB = EPBX > 0 ? EPBX : (256 / ND) > 0 ? 256 / ND : 1;
   static constexpr int THREADS = ((EPB * ND + 31) / 32) * 32;
   static constexpr int NP = N * (N - 1) / 2;  // pairs per line
   static constexpr int NLINE = ND / N;
@@ -105,9 +107,9 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes() {
 
 // Shared-memory layout of the volume kernel, in elements of R:
 // [ops | prim + pair fluxes, or the viscous flux | state (NEEDQ) | metric].
-template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int EPBX = 0>
 struct VolSmem {
-  using S = Shape<DIM, N>;
+  using S = Shape<DIM, N, EPBX>;
   static constexpr bool NEEDQ = VOL == VOL_CENTRAL;
   static constexpr int PRIM = VOL == VOL_LTEEC ? S::NEQ + LTE_P_COUNT : nprim<R, DIM>();
   static constexpr int REGION = S::EPB * (PRIM * S::ND + S::PAIRS * S::NEQ);
@@ -180,20 +182,20 @@ __device__ __forceinline__ void surface_flux_rt(int kind, const GasT<R> &g, cons
 // persistent kernel (block from its work list).
 // Stride (in R) between the NEQ arrays of a block's state staged in shared
 // memory: EPB*ND rounded up to 16 bytes, so every array starts 16-byte aligned.
-template <typename R, int DIM, int N>
+template <typename R, int DIM, int N, int EPBX = 0>
 __host__ __device__ constexpr int stage_kstride() {
-  using S = Shape<DIM, N>;
+  using S = Shape<DIM, N, EPBX>;
   return (int)(((size_t)S::EPB * S::ND * sizeof(R) + 15) / 16 * 16 / sizeof(R));
 }
 
 // su: the block's state staged in shared memory (array k at k*stage_kstride,
 // element el's node n at el*ND + n), or nullptr to read it from a.u.
-template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND>
+template <typename R, int DIM, int N, int VOL, bool NS, bool BLEND, int EPBX = 0>
 __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block,
                                             const R *su = nullptr) {
-  using S = Shape<DIM, N>;
+  using S = Shape<DIM, N, EPBX>;
   static_assert(VOL != VOL_LTEEC || (!BLEND && !IsF32<R>::value), "LTEEC: FP64, no blending");
-  using L_ = VolSmem<R, DIM, N, VOL, NS, BLEND>;
+  using L_ = VolSmem<R, DIM, N, VOL, NS, BLEND, EPBX>;
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NPRIM = L_::PRIM, PAIRS = S::PAIRS;
   constexpr int MB = DIM * DIM;
   constexpr bool NEEDQ = L_::NEEDQ;
@@ -238,7 +240,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     R q[NEQ];
     if (su) {
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) q[k] = su[k * stage_kstride<R, DIM, N>() + el * ND + n];
+      for (int k = 0; k < NEQ; ++k) q[k] = su[k * stage_kstride<R, DIM, N, EPBX>() + el * ND + n];
     } else {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) q[k] = a.u[k * L + (long long)e * ND + n];
@@ -904,9 +906,9 @@ struct GradArgs {
   double *bgrad;  // [b][fp][dim][dim+2]
 };
 
-template <typename R, int DIM, int N>
+template <typename R, int DIM, int N, int EPBX = 0>
 __host__ __device__ constexpr size_t grad_smem_bytes() {
-  using S = Shape<DIM, N>;
+  using S = Shape<DIM, N, EPBX>;
   return sizeof(R) * (S::DPAD + (size_t)S::EPB * S::NEQ * (S::ND + 2 * DIM * S::NFP));
 }
 
@@ -933,16 +935,16 @@ __global__ void __launch_bounds__(256) entropy_kernel(const R *__restrict__ u, l
 // BR1 gradient (include/NSOperator_impl.hpp:11-159,194-517;
 // include/DGSEMIntegrator.hpp:764-850,1011-1044).  SV: the entropy variables
 // come from a.svars (entropy_kernel) instead of being evaluated here.
-template <typename R, int DIM, int N, bool LTE, bool SV = false>
+template <typename R, int DIM, int N, bool LTE, bool SV = false, int EPBX = 0>
 __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block) {
   static_assert(!LTE || !IsF32<R>::value, "LTE gas: FP64 only");
-  using S = Shape<DIM, N>;
+  using S = Shape<DIM, N, EPBX>;
   constexpr int ND = S::ND, NEQ = S::NEQ, EPB = S::EPB, NFP = S::NFP, NLF = 2 * DIM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *sD = reinterpret_cast<R *>(smem_raw);   // N*N (padded)
   R *sS = sD + S::DPAD;                      // [EPB][NEQ][ND] own entropy variables
   R *sN = sS + EPB * NEQ * ND;               // [EPB][2*DIM][NEQ][NFP] neighbour traces
-  if (dynamic_smem_bytes() < grad_smem_bytes<R, DIM, N>()) {
+  if (dynamic_smem_bytes() < grad_smem_bytes<R, DIM, N, EPBX>()) {
     if (threadIdx.x == 0 && a.status) atomicOr(a.status, STATUS_LAUNCH);
     return;
   }
@@ -1122,9 +1124,10 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
     for (int cc = 0; cc < DIM; ++cc) lte_grad_entropy_to_prim<DIM>(q, T, g[cc], dp + cc * NEQ);
     lte_viscous_flux<DIM>(a.gas, q, T, dp, vf);
   } else {
+    const NodeGas<R, DIM> ng = node_gas<R, DIM>(a.gas, q);
 #pragma unroll
-    for (int cc = 0; cc < DIM; ++cc) grad_entropy_to_prim<R, DIM>(a.gas, q, g[cc], dp + cc * NEQ);
-    viscous_flux<R, DIM>(a.gas, q, dp, vf);
+    for (int cc = 0; cc < DIM; ++cc) grad_entropy_to_prim_ng<R, DIM>(ng, q, g[cc], dp + cc * NEQ);
+    viscous_flux_ng<R, DIM>(a.gas, q, ng, dp, vf);
   }
   constexpr int NV = NEQ - 1;
 #pragma unroll
@@ -1333,11 +1336,12 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
   const R *q = sQ + el * NEQ * ND + n;  // q[k * ND]
   R qv[NEQ];
 #pragma unroll
-  for (int cc = 0; cc < DIM; ++cc) {
+  for (int k = 0; k < NEQ; ++k) qv[k] = q[k * ND];
+  const NodeGas<R, DIM> ng = node_gas<R, DIM>(a.gas, qv);
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) qv[k] = q[k * ND];
+  for (int cc = 0; cc < DIM; ++cc) {
     R dpc[NEQ];
-    grad_entropy_to_prim<R, DIM>(a.gas, qv, g[cc], dpc);
+    grad_entropy_to_prim_ng<R, DIM>(ng, qv, g[cc], dpc);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) g[cc][k] = dpc[k];
   }
@@ -1345,13 +1349,10 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
   constexpr int NV = NEQ - 1, E = DIM + 1;
   const long long base = (long long)e * ND + n;
   {
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) qv[k] = q[k * ND];
-    const R mu = viscosity<R, DIM>(a.gas, qv);
+    const R mu = viscosity_ng<R, DIM>(a.gas, ng);
     const R kappa = mu * a.gas.cp * a.gas.Pr_inv;
-    const R rho = qv[0];
-    const R p = pressure<R, DIM>(a.gas, qv);
-    const R pressor = fdiv(p, rho);
+    const R rho = ng.rho;
+    const R pressor = ng.p_rho;
     const R fac = fdiv(a.gas.gm1_inv, a.gas.cv * rho);
     R div = R(0);
 #pragma unroll
@@ -1365,7 +1366,7 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
         if (mom == dir) tau = mu * (R(2) * dp[dir * NEQ + 1 + mom] - a.gas.mu_bulk * div);
         else tau = mu * (dp[dir * NEQ + 1 + mom] + dp[mom * NEQ + 1 + dir]);
         a.vflux[((long long)dir * NV + mom) * L + base] = tau;
-        ef += fdiv(q[(1 + mom) * ND], rho) * tau;
+        ef += ng.v[mom] * tau;
       }
       a.vflux[((long long)dir * NV + DIM) * L + base] = ef;
     }
@@ -1810,27 +1811,27 @@ struct BatchWork {
   int block;
 };
 
-template <typename R, int DIM, int N, int VOL, bool NS>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+template <typename R, int DIM, int N, int VOL, bool NS, int EPBX = 0>
+__global__ void __launch_bounds__(Shape<DIM, N, EPBX>::THREADS)
 volume_batched(const VolArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
                const int *__restrict__ nwork) {
   const int n = *nwork;
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     __syncthreads();  // the previous item's shared memory is free
     const BatchWork it = work[w];
-    volume_body<R, DIM, N, VOL, NS, false>(args[it.item], it.block);
+    volume_body<R, DIM, N, VOL, NS, false, EPBX>(args[it.item], it.block);
   }
 }
 
-template <typename R, int DIM, int N>
-__global__ void __launch_bounds__(Shape<DIM, N>::THREADS)
+template <typename R, int DIM, int N, int EPBX = 0>
+__global__ void __launch_bounds__(Shape<DIM, N, EPBX>::THREADS)
 grad_batched(const GradArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
              const int *__restrict__ nwork) {
   const int n = *nwork;
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     __syncthreads();
     const BatchWork it = work[w];
-    grad_body<R, DIM, N, false>(args[it.item], it.block);
+    grad_body<R, DIM, N, false, false, EPBX>(args[it.item], it.block);
   }
 }
 

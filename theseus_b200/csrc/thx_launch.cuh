@@ -144,30 +144,37 @@ cudaError_t launch_lte_temperature(const double *u, long long L, const LteDev &t
   return cudaGetLastError();
 }
 
-template <typename R, int DIM, int N, int VOL, bool NS>
+template <typename R, int DIM, int N, int VOL, bool NS, int EPBX = 0>
 cudaError_t launch_volume_batched(const VolArgs<R> *args, const BatchWork *work, const int *nwork,
                                   int grid, cudaStream_t s, int prepare) {
-  using S = Shape<DIM, N>;
-  constexpr size_t smem = volume_smem_bytes<R, DIM, N, VOL, NS, false>(true);
+  using S = Shape<DIM, N, EPBX>;
+  constexpr size_t smem = VolSmem<R, DIM, N, VOL, NS, false, EPBX>::bytes(true);
   if (prepare)
-    return cudaFuncSetAttribute(volume_batched<R, DIM, N, VOL, NS>,
+    return cudaFuncSetAttribute(volume_batched<R, DIM, N, VOL, NS, EPBX>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (grid <= 0) return cudaSuccess;
-  volume_batched<R, DIM, N, VOL, NS><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
+  volume_batched<R, DIM, N, VOL, NS, EPBX><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
   return cudaGetLastError();
 }
 
-template <typename R, int DIM, int N>
+template <typename R, int DIM, int N, int EPBX = 0>
 cudaError_t launch_grad_batched(const GradArgs<R> *args, const BatchWork *work, const int *nwork,
                                 int grid, cudaStream_t s, int prepare) {
-  using S = Shape<DIM, N>;
-  constexpr size_t smem = grad_smem_bytes<R, DIM, N>();
+  using S = Shape<DIM, N, EPBX>;
+  constexpr size_t smem = grad_smem_bytes<R, DIM, N, EPBX>();
   if (prepare)
-    return cudaFuncSetAttribute(grad_batched<R, DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    return cudaFuncSetAttribute(grad_batched<R, DIM, N, EPBX>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (grid <= 0) return cudaSuccess;
-  grad_batched<R, DIM, N><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
+  grad_batched<R, DIM, N, EPBX><<<grid, S::THREADS, smem, s>>>(args, work, nwork);
   return cudaGetLastError();
+}
+
+// Elements per CTA of the batched kernels' half-size variant (0: none, the
+// full-size CTA already holds one element).
+template <int DIM, int N>
+constexpr int half_epb() {
+  return Shape<DIM, N>::EPB >= 2 ? Shape<DIM, N>::EPB / 2 : 0;
 }
 
 template <typename R, int DIM, int SURF, bool NS>
@@ -265,6 +272,10 @@ struct OrderKernelsT {
   VolLaunch<R> fv;               // subcell FV rate of blended elements
   VolBatchLaunch<R> volb[4][2];  // [volume flux][ns]
   GradBatchLaunch<R> gradb;
+  // half-size CTAs (epb_half elements each; 0 and null when EPB is 1)
+  int epb, epb_half;
+  VolBatchLaunch<R> volb_half[4][2];
+  GradBatchLaunch<R> gradb_half;
   // FP64 islands (Euler, blending; set in the FP64 units only)
   VolListLaunch<R> voll[4];      // [volume flux]
   VolListLaunch<R> fvl;
