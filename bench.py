@@ -570,7 +570,8 @@ def other_workloads(args):
     import torch
     out = {}
     for name, fn in (("vortex_2d", run_vortex), ("sedov", run_sedov), ("lte", run_lte),
-                     ("serving", run_serving), ("contraction_trial", run_trials)):
+                     ("serving", run_serving), ("batch", run_batch),
+                     ("contraction_trial", run_trials)):
         try:
             full = fn(args)
             out[name] = compact(name, full)
@@ -591,6 +592,7 @@ def compact(name, d):
         "serving": ["value", "unit", "latency_s", "makespan_s", "dof_rhs_per_s", "one_at_a_time_fp64",
                     "speedup_vs_one_at_a_time", "final_solution_rel_l2_vs_fp64"],
         "contraction_trial": ["results"],
+        "batch": ["value", "unit", "steps", "groups"],
     }[name]
     r = {k: d[k] for k in keep if k in d}
     if name == "sedov":
@@ -733,6 +735,77 @@ def run_trials(args):
                        "directions": 3, "padding": "rows of S^T to 8 (FP64) / 16 (TF32), K=5 to 8, "
                                                     "N columns: 5 of 8 used"},
             "results": out}
+
+
+def run_batch(args):
+    """Batched kernels against one-case kernels, FP32-mixed: for each group
+    kind (2-D vortex cases of p=2 Euler, p=3 Euler, p=3 Navier-Stokes, p=5
+    Navier-Stokes), 64 equal cases of 32^2 quads (24^2 at p=5) advanced
+    together through the batch engine, against one mesh of the same total
+    size (256^2, 192^2 at p=5) through the one-case fused SSP-RK3 loop.  The
+    engine's first batch tunes the group; the second is timed from its last
+    admission to its last completion (wall clock: the engine launches on its
+    own streams), the one-case loop by CUDA events.  Reports node-RHS/s of
+    both and their ratio, with the group's tuned configuration."""
+    import torch
+    import theseus_b200 as T
+    from theseus_b200 import cases
+    from theseus_b200.serving import BatchEngine, Case
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    flux = dict(numerical_flux="chandrashekar", surface_flux="roe")
+    steps, ncase = args.batch_steps, 64
+
+    def vcase(order, n, viscous, seed):
+        m = T.periodic_box(2, order, (n, n), [-5.0, -5.0], [5.0, 5.0])
+        c = np.sqrt(1.4)
+        v = 0.5 * c / np.sqrt(2.0)
+        u0 = cases.isentropic_vortex(m.coords, strength=3.0, u_inf=(v, v))
+        u0 = u0 * (1.0 + 1e-3 * np.random.default_rng(seed).uniform(-1, 1, u0.shape))
+        dt = 0.4 * (10.0 / n) / ((2 * order + 1) * (np.sqrt(2) * v + c + 1.0))
+        return Case(mesh=m, u0=u0, nsteps=steps, dt=dt, viscous=viscous, mu=0.01 if viscous else 0.0,
+                    Pr=0.72, state_offset=(1.0, v, v, 1.0 / 0.4 + v * v, 0.0))
+
+    groups = []
+    for order, n, viscous in ((2, 32, False), (3, 32, False), (3, 32, True), (5, 24, True)):
+        batch = [vcase(order, n, viscous, s) for s in range(ncase)]
+        eng = BatchEngine(precision="fp32", steps_per_launch=10, **flux)
+        for rep in range(2):
+            ids = [eng.admit(c) for c in batch]
+            assert None not in ids
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            left = set(ids)
+            while left:
+                eng.advance()
+                for cid in eng.poll():
+                    left.discard(cid)
+            wall = time.perf_counter() - t0
+            for cid in ids:
+                eng.fetch(cid, batch[0].u0.shape)
+        tuned = eng.groups()
+        eng.close()
+        nodes = sum(c.mesh.num_nodes for c in batch)
+        big = vcase(order, int(round(n * np.sqrt(ncase))), viscous, 0)
+        op = (T.NSOperator if viscous else T.EulerOperator)(
+            big.mesh, precision="fp32", mu=big.mu, Pr=big.Pr, state_offset=list(big.state_offset), **flux)
+        u = torch.as_tensor(big.u0, device="cuda").contiguous()
+        op.rk3_steps(u, big.dt, 5)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        op.rk3_steps(u, big.dt, steps)
+        b.record()
+        torch.cuda.synchronize()
+        one = 3 * steps * big.mesh.num_nodes / (a.elapsed_time(b) * 1e-3)
+        del op, u
+        batched = 3 * steps * nodes / wall
+        groups.append({"order": order, "mesh": [n, n], "navier_stokes": viscous, "cases": ncase,
+                       "batched_dof_rhs_per_s": batched, "one_case_dof_rhs_per_s": one,
+                       "one_case_mesh": [int(round(n * np.sqrt(ncase)))] * 2,
+                       "ratio": batched / one, "tuned": tuned[0] if tuned else None})
+    return {"metric": "batched / one-case DOF*RHS/s (FP32-mixed, equal 2-D cases)",
+            "value": float(np.mean([g["ratio"] for g in groups])), "unit": "ratio",
+            "steps": steps, "groups": groups}
 
 
 def run_serving(args):
@@ -1057,12 +1130,13 @@ def main():
     ap.add_argument("--n", type=int, default=32, help="elements per direction (profiling cases)")
     ap.add_argument("--rk-steps", type=int, default=200, help="SSP-RK3 steps of the precision comparison")
     ap.add_argument("--workload", default="rhs",
-                    choices=["rhs", "serving", "lte", "sedov", "setup", "vortex", "trials"],
+                    choices=["rhs", "serving", "lte", "sedov", "setup", "vortex", "trials", "batch"],
                     help="rhs: the headline RHS throughput (with compact results of vortex, "
                          "sedov, lte and serving unless --no-workloads); serving: the batched "
                          "case stream; lte: the LTE-gas Taylor-Green vortex; sedov: the blended "
                          "blast; setup: mesh set-up on the device; vortex: the 2-D isentropic vortex; "
-                         "trials: the tensor-core trial of the gradient's derivative contraction")
+                         "trials: the tensor-core trial of the gradient's derivative contraction; "
+                         "batch: batched against one-case kernels on equal 2-D cases")
     ap.add_argument("--volume-staging", type=int, default=0, choices=[0, 1],
                     help="rhs: 1 stages each element block's state by bulk copy (TMA) in the "
                          "volume kernel")
@@ -1075,6 +1149,7 @@ def main():
     ap.add_argument("--cases", type=int, default=4096, help="serving: cases in the stream")
     ap.add_argument("--sample", type=int, default=256, help="serving: cases also run one at a time")
     ap.add_argument("--chunk", type=int, default=10, help="serving: SSP-RK3 steps per graph launch")
+    ap.add_argument("--batch-steps", type=int, default=1000, help="batch: SSP-RK3 steps per case")
     ap.add_argument("--admitters", type=int, default=1,
                     help="serving: host threads setting up arriving cases (1: strict arrival order)")
     args = ap.parse_args()
@@ -1084,7 +1159,7 @@ def main():
         run_ours(args)
     else:
         fn = {"serving": run_serving, "lte": run_lte, "sedov": run_sedov, "setup": run_setup,
-              "vortex": run_vortex, "trials": run_trials}[args.workload]
+              "vortex": run_vortex, "trials": run_trials, "batch": run_batch}[args.workload]
         print(json.dumps(fn(args)), flush=True)
 
 

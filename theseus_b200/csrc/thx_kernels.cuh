@@ -1811,15 +1811,38 @@ struct BatchWork {
   int block;
 };
 
+// A work item's argument record copied into shared memory by the whole CTA
+// (one coalesced read): the body then reads its fields at shared-memory
+// latency, as a one-case kernel reads its parameters from the constant bank,
+// instead of one dependent global load per field.
+template <typename A>
+__device__ __forceinline__ void stage_record(unsigned char *dst, const A *src) {
+  static_assert(sizeof(A) % 8 == 0 && alignof(A) >= 8, "8-byte words");
+  const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(A) / 8); i += blockDim.x) d[i] = s[i];
+}
+
+// The batched volume kernel is compiled for four resident 256-thread CTAs per
+// SM (eight of the half-size CTAs): 64 registers a thread.  Bounded to the
+// FP32 one-case kernel's six CTAs (40 registers) its persistent loop spills
+// about 100 bytes per thread and runs 4-8 % slower (2-D).
+template <typename R, int DIM, int N, int EPBX>
+constexpr int vol_batch_min_blocks() {
+  return 4 * Shape<DIM, N>::THREADS / Shape<DIM, N, EPBX>::THREADS;
+}
 template <typename R, int DIM, int N, int VOL, bool NS, int EPBX = 0>
-__global__ void __launch_bounds__(Shape<DIM, N, EPBX>::THREADS)
+__global__ void __launch_bounds__(Shape<DIM, N, EPBX>::THREADS, (vol_batch_min_blocks<R, DIM, N, EPBX>()))
 volume_batched(const VolArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
                const int *__restrict__ nwork) {
+  __shared__ __align__(16) unsigned char sa[sizeof(VolArgs<R>)];
   const int n = *nwork;
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     __syncthreads();  // the previous item's shared memory is free
     const BatchWork it = work[w];
-    volume_body<R, DIM, N, VOL, NS, false, EPBX>(args[it.item], it.block);
+    stage_record(sa, &args[it.item]);
+    __syncthreads();
+    volume_body<R, DIM, N, VOL, NS, false, EPBX>(*reinterpret_cast<const VolArgs<R> *>(sa), it.block);
   }
 }
 
@@ -1827,23 +1850,32 @@ template <typename R, int DIM, int N, int EPBX = 0>
 __global__ void __launch_bounds__(Shape<DIM, N, EPBX>::THREADS)
 grad_batched(const GradArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
              const int *__restrict__ nwork) {
+  __shared__ __align__(16) unsigned char sa[sizeof(GradArgs<R>)];
   const int n = *nwork;
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
     __syncthreads();
     const BatchWork it = work[w];
-    grad_body<R, DIM, N, false, false, EPBX>(args[it.item], it.block);
+    stage_record(sa, &args[it.item]);
+    __syncthreads();
+    grad_body<R, DIM, N, false, false, EPBX>(*reinterpret_cast<const GradArgs<R> *>(sa), it.block);
   }
 }
 
-// face work blocks are 128 face points
+// face work blocks are 128 face points; compiled for eight resident CTAs per
+// SM in FP32 (the register budget of the one-case FP32 face kernel)
 template <typename R, int DIM, int SURF, bool NS>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, IsF32<R>::value ? 8 : 5)
 face_batched(const FaceArgs<R> *__restrict__ args, const BatchWork *__restrict__ work,
              const int *__restrict__ nwork) {
+  __shared__ __align__(16) unsigned char sa[sizeof(FaceArgs<R>)];
   const int n = *nwork;
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    __syncthreads();
     const BatchWork it = work[w];
-    face_body<R, DIM, SURF, NS>(args[it.item], (long long)it.block * 128 + threadIdx.x);
+    stage_record(sa, &args[it.item]);
+    __syncthreads();
+    face_body<R, DIM, SURF, NS>(*reinterpret_cast<const FaceArgs<R> *>(sa),
+                                (long long)it.block * 128 + threadIdx.x);
   }
 }
 
