@@ -150,6 +150,13 @@ int to_device(void *dst, const void *src, size_t bytes) {
 }
 
 int dev_zero(void *dst, size_t bytes) {
+  if (pool_mode() && t_alloc_owner->ring) {
+    // through the upload ring: the set-up stream then holds copies only,
+    // which the copy engines run while persistent kernels fill every SM
+    thread_local std::vector<unsigned char> zeros;
+    if (zeros.size() < bytes) zeros.assign(bytes, 0);
+    return t_alloc_owner->ring->copy(dst, zeros.data(), bytes, t_alloc_owner->setup_stream);
+  }
   const cudaError_t e = pool_mode() ? cudaMemsetAsync(dst, 0, bytes, t_alloc_owner->setup_stream)
                                     : cudaMemset(dst, 0, bytes);
   return e == cudaSuccess ? THX_OK : THX_ERR_CUDA;

@@ -172,7 +172,7 @@ class Engine final : public EngineBase {
     int least = 0, greatest = 0;
     THX_CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     THX_CU(cudaStreamCreateWithPriority(&setup_, cudaStreamNonBlocking, greatest));
-    if (ring_.init(size_t(64) << 20) != THX_OK) return THX_ERR_OUT_OF_MEMORY;
+    if (ring_.init(size_t(256) << 20) != THX_OK) return THX_ERR_OUT_OF_MEMORY;
     return THX_OK;
   }
 
@@ -298,7 +298,7 @@ class Engine final : public EngineBase {
     }
     const double t2 = now();
     if (ring_.copy(ec->u, u0, n * sizeof(double), setup_) != THX_OK ||
-        (h->mixed && op_to_working_copy(h, ec->u, setup_) != THX_OK) ||
+        (h->mixed && upload_working_copy(h, u0) != THX_OK) ||
         cudaEventCreateWithFlags(&ec->done, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ec->ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventRecord(ec->ready, setup_) != cudaSuccess) {
@@ -323,6 +323,39 @@ class Engine final : public EngineBase {
     *id = ec->id;
     cases_[ec->id] = std::move(ec);
     return THX_OK;
+  }
+
+  // The FP32 working copy of an admitted case's initial state, narrowed on
+  // the host exactly as the to_working kernel narrows it, (float)(u - offset),
+  // with its FP64 positivity check, and uploaded through the ring: the
+  // set-up stream holds no kernel, whose CTAs would wait for the persistent
+  // kernels of the running groups to leave an SM.
+  int upload_working_copy(thx_operator_s *h, const double *u0) {
+    const long long L = h->L;
+    const int neq = h->neq, dim = h->dim;
+    thread_local std::vector<float> wf;
+    wf.resize((size_t)L * neq);
+    for (int k = 0; k < neq; ++k) {
+      const double o = h->off.v[k];
+      const double *src = u0 + (size_t)k * L;
+      float *dst = wf.data() + (size_t)k * L;
+      for (long long i = 0; i < L; ++i) dst[i] = (float)(src[i] - o);
+    }
+    bool bad = false;
+    const double gm1 = h->g64.gm1;
+    for (long long i = 0; i < L && !bad; ++i) {
+      double m2 = 0.0;
+      for (int d = 0; d < dim; ++d) m2 += u0[(size_t)(1 + d) * L + i] * u0[(size_t)(1 + d) * L + i];
+      const double rho = u0[i];
+      const double p = gm1 * (u0[(size_t)(dim + 1) * L + i] - 0.5 * m2 / rho);
+      bad = !(rho > 0.0 && p > 0.0);
+    }
+    int st = ring_.copy(h->yf, wf.data(), wf.size() * sizeof(float), setup_);
+    if (!st && bad) {
+      static const unsigned flag = STATUS_NONPOSITIVE;
+      st = ring_.copy(h->status, &flag, sizeof(flag), setup_);
+    }
+    return st;
   }
 
   int advance() override {
