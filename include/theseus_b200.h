@@ -559,8 +559,9 @@ int thx_engine_get_stats(thx_engine e, thx_engine_stats *out);
  * CTA of the volume and gradient kernels (as many as fit 256 threads, or
  * half as many), then the volume grid over {1,2,4} x SMs, the face grid over
  * {4,8,16} x SMs and (Navier-Stokes) the gradient grid over {1,2,4} x SMs,
- * each candidate timed with CUDA events around one launch that advances real
- * cases; cost = device milliseconds per (solution node x step). */
+ * each candidate timed with CUDA events around two launches that advance real
+ * cases (the better one counts); cost = device milliseconds per (solution
+ * node x step). */
 typedef struct {
   int32_t dim, order, navier_stokes;
   int32_t active_cases;

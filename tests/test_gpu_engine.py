@@ -153,7 +153,7 @@ def test_engine_grid_tuning(cuda):
         assert g["elements_per_block"] in (full, full // 2)
     assert ns[1]["gradient_grid"] in (sms, 2 * sms, 4 * sms) and ns[0]["gradient_grid"] == 0
     final = eng.groups()
-    # 100 launches per group are far more than the 11 timed ones the search needs
+    # 100 launches per group are far more than the 22 timed ones the search needs
     assert all(g["tuned"] == 1 and g["active_cases"] == 0 and g["best_cost_ms"] > 0 for g in final), final
     for c, g in zip(batch, out):
         assert np.array_equal(g, alone(c, "fp64"))

@@ -141,6 +141,7 @@ struct Group {
   Grids best;
   double best_cost = -1.0;
   int tune_axis = 0, tune_index = 0;  // 0 CTA size, 1 volume, 2 face, 3 gradient; 4: done
+  int tune_rep = 0;                   // timings taken of the current candidate
   bool tuned = false;
   Grids timing_grids;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -567,7 +568,7 @@ class Engine final : public EngineBase {
       cudaGetLastError();
       return THX_ERR_CUDA;
     }
-    G->best.vol = 1 * sms_;
+    G->best.vol = 4 * sms_;
     G->best.face = 8 * sms_;
     G->best.grad = 2 * sms_;
     G->tune_axis = next_axis(*G, 0);
@@ -785,6 +786,9 @@ class Engine final : public EngineBase {
         G.best = G.timing_grids;
       }
     }
+    // every candidate is timed on two launches; the better one counts
+    if (++G.tune_rep < 2) return;
+    G.tune_rep = 0;
     if (++G.tune_index >= axis_size(G, G.tune_axis)) {
       G.tune_index = 0;
       G.tune_axis = next_axis(G, G.tune_axis + 1);
