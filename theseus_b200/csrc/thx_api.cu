@@ -760,7 +760,7 @@ namespace {
 template <typename R>
 int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, double dt,
             double *um, double *y, float *yf, cudaEvent_t *ev = nullptr, double *du64 = nullptr,
-            const double *dt_dev = nullptr, const double *u64 = nullptr) {
+            const double *dt_dev = nullptr, const double *u64 = nullptr, bool narrow_in_grad = false) {
   R *tag = nullptr;
   if (ev) cudaEventRecord(ev[0], s);
   GradArgs<R> ga;
@@ -769,6 +769,14 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   op_args<R>(h, u, du, stage, dt, um, y, yf, ga, fa, va);
   va.du64 = du64;
   va.dt_dev = dt_dev;
+  if constexpr (IsF32<R>::value) {
+    if (narrow_in_grad) {
+      // the gradient kernel narrows the FP64 state into the working copy
+      ga.u64 = u64;
+      ga.yf = h->yf;
+      for (int k = 0; k < 5; ++k) ga.off[k] = h->off.v[k];
+    }
+  }
   if constexpr (!IsF32<R>::value) {
     if (h->lte) {
       cudaError_t te = h->dim == 2
@@ -884,10 +892,17 @@ int to_working_copy(thx_operator_s *h, const double *u, cudaStream_t s) {
 }
 
 int rhs_mixed(thx_operator_s *h, const double *u, double *dudt, cudaStream_t s, cudaEvent_t *ev) {
-  // the volume kernel writes the FP32 rate widened to FP64 directly
+  // the volume kernel writes the FP32 rate widened to FP64 directly.  Navier-
+  // Stokes without blending: the gradient kernel, the first to read the state,
+  // narrows it into the working copy (one pass over the FP64 state fewer);
+  // otherwise the indicator or the face kernel reads the copy first and a
+  // separate narrowing pass runs ahead.
+  const bool in_grad = h->ns && !h->blend && !h->lte && !h->islands;
   int st;
-  if ((st = to_working_copy(h, u, s))) return st;
-  return run_rhs<float>(h, h->yf, nullptr, s, 0, 0.0, nullptr, nullptr, nullptr, ev, dudt, nullptr, u);
+  if (!h->yf && (st = dev_alloc(&h->yf, (size_t)(h->L * h->neq), h->allocs))) return st;
+  if (!in_grad && (st = to_working_copy(h, u, s))) return st;
+  return run_rhs<float>(h, h->yf, nullptr, s, 0, 0.0, nullptr, nullptr, nullptr, ev, dudt, nullptr, u,
+                        in_grad);
 }
 
 }  // namespace

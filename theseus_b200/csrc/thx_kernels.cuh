@@ -904,6 +904,15 @@ struct GradArgs {
   const thx_bc *bcs;
   const double *bc_data;
   double *bgrad;  // [b][fp][dim][dim+2]
+  // FP32-mixed right-hand side of an FP64 state (u64 set): the kernel reads
+  // the FP64 state, narrows it as the to_working kernel does,
+  // (float)(u64 - off), writes its own nodes' working copy to yf for the
+  // face and volume kernels that follow, and checks their FP64 positivity;
+  // u is not read.  Neighbour traces are narrowed from u64 as well, so no
+  // CTA reads a working copy another CTA is writing.
+  const double *u64;
+  float *yf;
+  double off[5];
 };
 
 template <typename R, int DIM, int N, int EPBX = 0>
@@ -958,8 +967,20 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
   R q[NEQ];
   if (active) {
     R raw[NEQ];
+    if (IsF32<R>::value && a.u64) {
+      double d[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
+      for (int k = 0; k < NEQ; ++k) d[k] = a.u64[k * L + (long long)e * ND + n];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        raw[k] = (R)(d[k] - a.off[k]);
+        a.yf[k * L + (long long)e * ND + n] = (float)raw[k];
+      }
+      if (!fp64_state_positive<DIM>(d, (double)a.gas.gm1)) atomicOr(a.status, STATUS_NONPOSITIVE);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) raw[k] = a.u[k * L + (long long)e * ND + n];
+    }
     reconstruct<R, DIM>(a.gas, raw, q);
     R w[NEQ];
     if constexpr (SV) {
@@ -991,8 +1012,13 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
       for (int k = 0; k < NEQ; ++k) so[k] = a.svars[k * L + (long long)eo * ND + no];
     } else {
       R ro[NEQ], qo[NEQ];
+      if (IsF32<R>::value && a.u64) {
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
+        for (int k = 0; k < NEQ; ++k) ro[k] = (R)(a.u64[k * L + (long long)eo * ND + no] - a.off[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
+      }
       reconstruct<R, DIM>(a.gas, ro, qo);
       if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], so);
       else entropy_vars<R, DIM>(a.gas, qo, so);
