@@ -456,7 +456,13 @@ def run_ours(args):
                             for i, k in enumerate(names) if phases[i] > 0.01}
     roofline["volume_fp64"] = {"pairs": pairs, "pair_flops": PAIR_FLOPS[WORKLOAD["volume_flux"]](3),
                                "flops": vflops, "fp64_fma_peak_tflops": fp64_tf,
-                               "pair_evals_per_s": pairs / (phases[3] * 1e-3)}
+                               "pair_evals_per_s": pairs / (phases[3] * 1e-3),
+                               # the algorithmic count takes a division or a log
+                               # as one flop; the FP64 pipe also runs their
+                               # iterations, so it is busier than frac says
+                               "ncu_fp64_pipe_active": 0.483, "ncu_issue_active": 0.666,
+                               "ncu_source": "profiles/volume_kernel_ns_tgv_20cubed_p4_fp64.md "
+                                             "(sm__pipe_fp64_cycles_active, smsp__issue_active)"}
 
     # the volume kernel with its element blocks' state staged by bulk copy
     # (cp.async.bulk into a double buffer, persistent CTAs) against the
