@@ -143,6 +143,22 @@ THX_HD LteEval lte_at(const LteDev &t, double rho, double T) {
   return r;
 }
 
+// lte_at(t, a.rho, b.T) for two points that lte_at has already located: the
+// density cell and position are a's, the temperature cell and position b's
+// (the same searches on the same values give the same cells), so the cross
+// state of a discrete gradient needs no table search.
+THX_HD LteEval lte_cross(const LteEval &a, const LteEval &b) {
+  LteEval r;
+  const int nx = a.cell.nx;
+  r.cell = {(b.cell.off / nx) * nx + a.cell.off % nx, nx, a.cell.dr, b.cell.dt};
+  r.xi = a.xi;
+  r.eta = b.eta;
+  r.rho = a.rho;
+  r.T = b.T;
+  r.valid = a.valid && b.valid;
+  return r;
+}
+
 THX_HD double lte_pressure(const LteDev &t, const LteEval &s) {
   return s.rho * s.rho * lte_eval<1, 0>(t, s.cell, s.xi, s.eta);
 }
@@ -276,8 +292,8 @@ THX_HDC void lte_discrete_gradient(const LteDev &t, const LteEval &left, const L
     if (ddiff) gr = 0.5 * (lte_density_secant<P>(t, A, B, A.eta) * b1 + lte_density_secant<P>(t, A, B, B.eta) * b2);
     if (bdiff) gb = 0.5 * (lte_beta_secant<P>(t, A, B, A.xi, A.rho) + lte_beta_secant<P>(t, A, B, B.xi, B.rho));
   } else if (ddiff || bdiff) {
-    const double f12 = lte_value<P>(t, lte_at(t, A.rho, B.T));
-    const double f21 = lte_value<P>(t, lte_at(t, B.rho, A.T));
+    const double f12 = lte_value<P>(t, lte_cross(A, B));
+    const double f21 = lte_value<P>(t, lte_cross(B, A));
     if (ddiff) gr = 0.5 * ((f21 * b1 - f11 * b1) + (f22 * b2 - f12 * b2)) / dr;
     if (bdiff) gb = 0.5 * ((f12 * b2 - f11 * b1) + (f22 * b2 - f21 * b1)) / db;
   }
@@ -433,7 +449,7 @@ THX_HDC void lte_discrete_gradients(const LteDev &t, const LteEval &left, const 
       gb = 0.5 * (gs[0] + gs[1]);
     }
   } else if (ddiff || bdiff) {
-    const LteEval s12 = lte_at(t, A.rho, B.T), s21 = lte_at(t, B.rho, A.T);
+    const LteEval s12 = lte_cross(A, B), s21 = lte_cross(B, A);
     const LteCorners k12 = lte_corners(t, s12.cell), k21 = lte_corners(t, s21.cell);
     const double hr12 = lte_eval_k<1, 0>(k12, s12.xi, s12.eta);
     const double hr21 = lte_eval_k<1, 0>(k21, s21.xi, s21.eta);
