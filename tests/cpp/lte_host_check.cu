@@ -55,7 +55,9 @@ int main() {
       bool b = false;
       orc::lte::lteec(o, 3, face, q1, q2, d1, face ? d1 : d2, Fo, &b);
       if (face) {
-        thx::lte_ec_flux<3, true>(t, q1, q2, s1, s2, j1, j2, d1, d1, Fp);
+        // the face kernel's jets carry the traces' squared sound speeds
+        thx::lte_ec_flux<3, true>(t, q1, q2, s1, s2, thx::lte_face_jet(t, s1), thx::lte_face_jet(t, s2),
+                                  d1, d1, Fp);
       } else {
         // the volume kernel passes the averaged metric as both rows
         for (int i = 0; i < 3; ++i) m[i] = 0.5 * (d1[i] + d2[i]);

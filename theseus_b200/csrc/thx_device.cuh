@@ -953,6 +953,7 @@ __device__ __forceinline__ LteJet lte_unpack_jet(const double *x /* LTE_P_* bloc
   j.HT = x[LTE_P_HT];
   j.Hrr = x[LTE_P_HRR];
   j.HrT = x[LTE_P_HRT];
+  j.c2 = 0.0;  // volume fluxes do not use it
   return j;
 }
 

@@ -846,8 +846,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long 
     static_assert(!IsF32<R>::value, "LTEEC: FP64 only");
     const LteEval sm = lte_at(a.gas.lte, qm[0], a.gas.Tn[im]);
     const LteEval sp = lte_at(a.gas.lte, qp[0], a.gas.Tn[ip]);
-    lte_ec_flux<DIM, true>(a.gas.lte, qm, qp, sm, sp, lte_jet(a.gas.lte, sm), lte_jet(a.gas.lte, sp),
-                           nrm, nrm, F);
+    lte_ec_flux<DIM, true>(a.gas.lte, qm, qp, sm, sp, lte_face_jet(a.gas.lte, sm),
+                           lte_face_jet(a.gas.lte, sp), nrm, nrm, F);
   } else {
     FState<R, DIM> A, B;
     make_fstate<R, DIM>(a.gas, qm, A);
@@ -1431,7 +1431,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 3) grad_sv_kernel(cons
 // (include/LTEHelmholtzGasEOS.hpp:59-76 evaluates it on every gas query; the
 // face, gradient and volume kernels read the stored T instead).
 template <int DIM>
-__global__ void __launch_bounds__(256) lte_temperature_kernel(const double *u, long long L, LteDev t,
+__global__ void __launch_bounds__(256, 2) lte_temperature_kernel(const double *u, long long L, LteDev t,
                                                               double *Tn, unsigned *status) {
   constexpr int NEQ = DIM + 2;
   const long long stride = (long long)gridDim.x * blockDim.x;

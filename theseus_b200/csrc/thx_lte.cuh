@@ -40,6 +40,17 @@ THX_HD int lte_find_cell(const double *grid, int count, double v) {
   return lo;
 }
 
+// lte_find_cell(grid, count, v) found by walking from the cell `from`
+// (0 <= from <= count - 2): the same cell, in a step or two when v moved
+// little since `from` was found.
+THX_HD int lte_walk_cell(const double *grid, int count, double v, int from) {
+  if (count < 2 || !isfinite(v) || v < grid[0] || v > grid[count - 1]) return -1;
+  int lo = from;
+  while (lo > 0 && v < grid[lo]) --lo;
+  while (lo < count - 2 && v >= grid[lo + 1]) ++lo;
+  return lo;
+}
+
 template <int D> THX_HD double hpos(int side, double x) {
   const double x2 = x * x;
   if (D == 0) { const double x3 = x2 * x; return side == 0 ? 2 * x3 - 3 * x2 + 1 : -2 * x3 + 3 * x2; }
@@ -195,6 +206,50 @@ THX_HD double lte_transport(const LteDev &t, const LteEval &s, int prop) {
          p[t.nx + 1] * s.xi * s.eta;
 }
 
+// One cell's sixteen corner values (H, H_rho, H_T, H_rhoT at its four
+// corners), read once and evaluated at several points or orders:
+// lte_eval_k does lte_eval's operations in lte_eval's order.
+struct LteCorners {
+  double H[4], Hr[4], HT[4], HrT[4];  // corner j = rho side + 2 * T side
+  double dr, dt;
+};
+
+THX_HD LteCorners lte_corners(const LteDev &t, const LteCell &c) {
+  const long ps = (long)t.nx * t.ny;
+  const double *H = t.planes + c.off;
+  LteCorners k;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int o = (j & 1) + (j >> 1) * c.nx;
+    k.H[j] = H[o];
+    k.Hr[j] = H[ps + o];
+    k.HT[j] = H[2 * ps + o];
+    k.HrT[j] = H[3 * ps + o];
+  }
+  k.dr = c.dr;
+  k.dt = c.dt;
+  return k;
+}
+
+template <int DR, int DT>
+THX_HD double lte_eval_k(const LteCorners &k, double xi, double eta) {
+  double r = 0.0;
+#pragma unroll
+  for (int ds = 0; ds < 2; ++ds) {
+    const double dv = hpos<DR>(ds, xi), dsl = hslope<DR>(ds, xi);
+#pragma unroll
+    for (int ts = 0; ts < 2; ++ts) {
+      const int o = ds + 2 * ts;
+      const double tv = hpos<DT>(ts, eta), tsl = hslope<DT>(ts, eta);
+      r += k.H[o] * dv * tv;
+      r += (k.Hr[o] * k.dr) * dsl * tv;
+      r += (k.HT[o] * k.dt) * dv * tsl;
+      r += (k.HrT[o] * k.dr * k.dt) * dsl * tsl;
+    }
+  }
+  return r / (hscale<DR>(k.dr) * hscale<DT>(k.dt));
+}
+
 enum LteStatus { LTE_CONVERGED = 0, LTE_OUTSIDE = 1, LTE_INVALID = 2, LTE_ITERATIONS = 3 };
 
 // Inverse-table guess, then Newton on e(rho, T) with the analytic cv.
@@ -208,10 +263,24 @@ THX_HDC double lte_temperature(const LteDev &t, double rho, double e, int *statu
   const double lower = p[0] + x * (p[1] - p[0]);
   const double upper = p[t.nx] + x * (p[t.nx + 1] - p[t.nx]);
   double T = lower + y * (upper - lower);
+  // lte_at(t, rho, T) every iteration, with the density cell (the search
+  // above) and its position held, the temperature cell found by walking from
+  // the previous iteration's, and the cell's corners read when it changes;
+  // lte_cv and lte_energy are then lte_eval_k of those corners
+  const double dr = t.rho[i + 1] - t.rho[i];
+  const double xi = (rho - t.rho[i]) / dr;
+  int jt = -1;
+  LteCorners k;
   for (int it = 0; it < 100; ++it) {
-    const LteEval s = lte_at(t, rho, T);
-    if (!s.valid) return T;
-    const double cv = lte_cv(t, s), guess = lte_energy(t, s);
+    const int jn = jt < 0 ? lte_find_cell(t.T, t.ny, T) : lte_walk_cell(t.T, t.ny, T, jt);
+    if (jn < 0) return T;
+    if (jn != jt) {
+      jt = jn;
+      k = lte_corners(t, LteCell{jt * t.nx + i, t.nx, dr, t.T[jt + 1] - t.T[jt]});
+    }
+    const double eta = (T - t.T[jt]) / k.dt;
+    const double cv = -T * lte_eval_k<0, 2>(k, xi, eta);
+    const double guess = lte_eval_k<0, 0>(k, xi, eta) - T * lte_eval_k<0, 1>(k, xi, eta);
     if (!isfinite(cv) || cv <= 0 || !isfinite(guess)) { *status = LTE_INVALID; return T; }
     const double step = (e - guess) / cv;
     const double next = T + step;
@@ -315,47 +384,6 @@ THX_HDC void lte_discrete_gradient(const LteDev &t, const LteEval &left, const L
 // jet once and, when both endpoints share a table cell, reads that cell's
 // sixteen corner values once.  Every output is computed with the operations,
 // in the order, of lte_discrete_gradient<P>.
-struct LteCorners {
-  double H[4], Hr[4], HT[4], HrT[4];  // corner j = rho side + 2 * T side
-  double dr, dt;
-};
-
-THX_HD LteCorners lte_corners(const LteDev &t, const LteCell &c) {
-  const long ps = (long)t.nx * t.ny;
-  const double *H = t.planes + c.off;
-  LteCorners k;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int o = (j & 1) + (j >> 1) * c.nx;
-    k.H[j] = H[o];
-    k.Hr[j] = H[ps + o];
-    k.HT[j] = H[2 * ps + o];
-    k.HrT[j] = H[3 * ps + o];
-  }
-  k.dr = c.dr;
-  k.dt = c.dt;
-  return k;
-}
-
-template <int DR, int DT>
-THX_HD double lte_eval_k(const LteCorners &k, double xi, double eta) {
-  double r = 0.0;
-#pragma unroll
-  for (int ds = 0; ds < 2; ++ds) {
-    const double dv = hpos<DR>(ds, xi), dsl = hslope<DR>(ds, xi);
-#pragma unroll
-    for (int ts = 0; ts < 2; ++ts) {
-      const int o = ds + 2 * ts;
-      const double tv = hpos<DT>(ts, eta), tsl = hslope<DT>(ts, eta);
-      r += k.H[o] * dv * tv;
-      r += (k.Hr[o] * k.dr) * dsl * tv;
-      r += (k.HT[o] * k.dt) * dv * tsl;
-      r += (k.HrT[o] * k.dr * k.dt) * dsl * tsl;
-    }
-  }
-  return r / (hscale<DR>(k.dr) * hscale<DT>(k.dt));
-}
-
 template <int AXIS, int DR, int DT>
 THX_HD double lte_divided_k(const LteCorners &k, double xi1, double eta1, double xi2, double eta2) {
   double r = 0.0;
@@ -381,6 +409,7 @@ THX_HD double lte_divided_k(const LteCorners &k, double xi1, double eta1, double
 // Jets of one endpoint at its own point: H, H_rho, H_T, H_rhorho, H_rhoT.
 struct LteJet {
   double H, Hr, HT, Hrr, HrT;
+  double c2;  // squared sound speed (lte_face_jet only)
 };
 
 THX_HD LteJet lte_jet(const LteDev &t, const LteEval &s) {
@@ -391,6 +420,22 @@ THX_HD LteJet lte_jet(const LteDev &t, const LteEval &s) {
   j.HT = lte_eval_k<0, 1>(k, s.xi, s.eta);
   j.Hrr = lte_eval_k<2, 0>(k, s.xi, s.eta);
   j.HrT = lte_eval_k<1, 1>(k, s.xi, s.eta);
+  j.c2 = 0.0;
+  return j;
+}
+
+// lte_jet and lte_c2 of a face trace from one read of its cell's corners
+// (lte_c2 alone reads them four times), with lte_c2's operations.
+THX_HD LteJet lte_face_jet(const LteDev &t, const LteEval &s) {
+  const LteCorners k = lte_corners(t, s.cell);
+  LteJet j;
+  j.H = lte_eval_k<0, 0>(k, s.xi, s.eta);
+  j.Hr = lte_eval_k<1, 0>(k, s.xi, s.eta);
+  j.HT = lte_eval_k<0, 1>(k, s.xi, s.eta);
+  j.Hrr = lte_eval_k<2, 0>(k, s.xi, s.eta);
+  j.HrT = lte_eval_k<1, 1>(k, s.xi, s.eta);
+  const double m = j.HrT;
+  j.c2 = 2 * s.rho * j.Hr + s.rho * s.rho * j.Hrr - s.rho * s.rho * m * m / lte_eval_k<0, 2>(k, s.xi, s.eta);
   return j;
 }
 
@@ -499,7 +544,7 @@ THX_HD void lte_ec_flux(const LteDev &t, const double *q1, const double *q2, con
   const double rho_mean = pr / gr;
   const double e_mean = gb - pb / rho_mean;
   double c1 = 0, c2 = 0;
-  if (FACE) { c1 = sqrt(lte_c2(t, s1)); c2 = sqrt(lte_c2(t, s2)); }
+  if (FACE) { c1 = sqrt(j1.c2); c2 = sqrt(j2.c2); }  // j1, j2 from lte_face_jet
   const double pm = 0.5 * (p1 + p2);
   double vn = 0, ck = 0, pw = 0, v1n = 0, v2n = 0, nn = 0;
 #pragma unroll
