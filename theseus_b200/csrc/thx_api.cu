@@ -427,6 +427,8 @@ int create_impl(const thx_geometry *g, const thx_config *cfg, thx_operator_s *h,
     h->g64.lte.inv = inv;
     if ((st = dev_alloc(&h->Tn, (size_t)h->L, A))) return st;
     h->g64.Tn = h->Tn;
+    if ((st = dev_alloc(&h->Cn, (size_t)h->L, A))) return st;
+    h->g64.Cn = h->Cn;
   }
   // a donor's device geometry is shared, not rebuilt (batch engine: cases
   // that name the same mesh)
@@ -780,8 +782,8 @@ int run_rhs(thx_operator_s *h, const R *u, R *du, cudaStream_t s, int stage, dou
   if constexpr (!IsF32<R>::value) {
     if (h->lte) {
       cudaError_t te = h->dim == 2
-          ? launch_lte_temperature<2>(u, h->L, h->g64.lte, h->Tn, h->status, s)
-          : launch_lte_temperature<3>(u, h->L, h->g64.lte, h->Tn, h->status, s);
+          ? launch_lte_temperature<2>(u, h->L, h->g64.lte, h->Tn, h->Cn, h->status, s)
+          : launch_lte_temperature<3>(u, h->L, h->g64.lte, h->Tn, h->Cn, h->status, s);
       if (te != cudaSuccess) return THX_ERR_CUDA;
     }
   }

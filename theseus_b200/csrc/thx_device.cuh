@@ -40,6 +40,9 @@ struct GasT {
   // temperatures recovered once per right-hand side, [elem][node].
   LteDev lte{};
   const double *Tn = nullptr;
+  // table cell (lte_at's cell.off) of (rho, Tn) per node, written with Tn;
+  // -1 where lte_at finds none
+  const int *Cn = nullptr;
 };
 
 // The FP32-mixed path carries the state as an offset from qref and the
@@ -973,8 +976,9 @@ __device__ __forceinline__ LteEval lte_unpack(const double *x /* LTE_P_* block *
 
 // include/LTEHelmholtzGasEOS.hpp:144-157: (beta (g - |u|^2/2), beta u, -beta)
 template <int DIM>
-__device__ __forceinline__ void lte_entropy_vars(const LteDev &t, const double *q, double T, double *w) {
-  const LteEval s = lte_at(t, q[0], T);
+__device__ __forceinline__ void lte_entropy_vars(const LteDev &t, const double *q, double T, int cell,
+                                                 double *w) {
+  const LteEval s = lte_at_cell(t, q[0], T, cell);
   const double beta = 1 / s.T;
   double m2 = 0.0;
 #pragma unroll
@@ -1002,9 +1006,9 @@ __device__ __forceinline__ void lte_grad_entropy_to_prim(const double *q, double
 // (include/LTEHelmholtzGasEOS.hpp:133-142).
 template <int DIM>
 __device__ __forceinline__ void lte_viscous_flux(const GasT<double> &g, const double *q, double T,
-                                                 const double *dp, double *vf) {
+                                                 int cell, const double *dp, double *vf) {
   constexpr int NEQ = DIM + 2, E = DIM + 1;
-  const LteEval s = lte_at(g.lte, q[0], T);
+  const LteEval s = lte_at_cell(g.lte, q[0], T, cell);
   const double mu = lte_transport(g.lte, s, 4);
   const double kappa = lte_transport(g.lte, s, 5);
   const double rho = q[0];

@@ -248,7 +248,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
     if constexpr (VOL == VOL_LTEEC) {
       // conserved state, recovered T, its table cell and the pressure
       const double T = a.gas.Tn[(long long)e * ND + n];
-      const LteEval sv = lte_at(a.gas.lte, q[0], T);
+      const LteEval sv = lte_at_cell(a.gas.lte, q[0], T, a.gas.Cn[(long long)e * ND + n]);
       R pr[NPRIM];
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) pr[k] = q[k];
@@ -844,8 +844,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long 
     // include/LTEECFlux.hpp:86-99 with the Lax dissipation
     // (include/DissipationOperator.hpp:15-55); T recovered per node
     static_assert(!IsF32<R>::value, "LTEEC: FP64 only");
-    const LteEval sm = lte_at(a.gas.lte, qm[0], a.gas.Tn[im]);
-    const LteEval sp = lte_at(a.gas.lte, qp[0], a.gas.Tn[ip]);
+    const LteEval sm = lte_at_cell(a.gas.lte, qm[0], a.gas.Tn[im], a.gas.Cn[im]);
+    const LteEval sp = lte_at_cell(a.gas.lte, qp[0], a.gas.Tn[ip], a.gas.Cn[ip]);
     lte_ec_flux<DIM, true>(a.gas.lte, qm, qp, sm, sp, lte_face_jet(a.gas.lte, sm),
                            lte_face_jet(a.gas.lte, sp), nrm, nrm, F);
   } else {
@@ -987,7 +987,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) w[k] = a.svars[k * L + (long long)e * ND + n];
     } else if constexpr (LTE) {
-      lte_entropy_vars<DIM>(a.gas.lte, q, a.gas.Tn[(long long)e * ND + n], w);
+      lte_entropy_vars<DIM>(a.gas.lte, q, a.gas.Tn[(long long)e * ND + n], a.gas.Cn[(long long)e * ND + n], w);
     } else {
       entropy_vars<R, DIM>(a.gas, q, w);
     }
@@ -1020,7 +1020,9 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
         for (int k = 0; k < NEQ; ++k) ro[k] = a.u[k * L + (long long)eo * ND + no];
       }
       reconstruct<R, DIM>(a.gas, ro, qo);
-      if constexpr (LTE) lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], so);
+      if constexpr (LTE)
+        lte_entropy_vars<DIM>(a.gas.lte, qo, a.gas.Tn[(long long)eo * ND + no], a.gas.Cn[(long long)eo * ND + no],
+                              so);
       else entropy_vars<R, DIM>(a.gas, qo, so);
     }
 #pragma unroll
@@ -1148,7 +1150,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
     const double T = a.gas.Tn[(long long)e * ND + n];
 #pragma unroll
     for (int cc = 0; cc < DIM; ++cc) lte_grad_entropy_to_prim<DIM>(q, T, g[cc], dp + cc * NEQ);
-    lte_viscous_flux<DIM>(a.gas, q, T, dp, vf);
+    lte_viscous_flux<DIM>(a.gas, q, T, a.gas.Cn[(long long)e * ND + n], dp, vf);
   } else {
     const NodeGas<R, DIM> ng = node_gas<R, DIM>(a.gas, q);
 #pragma unroll
@@ -1432,7 +1434,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 3) grad_sv_kernel(cons
 // face, gradient and volume kernels read the stored T instead).
 template <int DIM>
 __global__ void __launch_bounds__(256, 2) lte_temperature_kernel(const double *u, long long L, LteDev t,
-                                                              double *Tn, unsigned *status) {
+                                                              double *Tn, int *Cn, unsigned *status) {
   constexpr int NEQ = DIM + 2;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride) {
@@ -1447,6 +1449,9 @@ __global__ void __launch_bounds__(256, 2) lte_temperature_kernel(const double *u
     int st;
     const double T = lte_temperature(t, q[0], ei, &st);
     Tn[i] = T;
+    // the node's table cell, read by the kernels that evaluate the gas here
+    const LteEval s = lte_at(t, q[0], T);
+    Cn[i] = s.valid ? s.cell.off : -1;
     if (st != LTE_CONVERGED) atomicOr(status, STATUS_EOS);
   }
 }

@@ -137,10 +137,10 @@ cudaError_t launch_entropy(const R *u, long long L, const GasT<R> &g, R *sv, cud
 
 template <int DIM>
 cudaError_t launch_lte_temperature(const double *u, long long L, const LteDev &t, double *Tn,
-                                   unsigned *status, cudaStream_t s) {
+                                   int *Cn, unsigned *status, cudaStream_t s) {
   if (L <= 0) return cudaSuccess;
   const int grid = (int)std::min<long long>((L + 255) / 256, 148LL * 8);
-  lte_temperature_kernel<DIM><<<grid, 256, 0, s>>>(u, L, t, Tn, status);
+  lte_temperature_kernel<DIM><<<grid, 256, 0, s>>>(u, L, t, Tn, Cn, status);
   return cudaGetLastError();
 }
 

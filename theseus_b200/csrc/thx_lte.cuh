@@ -170,6 +170,25 @@ THX_HD LteEval lte_cross(const LteEval &a, const LteEval &b) {
   return r;
 }
 
+// lte_at(t, rho, T) given the cell lte_at finds there (cell.off, as the
+// temperature recovery stores it per node): the same evaluation without the
+// two binary searches.  A cell that is not a valid lower corner (-1: none
+// found) falls back to the search.
+THX_HD LteEval lte_at_cell(const LteDev &t, double rho, double T, int cell) {
+  if (cell < 0) return lte_at(t, rho, T);
+  const int i = cell % t.nx, j = cell / t.nx;
+  if (i > t.nx - 2 || j > t.ny - 2) return lte_at(t, rho, T);
+  LteEval r;
+  const double dr = t.rho[i + 1] - t.rho[i], dt = t.T[j + 1] - t.T[j];
+  r.cell = {cell, t.nx, dr, dt};
+  r.xi = (rho - t.rho[i]) / dr;
+  r.eta = (T - t.T[j]) / dt;
+  r.rho = rho;
+  r.T = T;
+  r.valid = true;
+  return r;
+}
+
 THX_HD double lte_pressure(const LteDev &t, const LteEval &s) {
   return s.rho * s.rho * lte_eval<1, 0>(t, s.cell, s.xi, s.eta);
 }

@@ -179,6 +179,7 @@ struct thx_operator_s {
   thx::GasT<float> g32;
   bool lte = false;        // LTE Helmholtz gas (g64.lte, g64.Tn on the device)
   double *Tn = nullptr;    // recovered node temperatures [elem][node]
+  int *Cn = nullptr;       // their table cells (lte_at's cell.off; -1: none)
   double threshold = 0.0;
   double adv_scale = 0.0, dif_scale = 0.0, surf_scale = 0.0;
   std::vector<void *> allocs;
