@@ -461,7 +461,7 @@ def run_ours(args):
                                # as one flop; the FP64 pipe also runs their
                                # iterations, so it is busier than frac says
                                "ncu_fp64_pipe_active": 0.483, "ncu_issue_active": 0.666,
-                               "ncu_source": "profiles/volume_kernel_ns_tgv_20cubed_p4_fp64.md "
+                               "ncu_source": "ncu capture of this volume kernel on the 20^3 mesh "
                                              "(sm__pipe_fp64_cycles_active, smsp__issue_active)"}
 
     # the volume kernel with its element blocks' state staged by bulk copy
