@@ -876,6 +876,15 @@ __global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
   face_body<R, DIM, SURF, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// The LTEEC face flux: the same body compiled for four resident CTAs per SM
+// (128 registers).  Left to itself the compiler takes 255 registers and two
+// CTAs fit; with the spills of the bounded form it is still 15 % faster (24^3
+// p=4: 0.244 -> 0.208 ms; three CTAs, 168 registers: 0.215 ms).
+template <int DIM, bool NS>
+__global__ void __launch_bounds__(128, 4) face_kernel_lte(const FaceArgs<double> a) {
+  face_body<double, DIM, SURF_LTEEC, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 template <typename R>
 struct GradArgs {
@@ -1419,6 +1428,14 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
 template <typename R, int DIM, int N, bool LTE, bool SV = false>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
   grad_body<R, DIM, N, LTE, SV>(a, blockIdx.x);
+}
+
+// The LTE gradient: the same body compiled for three resident CTAs per SM
+// (80 registers; the compiler's own 124 fit two): 0.279 -> 0.235 ms at 24^3
+// p=4 (four CTAs, 64 registers with heavier spills: 0.243 ms).
+template <int DIM, int N>
+__global__ void __launch_bounds__(Shape<DIM, N>::THREADS, 3) grad_kernel_lte(const GradArgs<double> a) {
+  grad_body<double, DIM, N, true, false>(a, blockIdx.x);
 }
 
 // The gradient kernel that reads precomputed entropy variables, bounded to

@@ -93,7 +93,8 @@ cudaError_t launch_face(const FaceArgs<R> &a, cudaStream_t s) {
   const long long total = (long long)a.nf * nfp;
   if (total <= 0) return cudaSuccess;
   const int grid = (int)((total + 127) / 128);
-  face_kernel<R, DIM, SURF, NS><<<grid, 128, 0, s>>>(a);
+  if constexpr (SURF == SURF_LTEEC) face_kernel_lte<DIM, NS><<<grid, 128, 0, s>>>(a);
+  else face_kernel<R, DIM, SURF, NS><<<grid, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -101,12 +102,20 @@ template <typename R, int DIM, int N, bool LTE = false>
 cudaError_t launch_grad(const GradArgs<R> &a, cudaStream_t s, int prepare) {
   using S = Shape<DIM, N>;
   constexpr size_t smem = grad_smem_bytes<R, DIM, N>();
-  if (prepare)
-    return cudaFuncSetAttribute(grad_kernel<R, DIM, N, LTE>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (a.ne <= 0) return cudaSuccess;
-  const int grid = (a.ne + S::EPB - 1) / S::EPB;
-  grad_kernel<R, DIM, N, LTE><<<grid, S::THREADS, smem, s>>>(a);
+  if constexpr (LTE) {
+    if (prepare)
+      return cudaFuncSetAttribute(grad_kernel_lte<DIM, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem);
+    if (a.ne <= 0) return cudaSuccess;
+    grad_kernel_lte<DIM, N><<<(a.ne + S::EPB - 1) / S::EPB, S::THREADS, smem, s>>>(a);
+  } else {
+    if (prepare)
+      return cudaFuncSetAttribute(grad_kernel<R, DIM, N, LTE>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (a.ne <= 0) return cudaSuccess;
+    const int grid = (a.ne + S::EPB - 1) / S::EPB;
+    grad_kernel<R, DIM, N, LTE><<<grid, S::THREADS, smem, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
