@@ -142,6 +142,8 @@ struct Group {
   double best_cost = -1.0;
   int tune_axis = 0, tune_index = 0;  // 0 CTA size, 1 volume, 2 face, 3 gradient; 4: done
   int tune_rep = 0;                   // timings taken of the current candidate
+  bool members_changed = true;        // cases joined or left since the last launch
+  int unsteady = 0;                   // candidate launches deferred in a row
   bool tuned = false;
   Grids timing_grids;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -811,6 +813,7 @@ class Engine final : public EngineBase {
       if (q != cudaSuccess) return cuda_failed(q, "cudaEventQuery(case set-up)");
       G.cases.push_back(c);
       G.pending.erase(G.pending.begin() + i);
+      G.members_changed = true;
       G.dirty = true;
     }
     // cases with fewer steps left than a launch holds finish one at a time
@@ -825,6 +828,7 @@ class Engine final : public EngineBase {
         c->finished = true;
         THX_CU(cudaEventRecord(c->done, G.stream));
         G.cases.erase(G.cases.begin() + i);
+        G.members_changed = true;
         G.dirty = true;
       } else {
         ++i;
@@ -839,8 +843,20 @@ class Engine final : public EngineBase {
     int st;
     typename Group<R>::Grids grids = G.best;
     bool measure = false;
-    if (!G.tuned && !G.timing && tune_candidate(G, G.tune_index, grids)) measure = true;
-    else if (!G.tuned && G.timing && G.exec) grids = G.exec_grids;
+    if (!G.tuned && !G.timing && tune_candidate(G, G.tune_index, grids)) {
+      // time a candidate on a launch with the same cases as the one before
+      // (a launch that cases joined or left runs a different load); after
+      // four such launches in a row, time it anyway
+      if (G.members_changed && G.unsteady < 4) {
+        ++G.unsteady;
+        grids = G.exec ? G.exec_grids : G.best;
+      } else {
+        measure = true;
+        G.unsteady = 0;
+      }
+    } else if (!G.tuned && G.timing && G.exec) {
+      grids = G.exec_grids;
+    }
     // the work lists follow the CTA size
     const int epb = grids.half ? G.epb_half : G.epb_full;
     if (epb != G.epb) {
@@ -863,6 +879,7 @@ class Engine final : public EngineBase {
       G.timing_work = G.nodes * k_;
     }
     ++launches_;
+    G.members_changed = false;
     t_launch_ += now() - tb;
     THX_CU(cudaEventRecord(G.ring[G.ring_pos], G.stream));
     G.ring_pos ^= 1;
@@ -873,6 +890,7 @@ class Engine final : public EngineBase {
         c->finished = true;
         THX_CU(cudaEventRecord(c->done, G.stream));
         G.cases.erase(G.cases.begin() + i);
+        G.members_changed = true;
         G.dirty = true;
       } else {
         ++i;

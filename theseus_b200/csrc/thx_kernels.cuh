@@ -953,7 +953,9 @@ __global__ void __launch_bounds__(256) entropy_kernel(const R *__restrict__ u, l
 // BR1 gradient (include/NSOperator_impl.hpp:11-159,194-517;
 // include/DGSEMIntegrator.hpp:764-850,1011-1044).  SV: the entropy variables
 // come from a.svars (entropy_kernel) instead of being evaluated here.
-template <typename R, int DIM, int N, bool LTE, bool SV = false, int EPBX = 0>
+// NARROW: compiled with the FP32-mixed reading of an FP64 state (GradArgs::u64);
+// the batched kernels, which never take it, leave it out.
+template <typename R, int DIM, int N, bool LTE, bool SV = false, int EPBX = 0, bool NARROW = false>
 __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block) {
   static_assert(!LTE || !IsF32<R>::value, "LTE gas: FP64 only");
   using S = Shape<DIM, N, EPBX>;
@@ -976,7 +978,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
   R q[NEQ];
   if (active) {
     R raw[NEQ];
-    if (IsF32<R>::value && a.u64) {
+    if (NARROW && IsF32<R>::value && a.u64) {
       double d[NEQ];
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) d[k] = a.u64[k * L + (long long)e * ND + n];
@@ -1021,7 +1023,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
       for (int k = 0; k < NEQ; ++k) so[k] = a.svars[k * L + (long long)eo * ND + no];
     } else {
       R ro[NEQ], qo[NEQ];
-      if (IsF32<R>::value && a.u64) {
+      if (NARROW && IsF32<R>::value && a.u64) {
 #pragma unroll
         for (int k = 0; k < NEQ; ++k) ro[k] = (R)(a.u64[k * L + (long long)eo * ND + no] - a.off[k]);
       } else {
@@ -1427,7 +1429,7 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
 
 template <typename R, int DIM, int N, bool LTE, bool SV = false>
 __global__ void __launch_bounds__(Shape<DIM, N>::THREADS) grad_kernel(const GradArgs<R> a) {
-  grad_body<R, DIM, N, LTE, SV>(a, blockIdx.x);
+  grad_body<R, DIM, N, LTE, SV, 0, IsF32<R>::value>(a, blockIdx.x);
 }
 
 // The LTE gradient: the same body compiled for three resident CTAs per SM
