@@ -295,7 +295,8 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) rate[k] = R(0);
 
-#pragma unroll 1
+  // directions unrolled: 2 % faster than rolled (32^3 p=4, FP64 and FP32)
+#pragma unroll
   for (int dir = 0; dir < DIM; ++dir) {
     // pair phase: every symmetric pair once, in (lower, upper) order
     for (int t = tid; t < EPB * PAIRS; t += blockDim.x) {
