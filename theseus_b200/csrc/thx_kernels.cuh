@@ -299,7 +299,7 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
 #pragma unroll
   for (int dir = 0; dir < DIM; ++dir) {
     // pair phase: every symmetric pair once, in (lower, upper) order
-    for (int t = tid; t < EPB * PAIRS; t += blockDim.x) {
+    for (int t = tid; t < EPB * PAIRS; t += S::THREADS) {  // launched with S::THREADS
       const int pel = t / PAIRS, pidx = t % PAIRS;
       if (e0 + pel >= a.ne) continue;
       const unsigned nn = sPT[dir * PAIRS + pidx];
@@ -1008,7 +1008,7 @@ __device__ __forceinline__ void grad_body(const GradArgs<R> &a, const int block)
   }
   // entropy variables of the neighbour's trace at every face point of the
   // CTA's elements, one converged task per face point
-  for (int t = tid; t < EPB * NLF * NFP; t += blockDim.x) {
+  for (int t = tid; t < EPB * NLF * NFP; t += S::THREADS) {  // launched with S::THREADS
     const int tel = t / (NLF * NFP), lf = (t / NFP) % NLF, fp = t % NFP;
     const int te = e0 + tel;
     if (te >= a.ne) continue;
@@ -1260,7 +1260,7 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
   }
   __syncthreads();
   // lift factors of every face point of the CTA's elements
-  for (int t = tid; t < EPB * NLF * NFP; t += blockDim.x) {
+  for (int t = tid; t < EPB * NLF * NFP; t += S::THREADS) {  // launched with S::THREADS
     const int tel = t / (NLF * NFP), lf = (t / NFP) % NLF, fp = t % NFP;
     const int te = e0 + tel;
     if (te >= a.ne) continue;
