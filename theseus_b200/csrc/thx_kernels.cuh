@@ -295,8 +295,10 @@ __device__ __forceinline__ void volume_body(const VolArgs<R> &a, const int block
 #pragma unroll
   for (int k = 0; k < NEQ; ++k) rate[k] = R(0);
 
-  // directions unrolled: 2 % faster than rolled (32^3 p=4, FP64 and FP32)
-#pragma unroll
+  // directions unrolled: 2 % faster than rolled (32^3 p=4, FP64 and FP32);
+  // rolled for the LTEEC flux, whose spills it would multiply
+  constexpr int DIR_UNROLL = VOL == VOL_LTEEC ? 1 : DIM;
+#pragma unroll DIR_UNROLL
   for (int dir = 0; dir < DIM; ++dir) {
     // pair phase: every symmetric pair once, in (lower, upper) order
     for (int t = tid; t < EPB * PAIRS; t += S::THREADS) {  // launched with S::THREADS
