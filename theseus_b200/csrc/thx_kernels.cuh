@@ -1261,7 +1261,9 @@ __device__ __forceinline__ void grad_body_sv(const GradArgs<R> &a, const int blo
     sK[t] = kind;
   }
   __syncthreads();
-  // lift factors of every face point of the CTA's elements
+  // lift factors of every face point of the CTA's elements (unrolled: the
+  // neighbours' gathers of the iterations issue together)
+#pragma unroll
   for (int t = tid; t < EPB * NLF * NFP; t += S::THREADS) {  // launched with S::THREADS
     const int tel = t / (NLF * NFP), lf = (t / NFP) % NLF, fp = t % NFP;
     const int te = e0 + tel;
