@@ -874,15 +874,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<R> &a, const long long 
   for (int k = 0; k < NEQ; ++k) a.fstar[((long long)f * NEQ + k) * nfp + fp] = F[k];
 }
 
-template <typename R, int DIM, int SURF, bool NS>
-__global__ void __launch_bounds__(128) face_kernel(const FaceArgs<R> a) {
-  face_body<R, DIM, SURF, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+// The face kernels: one thread per face point, each precision compiled for
+// its own number of resident 128-thread CTAs per SM.  FP64: eight (64
+// registers, some spills; 0.166 -> 0.158 ms at 32^3 p=4 NS against the
+// compiler's 92 registers at five CTAs; six, ten and twelve CTAs were no
+// faster or slower).  FP32: ten (48 registers; 2 % faster than the
+// compiler's 62 at eight).
+template <int DIM, int SURF, bool NS>
+__global__ void __launch_bounds__(128, 8) face_kernel_f64(const FaceArgs<double> a) {
+  face_body<double, DIM, SURF, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
-
-// FP32 face fluxes: the same body compiled for ten resident CTAs per SM (48
-// registers; 2 % faster than the compiler's 62 at eight CTAs).  The FP64
-// kernel keeps its own choice: an explicit bound changed its code for the
-// worse.
 template <int DIM, int SURF, bool NS>
 __global__ void __launch_bounds__(128, 10) face_kernel_f32(const FaceArgs<float> a) {
   face_body<float, DIM, SURF, NS>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);

@@ -95,7 +95,7 @@ cudaError_t launch_face(const FaceArgs<R> &a, cudaStream_t s) {
   const int grid = (int)((total + 127) / 128);
   if constexpr (SURF == SURF_LTEEC) face_kernel_lte<DIM, NS><<<grid, 128, 0, s>>>(a);
   else if constexpr (IsF32<R>::value) face_kernel_f32<DIM, SURF, NS><<<grid, 128, 0, s>>>(a);
-  else face_kernel<R, DIM, SURF, NS><<<grid, 128, 0, s>>>(a);
+  else face_kernel_f64<DIM, SURF, NS><<<grid, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
